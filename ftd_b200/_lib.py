@@ -1,0 +1,77 @@
+"""ctypes binding of ``libftdx.so`` (the C ABI declared in ``include/ftdx.h``).
+
+The library is loaded from the package directory.  There is no fallback: if
+the shared library is missing or fails to load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libftdx.so")
+
+FTDX_OK = 0
+STATUS_NAMES = {
+    0: "FTDX_OK", 1: "FTDX_ERR_INVALID_ARG", 2: "FTDX_ERR_UNSUPPORTED", 3: "FTDX_ERR_CUDA",
+    4: "FTDX_ERR_NO_DEVICE", 5: "FTDX_ERR_ALLOC", 6: "FTDX_ERR_CAPACITY", 7: "FTDX_ERR_TIMEOUT",
+    8: "FTDX_ERR_CACHE",
+}
+
+# enum values (include/ftdx.h)
+IN_FP16, IN_INT4 = 0, 1
+COMPUTE_FP8, COMPUTE_FP6, COMPUTE_FP4 = 0, 1, 2
+OUT_FP16, OUT_FP32 = 0, 1
+FORMAT_PACKED_TRIANGLE = 0
+
+
+class FtdxError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("verbosity", ctypes.c_int),
+                ("tune_cache", ctypes.c_char_p), ("reserved", ctypes.c_int * 8)]
+
+
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_f = ctypes.c_float
+
+# name -> (restype, argtypes); every function include/ftdx.h declares.
+PROTOTYPES = {
+    "ftdx_version": (_i, []),
+    "ftdx_status_string": (ctypes.c_char_p, [_i]),
+    "ftdx_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(Config)]),
+    "ftdx_destroy": (_i, [_vp]),
+    "ftdx_last_error": (ctypes.c_char_p, [_vp]),
+    "ftdx_herk": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _f, _f, _vp, _i]),
+    "ftdx_init_herk": (_i, [_vp, _i, _i, _i, _vp]),
+    "ftdx_end_herk": (_i, [_vp]),
+    "ftdx_device_status": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32)]),
+}
+
+_lib = None
+
+
+def load():
+    """Load libftdx.so (raises if it is missing: there is no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FtdxError(4, f"{LIB_PATH} is missing; build it with `python -m ftd_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in PROTOTYPES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(h, status: int, what: str):
+    if status != FTDX_OK:
+        msg = load().ftdx_last_error(h) if h else b""
+        raise FtdxError(status, f"{what}: {(msg or b'').decode(errors='replace')}")

@@ -1,0 +1,163 @@
+"""Python host mirror of the reference's HERK interface, over the C ABI.
+
+``Correlator`` mirrors ``cutlass_gemm_api::CutlassComplexGemm``
+(cutlass_interface/cutlass_gemm_api.h:157-789): ``herk``, ``init_herk``,
+``end_herk``.  The module functions mirror the GGP engine boundary
+(lib/cutlass_interface.cu:150-307): ``herk_batched_cutlass_qc`` (FP32 packed
+output), ``herk_batched_cutlass_qc_fp16`` and ``herk_batched_cutlass_fp16``.
+
+Arguments are device buffers: torch CUDA tensors or raw device addresses
+(int).  Streams are ``torch.cuda.Stream`` objects, raw handles (int) or None
+(the current torch stream when torch is in use, else the legacy stream).
+"""
+from __future__ import annotations
+
+import ctypes
+
+from . import _lib
+from ._lib import (COMPUTE_FP8, FORMAT_PACKED_TRIANGLE, IN_FP16, IN_INT4, OUT_FP16, OUT_FP32,
+                   FtdxError, check, load)
+
+__all__ = ["Correlator", "herk_batched_cutlass_qc", "herk_batched_cutlass_qc_fp16",
+           "herk_batched_cutlass_fp16", "init_cutlass_api", "tri_size", "FtdxError",
+           "IN_FP16", "IN_INT4", "OUT_FP16", "OUT_FP32", "COMPUTE_FP8"]
+
+
+def tri_size(n: int) -> int:
+    return n * (n + 1) // 2
+
+
+def _ptr(x) -> int:
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        if hasattr(x, "is_cuda") and not x.is_cuda:
+            raise FtdxError(1, "tensor is not on a CUDA device")
+        return x.data_ptr()
+    raise TypeError(f"cannot take a device pointer of {type(x)!r}")
+
+
+def _stream(s) -> int:
+    if s is None:
+        try:
+            import torch
+            if torch.cuda.is_available() and torch.cuda.is_initialized():
+                return torch.cuda.current_stream().cuda_stream
+        except ImportError:
+            pass
+        return 0
+    if isinstance(s, int):
+        return s
+    return s.cuda_stream
+
+
+class Correlator:
+    """One handle of the correlator library (not thread-safe; one per thread)."""
+
+    def __init__(self, device: int = -1, verbosity: int = 0, tune_cache: str | None = None):
+        L = load()
+        cfg = _lib.Config()
+        cfg.device = device
+        cfg.verbosity = verbosity
+        cfg.tune_cache = tune_cache.encode() if tune_cache else None
+        h = ctypes.c_void_p()
+        st = L.ftdx_create(ctypes.byref(h), ctypes.byref(cfg))
+        check(None, st, "ftdx_create")
+        self._h = h
+        self._L = L
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.ftdx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------ HERK
+    def herk(self, A, C, N: int, K: int, batch: int, input: int = IN_FP16,
+             compute: int = COMPUTE_FP8, output: int = OUT_FP16,
+             format: int = FORMAT_PACKED_TRIANGLE, alpha: float = 1.0, beta: float = 0.0,
+             stream=None, tune: bool = True) -> None:
+        """C = alpha * A A^H + beta * C (batched, packed lower triangle).
+
+        Defaults follow CutlassComplexGemm::herk (cutlass_gemm_api.h:750-760)."""
+        st = self._L.ftdx_herk(self._h, _ptr(A), _ptr(C), N, K, batch, input, compute, output,
+                               format, float(alpha), float(beta), _stream(stream), int(bool(tune)))
+        check(self._h, st, "ftdx_herk")
+
+    def init_herk(self, N: int, K: int, batch: int, stream=None) -> None:
+        check(self._h, self._L.ftdx_init_herk(self._h, N, K, batch, _stream(stream)),
+              "ftdx_init_herk")
+
+    def end_herk(self) -> None:
+        check(self._h, self._L.ftdx_end_herk(self._h), "ftdx_end_herk")
+
+    def device_status(self, stream=None) -> int:
+        """Synchronise the stream and return (and clear) the device status bits."""
+        bits = ctypes.c_uint32(0)
+        st = self._L.ftdx_device_status(self._h, _stream(stream), ctypes.byref(bits))
+        if st not in (_lib.FTDX_OK, 7):
+            check(self._h, st, "ftdx_device_status")
+        return bits.value
+
+
+# ---------------------------------------------------------------- GGP boundary
+_api: Correlator | None = None
+_tune_enabled = False
+
+
+def _get_api() -> Correlator:
+    global _api
+    if _api is None:
+        _api = Correlator()
+    return _api
+
+
+def init_cutlass_api(kernel_tune_verbosity: int = 0, kernel_tune_cache_path: str | None = None,
+                     strategy_tune_cache_path: str | None = None, herk_tune: bool = False,
+                     strategy_tune_verbosity: int = 1) -> None:
+    """Mirror of ggp::initCutlassApi (lib/cutlass_interface.cu:150-169)."""
+    global _api, _tune_enabled
+    if _api is not None:
+        _api.close()
+    _api = Correlator(verbosity=strategy_tune_verbosity if strategy_tune_verbosity > 1 else 0,
+                      tune_cache=strategy_tune_cache_path)
+    _tune_enabled = bool(herk_tune)
+
+
+def herk_batched_cutlass_qc(qc, tri, N: int, K: int, batch: int, stream=None) -> int:
+    """Mirror of ggp::herkBatchedCutlassQC (lib/cutlass_interface.cu:178-231): QC int4
+    [batch][N][K] -> FP32 packed triangle.  Returns 0 on success (raises otherwise)."""
+    _get_api().herk(qc, tri, N, K, batch, IN_INT4, COMPUTE_FP8, OUT_FP32,
+                    stream=stream, tune=_tune_enabled)
+    return 0
+
+
+def herk_batched_cutlass_qc_fp16(qc, tri, N: int, K: int, batch: int, stream=None) -> int:
+    """Mirror of ggp::herkBatchedCutlassQC_FP16 (lib/cutlass_interface.cu:243-289)."""
+    _get_api().herk(qc, tri, N, K, batch, IN_INT4, COMPUTE_FP8, OUT_FP16,
+                    stream=stream, tune=_tune_enabled)
+    return 0
+
+
+def herk_batched_cutlass_fp16(a16, tri, N: int, K: int, batch: int, stream=None) -> int:
+    """Mirror of ggp::herkBatchedCutlassFP16 (lib/cutlass_interface.cu:292-307)."""
+    _get_api().herk(a16, tri, N, K, batch, IN_FP16, COMPUTE_FP8, OUT_FP16,
+                    stream=stream, tune=_tune_enabled)
+    return 0

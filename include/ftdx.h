@@ -1,0 +1,114 @@
+/* ftdx.h -- C ABI of the B200 (sm_100a) X-engine correlator.
+ *
+ * One call computes, for every channel (batch entry) b,
+ *     C_b = alpha * A_b * A_b^H + beta * C_b
+ * where A_b is an N x K complex voltage matrix (N inputs = antennas x pols,
+ * K time samples) and C_b is stored as the packed lower triangle, row-major:
+ * element (i, j <= i) at i(i+1)/2 + j, interleaved (re, im), with Im(C_ii)
+ * forced to 0 before beta is applied.
+ *
+ * All data pointers are DEVICE pointers owned by the caller.  Work is queued
+ * on the caller's stream (`stream` is a cudaStream_t; NULL = legacy default
+ * stream).  Calls return immediately; a device-side wait that timed out is
+ * reported by ftdx_device_status().  No function throws, aborts or exits.
+ * A handle is not thread-safe: use one handle per host thread.
+ *
+ * Reference interfaces replaced (paths within cpviolator/ftd):
+ *   cutlass_interface/cutlass_gemm_api.h:157-789   class CutlassComplexGemm
+ *   lib/cutlass_interface.cu:150-307               ggp::initCutlassApi,
+ *                                                  ggp::herkBatchedCutlassQC{,_FP16},
+ *                                                  ggp::herkBatchedCutlassFP16
+ */
+#ifndef FTDX_H_
+#define FTDX_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FTDX_API __attribute__((visibility("default")))
+#else
+#define FTDX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FTDX_VERSION_MAJOR 0
+#define FTDX_VERSION_MINOR 1
+
+typedef enum ftdx_status {
+  FTDX_OK = 0,
+  FTDX_ERR_INVALID_ARG = 1,   /* bad size, null or misaligned pointer, bad enum */
+  FTDX_ERR_UNSUPPORTED = 2,   /* valid request this build does not implement */
+  FTDX_ERR_CUDA = 3,          /* a CUDA runtime/driver call failed */
+  FTDX_ERR_NO_DEVICE = 4,     /* no CUDA device, or not an sm_100 device */
+  FTDX_ERR_ALLOC = 5,         /* workspace allocation failed */
+  FTDX_ERR_CAPACITY = 6,      /* workspace too small while a graph is being captured */
+  FTDX_ERR_TIMEOUT = 7,       /* a bounded device-side wait gave up */
+  FTDX_ERR_CACHE = 8          /* tune cache file unreadable / malformed */
+} ftdx_status;
+
+/* Values equal the reference's enum class ordinals
+ * (cutlass_interface/cutlass_gemm_api.h:37-59). */
+typedef enum ftdx_input { FTDX_IN_FP16 = 0, FTDX_IN_INT4 = 1 } ftdx_input;
+typedef enum ftdx_compute {
+  FTDX_COMPUTE_FP8 = 0,
+  FTDX_COMPUTE_FP6 = 1,
+  FTDX_COMPUTE_FP4 = 2
+} ftdx_compute;
+typedef enum ftdx_output { FTDX_OUT_FP16 = 0, FTDX_OUT_FP32 = 1 } ftdx_output;
+typedef enum ftdx_format { FTDX_FORMAT_PACKED_TRIANGLE = 0 } ftdx_format;
+
+typedef struct ftdx_context* ftdx_handle;
+
+/* Handle configuration; zero-initialise and set what you need. */
+typedef struct ftdx_config {
+  int device;               /* CUDA device ordinal; <0 = current device */
+  int verbosity;            /* 0 silent, 1 summary, 2+ detailed (stderr) */
+  const char* tune_cache;   /* autotune cache file; NULL = $FTDX_TUNE_CACHE or none */
+  int reserved[8];
+} ftdx_config;
+
+/* Library version as (major << 16) | minor. */
+FTDX_API int ftdx_version(void);
+
+/* Human-readable text for a status code (static storage). */
+FTDX_API const char* ftdx_status_string(ftdx_status s);
+
+/* Create / destroy a handle.  Replaces CutlassComplexGemm::CutlassComplexGemm
+ * and ~CutlassComplexGemm (cutlass_gemm_api.h:159-164). cfg may be NULL. */
+FTDX_API ftdx_status ftdx_create(ftdx_handle* h, const ftdx_config* cfg);
+FTDX_API ftdx_status ftdx_destroy(ftdx_handle h);
+
+/* Text of the last error raised on this handle (static until the next call). */
+FTDX_API const char* ftdx_last_error(ftdx_handle h);
+
+/* Batched HERK.  Replaces CutlassComplexGemm::herk (cutlass_gemm_api.h:750-760,
+ * cutlass_gemm_api.cu:1707-1878).
+ *   A: INT4 -> [batch][N][K] QC bytes (high nibble Re, low nibble Im,
+ *             sign-magnitude); FP16 -> [batch][N][K][2] __half.
+ *   C: FP32 -> [batch][N(N+1)/2][2] float; FP16 -> [batch][N(N+1)/2][2] __half.
+ *   compute must be FTDX_COMPUTE_FP8 (FP6/FP4 -> FTDX_ERR_UNSUPPORTED).
+ *   Any K >= 1 is accepted (tails are zero-padded internally).
+ *   tune != 0 consults/updates the autotune cache for this shape. */
+FTDX_API ftdx_status ftdx_herk(ftdx_handle h, const void* A, void* C, int N, int K, int batch,
+                      ftdx_input input, ftdx_compute compute, ftdx_output output,
+                      ftdx_format format, float alpha, float beta, void* stream, int tune);
+
+/* Pre-size the workspace for problems up to (N, K, batch) so that later
+ * ftdx_herk calls allocate nothing (required before graph capture).
+ * Replaces CutlassComplexGemm::init_herk / end_herk (cutlass_gemm_api.h:617-624). */
+FTDX_API ftdx_status ftdx_init_herk(ftdx_handle h, int N, int K, int batch, void* stream);
+FTDX_API ftdx_status ftdx_end_herk(ftdx_handle h);
+
+/* Synchronise `stream`, then read and clear the device status word written by
+ * bounded waits inside the kernels.  *bits = 0 means no wait timed out.
+ * Returns FTDX_ERR_TIMEOUT if any bit was set. */
+FTDX_API ftdx_status ftdx_device_status(ftdx_handle h, void* stream, uint32_t* bits);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FTDX_H_ */

@@ -1,0 +1,39 @@
+#!/usr/bin/env bash
+# Builds oracle/_ref/libref_herk.so from the reference's own host correlator
+# code.  Reads the reference tree (default /root/reference, or $FTD_REFERENCE)
+# and writes only into oracle/_ref/ (git-ignored).  The extracted text is
+# never committed; ref_harness.cpp (ours) includes it.
+set -euo pipefail
+HERE="$(cd "$(dirname "$0")" && pwd)"
+REF="${FTD_REFERENCE:-/root/reference}"
+OUT="$HERE/_ref"
+T1="$REF/cutlass_interface/test_herk_int4.cu"
+T2="$REF/tests/visibility_pipeline_test.cpp"
+if [[ ! -f "$T1" || ! -f "$T2" ]]; then
+  echo "build_ref: reference sources not found under $REF" >&2
+  exit 2
+fi
+mkdir -p "$OUT"
+# Print the definition of a static function: from its signature line to the
+# first line that is a lone closing brace.
+extract() {  # file name
+  awk -v name="$2" '
+    !on && $0 ~ "^static .*[ *&]" name "\\(" { on = 1 }
+    on { print }
+    on && $0 ~ /^}[ \t]*$/ { exit }
+  ' "$1"
+}
+{
+  echo "// extracted from the reference tree by oracle/build_ref.sh -- do not commit"
+  extract "$T1" encode_int4
+  extract "$T1" cpu_herk
+  extract "$T2" decode_qc_byte
+  extract "$T2" cpu_herk_batch_first
+} > "$OUT/ref_extract.inc"
+for f in encode_int4 cpu_herk decode_qc_byte cpu_herk_batch_first; do
+  grep -q "$f(" "$OUT/ref_extract.inc" || { echo "build_ref: $f not found" >&2; exit 3; }
+done
+/usr/bin/g++ -O3 -fopenmp -march=x86-64-v3 -std=c++17 -fPIC -shared -I"$OUT" \
+    "$HERE/ref_harness.cpp" -o "$OUT/libref_herk.so.tmp"
+mv "$OUT/libref_herk.so.tmp" "$OUT/libref_herk.so"
+echo "$OUT/libref_herk.so"

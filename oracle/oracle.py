@@ -1,0 +1,165 @@
+"""CPU oracle for the correlator -- test infrastructure only.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module, and only as the checker or the timed CPU
+baseline; the product (``ftd_b200``) never does.
+
+* ``liboracle.so`` (``herk_oracle.c``): our C restatement of the reference's
+  host correlator ``cpu_herk`` (cutlass_interface/test_herk_int4.cu:51-70)
+  with exact int64 accumulation for QC int4 input and FP64 for float input.
+* ``_ref/libref_herk.so`` (``build_ref.sh`` + ``ref_harness.cpp``): the
+  reference's own ``cpu_herk``, ``encode_int4``, ``decode_qc_byte`` and
+  ``cpu_herk_batch_first`` compiled from the reference tree, used to pin the
+  restatement and as the timed CPU baseline.
+* Seeded input generators for the workloads the correlator is measured on.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libref_herk.so")
+
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_f32p = ctypes.POINTER(ctypes.c_float)
+
+_lib = None
+_ref = None
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the committed Makefile (if missing/stale)."""
+    src = os.path.join(HERE, "herk_oracle.c")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(src) > os.path.getmtime(LIB_PATH):
+        subprocess.run(["make", "-C", HERE, "liboracle.so"], check=True, capture_output=True)
+    return LIB_PATH
+
+
+def build_ref() -> str | None:
+    """Compile the reference's host correlator into _ref/ (needs the reference tree)."""
+    r = subprocess.run(["bash", os.path.join(HERE, "build_ref.sh")], capture_output=True, text=True)
+    return REF_PATH if r.returncode == 0 else None
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.oracle_encode_qc.argtypes = [_i32p, _i32p, ctypes.c_int64, _u8p]
+        L.oracle_decode_qc.argtypes = [_u8p, ctypes.c_int64, _i32p, _i32p]
+        L.oracle_herk_qc.argtypes = [_u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i64p]
+        L.oracle_herk_qc_rows.argtypes = [_u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, _i64p]
+        L.oracle_herk_c128.argtypes = [_f64p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f64p]
+        L.oracle_num_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def ref_lib():
+    """The reference's own host correlator, or None when it was not built."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_PATH):
+            return None
+        L = ctypes.CDLL(REF_PATH)
+        L.ref_gen_int4.argtypes = [ctypes.c_uint32, ctypes.c_int64, _u8p]
+        L.ref_encode.argtypes = [_i32p, _i32p, ctypes.c_int64, _u8p]
+        L.ref_cpu_herk.argtypes = [_u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f64p]
+        L.ref_cpu_herk_batch_first.argtypes = [_u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p]
+        L.ref_num_threads.restype = ctypes.c_int
+        _ref = L
+    return _ref
+
+
+# ----------------------------------------------------------------- codecs
+def encode_qc(re: np.ndarray, im: np.ndarray) -> np.ndarray:
+    re = np.ascontiguousarray(re, dtype=np.int32)
+    im = np.ascontiguousarray(im, dtype=np.int32)
+    out = np.empty(re.shape, dtype=np.uint8)
+    lib().oracle_encode_qc(_p(re, _i32p), _p(im, _i32p), re.size, _p(out, _u8p))
+    return out
+
+
+def decode_qc(qc: np.ndarray):
+    qc = np.ascontiguousarray(qc, dtype=np.uint8)
+    re = np.empty(qc.shape, dtype=np.int32)
+    im = np.empty(qc.shape, dtype=np.int32)
+    lib().oracle_decode_qc(_p(qc, _u8p), qc.size, _p(re, _i32p), _p(im, _i32p))
+    return re, im
+
+
+# ----------------------------------------------------------------- correlators
+def tri_size(n: int) -> int:
+    return n * (n + 1) // 2
+
+
+def herk_qc(qc: np.ndarray, N: int, K: int, batch: int) -> np.ndarray:
+    """Exact packed lower triangles, int64 array [batch, N(N+1)/2, 2]."""
+    qc = np.ascontiguousarray(qc, dtype=np.uint8).reshape(-1)
+    assert qc.size == batch * N * K
+    out = np.empty((batch, tri_size(N), 2), dtype=np.int64)
+    lib().oracle_herk_qc(_p(qc, _u8p), N, K, batch, _p(out, _i64p))
+    return out
+
+
+def herk_qc_rows(qc: np.ndarray, N: int, K: int, b: int, i0: int, i1: int) -> np.ndarray:
+    """Rows [i0, i1) of channel b, int64 [sum_i (i+1), 2] (rows back to back)."""
+    qc = np.ascontiguousarray(qc, dtype=np.uint8).reshape(-1)
+    n = tri_size(i1) - tri_size(i0)
+    out = np.empty((n, 2), dtype=np.int64)
+    lib().oracle_herk_qc_rows(_p(qc, _u8p), N, K, b, i0, i1, _p(out, _i64p))
+    return out
+
+
+def herk_c128(a: np.ndarray, N: int, K: int, batch: int) -> np.ndarray:
+    """FP64 packed lower triangles for complex input a[batch, N, K] -> [batch, P, 2]."""
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.complex128).reshape(batch, N, K))
+    av = a.view(np.float64)
+    out = np.empty((batch, tri_size(N), 2), dtype=np.float64)
+    lib().oracle_herk_c128(_p(av, _f64p), N, K, batch, _p(out, _f64p))
+    return out
+
+
+def ref_cpu_herk(qc: np.ndarray, N: int, K: int, batch: int) -> np.ndarray:
+    """The reference's cpu_herk (compiled from its source) -> float64 [batch, P, 2]."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("reference host correlator not built (oracle/build_ref.sh)")
+    qc = np.ascontiguousarray(qc, dtype=np.uint8).reshape(-1)
+    out = np.empty((batch, tri_size(N), 2), dtype=np.float64)
+    L.ref_cpu_herk(_p(qc, _u8p), N, K, batch, _p(out, _f64p))
+    return out
+
+
+def num_threads() -> int:
+    return lib().oracle_num_threads()
+
+
+# ----------------------------------------------------------------- generators
+def gaussian_int4(rng: np.random.Generator, shape, sigma: float = 2.5):
+    """Re and Im each round(N(0, sigma^2)) clipped to [-7, 7] (int32 arrays)."""
+    re = np.clip(np.rint(rng.normal(0.0, sigma, size=shape)), -7, 7).astype(np.int32)
+    im = np.clip(np.rint(rng.normal(0.0, sigma, size=shape)), -7, 7).astype(np.int32)
+    return re, im
+
+
+def gaussian_qc(seed: int, batch: int, N: int, K: int, sigma: float = 2.5) -> np.ndarray:
+    """Seeded QC bytes [batch, N, K] with the Gaussian int4 distribution."""
+    rng = np.random.default_rng(seed)
+    re, im = gaussian_int4(rng, (batch, N, K), sigma)
+    return encode_qc(re, im)
