@@ -1,0 +1,469 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 correlator on the DSA-2000-scale workload.
+
+Workload (one step): 2048 antennas x 2 pol = 4096 inputs, 64 channels,
+K = 1024 time samples of QC int4 voltages (Re, Im each round(N(0, 2.5^2))
+clipped to [-7, 7], seeded, generated on the device), correlated to packed
+lower triangles of complex64 (8,390,656 entries per channel).  Metric:
+effective TFLOPS = sum_f 8 * N(N+1)/2 * K / t (the FLOP convention of the
+correlator's specification).
+
+Arms
+  (default)          the library through its C ABI, inputs resident in HBM;
+                     `e2e` repeats the step through the same C ABI with host
+                     buffers (pinned H2D of the QC input and D2H of every
+                     packed triangle inside the timed region, pipelined over
+                     channel chunks on two streams).
+  --impl reference   the reference's own host correlator (cpu_herk,
+                     cutlass_interface/test_herk_int4.cu:51-70, compiled from
+                     its source into oracle/_ref/) on all host threads, on a
+                     bounded sample of the same workload.
+
+Multi-GPU (torchrun): every rank correlates its own 64 channels (weak
+scaling, no collective on the data path); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "HERK eff. TFLOPS & % FP8/FP4 peak vs plain FP8 path, same B200, stated error"
+UNIT = "TFLOPS"
+NOMINAL_FP8_TFLOPS = 4500.0  # datasheet dense FP8 (context only)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--inputs", type=int, default=4096, help="N (antennas x pols)")
+    p.add_argument("--channels", type=int, default=64)
+    p.add_argument("--k", type=int, default=1024, help="time samples per channel")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-peak", action="store_true")
+    return p.parse_args()
+
+
+def herk_flops(N, K, B):
+    return 8.0 * (N * (N + 1) // 2) * K * B
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling around the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.t0 = time.time()
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(gpu_index), "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        self.marks = []
+
+    def mark(self):
+        self.marks.append(time.time())
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [ln.strip().split(", ") for ln in self.f if ln.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        # Samples are ~100 ms apart; keep the ones taken inside the timed window
+        # (estimated from sample order), else all samples under load.
+        n = len(rows)
+        t_end = time.time()
+        dt = (t_end - self.t0) / max(n, 1)
+        sel = rows
+        if len(self.marks) >= 2:
+            a, b = self.marks[0], self.marks[1]
+            idx = [k for k in range(n) if a - dt <= self.t0 + k * dt <= b + dt]
+            if idx:
+                sel = [rows[k] for k in idx]
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [v for v in (num(r[1]) for r in sel) if v is not None]
+        smax = [v for v in (num(r[2]) for r in sel) if v is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in sel for k in range(4) if "Active" in r[5 + k]
+                          and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(sel),
+                "power_w_max": max((num(r[3]) or 0.0) for r in sel)}
+
+
+# ------------------------------------------------------------------ inputs
+def make_qc(torch, B, N, K, device, seed=1):
+    """Seeded QC int4 voltages on the device: [B, N, K] uint8."""
+    g = torch.Generator(device=device).manual_seed(seed)
+    out = torch.empty(B, N, K, dtype=torch.uint8, device=device)
+    for b in range(B):  # per channel to bound temporary memory
+        re = torch.clamp(torch.round(torch.randn(N, K, device=device, generator=g) * 2.5), -7, 7)
+        im = torch.clamp(torch.round(torch.randn(N, K, device=device, generator=g) * 2.5), -7, 7)
+        re = re.to(torch.int32)
+        im = im.to(torch.int32)
+        nr = torch.where(re < 0, 8 | (-re), re)
+        ni = torch.where(im < 0, 8 | (-im), im)
+        out[b] = ((nr << 4) | ni).to(torch.uint8)
+    return out
+
+
+def measure_fp8_peak(torch, device):
+    """Dense FP8 E4M3 matmul throughput of cuBLASLt (torch._scaled_mm), 8192^3,
+    best of 20 back-to-back launches after warm-up: the FP8 roofline denominator."""
+    M = 8192
+    a = torch.randn(M, M, device=device).to(torch.float8_e4m3fn)
+    b = torch.randn(M, M, device=device).to(torch.float8_e4m3fn).t()
+    one = torch.tensor(1.0, device=device)
+    for _ in range(5):
+        torch._scaled_mm(a, b, scale_a=one, scale_b=one, out_dtype=torch.bfloat16)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(20):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch._scaled_mm(a, b, scale_a=one, scale_b=one, out_dtype=torch.bfloat16)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * M ** 3 / best / 1e9
+
+
+# ------------------------------------------------------------------ CPU baseline
+class CpuSample:
+    """The reference's cpu_herk (cutlass_interface/test_herk_int4.cu:51-70,
+    compiled from its source into oracle/_ref/) on all host threads, over the
+    first n inputs of one channel of the workload, n sized once so that one
+    run takes about `target_s`.  Falls back to the oracle port (kind "port")
+    when the reference was not built."""
+
+    def __init__(self, N, K, target_s):
+        import numpy as np
+        from oracle import oracle
+        self.oracle = oracle
+        self.kind = "reference" if oracle.ref_lib() is not None else "port"
+        self.N, self.K = N, K
+        self.rng = np.random.default_rng(5)
+        n = 256
+        dt = self._run(n)
+        while dt < target_s / 3 and n < N:
+            n = min(N, int(n * min(4.0, max(1.3, (target_s / max(dt, 1e-3)) ** 0.5))))
+            dt = self._run(n)
+        self.n = n
+        self.cores = (oracle.ref_lib().ref_num_threads() if self.kind == "reference"
+                      else oracle.num_threads())
+
+    def _run(self, n):
+        o = self.oracle
+        re, im = o.gaussian_int4(self.rng, (1, n, self.K))
+        qc = o.encode_qc(re, im)
+        t = time.perf_counter()
+        if self.kind == "reference":
+            o.ref_cpu_herk(qc, n, self.K, 1)
+        else:
+            o.herk_qc(qc, n, self.K, 1)
+        return time.perf_counter() - t
+
+    def tflops(self):
+        dt = self._run(self.n)
+        return herk_flops(self.n, self.K, 1) / dt / 1e12, dt
+
+    def describe(self, dt):
+        fl = herk_flops(self.n, self.K, 1)
+        return {"unit": UNIT, "cores": int(self.cores), "kind": self.kind,
+                "sample": f"one channel, first {self.n} of {self.N} inputs, K={self.K} "
+                          f"({fl / 1e9:.1f} GFLOP in {dt:.2f} s); FP64 complex cpu_herk, OpenMP "
+                          f"over rows"}
+
+
+def cpu_reference_sample(N, K, target_s=3.0):
+    cs = CpuSample(N, K, target_s)
+    v, dt = cs.tflops()
+    return {"value": v, **cs.describe(dt)}
+
+
+# ------------------------------------------------------------------ arms
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    from oracle import oracle
+    N, K = args.inputs, args.k
+    cs = CpuSample(N, K, target_s=2.0)
+    samples = []
+    dt = 0.0
+    for s_ in range(args.warmup + args.steps):
+        v_, dt = cs.tflops()
+        if s_ >= args.warmup:
+            samples.append(v_)
+    v = statistics.median(samples)
+    info = cs.describe(dt)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": herk_flops(N, K, args.channels) / (v * 1e12) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Gaussian int4, sigma 2.5)",
+            "config": {"workload": f"DSA-2000 correlator: {N} inputs x {args.channels} channels x "
+                                   f"K={K}, QC int4 -> packed complex triangle",
+                       "inputs": N, "channels": args.channels, "k": K},
+            "cpu_baseline": {"value": v, **info},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if oracle.ref_lib() is None:
+        line["note"] = "reference host code not built; timed the oracle port"
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    from ftd_b200 import Correlator, tri_size
+    from ftd_b200._lib import IN_INT4, OUT_FP32
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    N, K, B = args.inputs, args.k, args.channels
+    P = tri_size(N)
+    flops = herk_flops(N, K, B)
+
+    qc = make_qc(torch, B, N, K, dev, seed=1 + rank)
+    C = torch.empty(B, P, 2, dtype=torch.float32, device=dev)
+    corr = Correlator(device=local)
+    corr.init_herk(N, K, B)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        corr.herk(qc, C, N, K, B, input=IN_INT4, output=OUT_FP32, stream=stream, tune=False)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if corr.device_status() != 0:
+        raise RuntimeError("device wait timed out during warm-up")
+
+    clocks = ClockSampler(local)
+    time.sleep(0.3)
+    corr.set_profiling(True)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.mark()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks.mark()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    prof = corr.profile_read()
+    corr.set_profiling(False)
+    clk = clocks.stop()
+    if corr.device_status() != 0:
+        raise RuntimeError("device wait timed out in the timed region")
+
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = flops * world / (ms_max * 1e-3) / 1e12
+    herk_ms = prof["herk_ms"] / max(prof["herk_launches"], 1)
+    prep_ms = prof["prep_ms"] / max(prof["prep_launches"], 1)
+
+    # --- plain per-channel path: the same kernels, one launch pair per channel
+    plain = None
+    if not args.no_plain:
+        for _ in range(2):
+            for b in range(B):
+                corr.herk(qc[b], C[b], N, K, 1, input=IN_INT4, output=OUT_FP32, stream=stream,
+                          tune=False)
+        torch.cuda.synchronize()
+        reps = max(3, min(args.steps, 10))
+        e0.record(stream)
+        for _ in range(reps):
+            for b in range(B):
+                corr.herk(qc[b], C[b], N, K, 1, input=IN_INT4, output=OUT_FP32, stream=stream,
+                          tune=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pms = e0.elapsed_time(e1) / reps
+        plain = {"value": flops / (pms * 1e-3) / 1e12, "ms_per_step": pms,
+                 "what": f"{B} launches of batch=1 per step (same kernels, no cross-channel "
+                         f"persistence)"}
+
+    # --- end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(torch, args, dev, qc, N, K, B, flops, world, dist)
+
+    peak = None
+    if not args.no_peak:
+        peak = measure_fp8_peak(torch, dev)
+
+    if rank != 0:
+        return 0
+    achieved = flops / (herk_ms * 1e-3) / 1e12
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "herk_fp8_traffic.json")
+    if os.path.exists(tfile):
+        t = json.load(open(tfile))
+        if t.get("workload") == [N, K]:
+            traffic = t["bytes_per_channel"] * B
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp8_e4m3 (fp32 accumulate)",
+        "data": "synthetic (seeded Gaussian int4 voltages, sigma 2.5, generated on device)",
+        "config": {"workload": f"DSA-2000 correlator: {N} inputs x {B} channels x K={K}, "
+                               f"QC int4 -> packed complex64 lower triangle",
+                   "inputs": N, "channels": B, "k": K, "per_gpu_channels": B,
+                   "l2": "inputs (268 MB) and outputs (4.3 GB) exceed L2; no flush needed",
+                   "parallelism": f"replicas x{world} (independent channels)"},
+        "roofline": {"bound": "tensor", "achieved": achieved,
+                     "peak": peak, "unit": UNIT,
+                     "frac": (achieved / peak) if peak else None,
+                     "traffic": traffic,
+                     "kernel": "herk_fp8_tc_kernel",
+                     "kernel_ms": herk_ms,
+                     "peak_source": "cuBLASLt dense FP8 e4m3 GEMM 8192^3 (torch._scaled_mm), "
+                                    "measured in this run",
+                     "frac_of_nominal_4500": achieved / NOMINAL_FP8_TFLOPS},
+        "kernels": {"herk_fp8_tc_kernel_ms": herk_ms, "qc_to_z_kernel_ms": prep_ms},
+        "gpu_launches": prof["herk_launches"] + prof["prep_launches"],
+        "plain_per_channel": plain,
+        "speedup_vs_plain": (value / world / plain["value"]) if plain else None,
+        "e2e": e2e,
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_reference_sample(N, K, target_s=10.0)
+    print(json.dumps(line), flush=True)
+    corr.close()
+    return 0
+
+
+def run_e2e(torch, args, dev, qc_dev, N, K, B, flops, world, dist):
+    """Same workload through the C ABI with host buffers: each step copies the
+    QC input host->device and every packed triangle device->host (pinned
+    memory), pipelined over channel chunks on two streams."""
+    from ftd_b200 import Correlator, tri_size
+    from ftd_b200._lib import IN_INT4, OUT_FP32
+    P = tri_size(N)
+    chunk = 4
+    nchunks = (B + chunk - 1) // chunk
+    h_in = torch.empty(B, N, K, dtype=torch.uint8, pin_memory=True)
+    h_in.copy_(qc_dev.cpu())
+    h_out = torch.empty(B, P, 2, dtype=torch.float32, pin_memory=True)
+    streams = [torch.cuda.Stream(dev) for _ in range(2)]
+    corrs = [Correlator(device=dev.index) for _ in range(2)]
+    d_in = [torch.empty(chunk, N, K, dtype=torch.uint8, device=dev) for _ in range(2)]
+    d_out = [torch.empty(chunk, P, 2, dtype=torch.float32, device=dev) for _ in range(2)]
+    for c in corrs:
+        c.init_herk(N, K, chunk)
+
+    def step():
+        for ci in range(nchunks):
+            s = ci % 2
+            b0, b1 = ci * chunk, min(B, (ci + 1) * chunk)
+            n = b1 - b0
+            with torch.cuda.stream(streams[s]):
+                d_in[s][:n].copy_(h_in[b0:b1], non_blocking=True)
+                corrs[s].herk(d_in[s], d_out[s], N, K, n, input=IN_INT4, output=OUT_FP32,
+                              stream=streams[s], tune=False)
+                h_out[b0:b1].copy_(d_out[s][:n], non_blocking=True)
+
+    main = torch.cuda.current_stream(dev)
+    for _ in range(1):
+        step()
+    torch.cuda.synchronize()
+    steps = max(2, min(args.steps, 5))
+    if dist is not None:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(main)
+    for s in streams:
+        s.wait_event(e0)
+    for _ in range(steps):
+        step()
+    for s in streams:
+        main.wait_stream(s)
+    e1.record(main)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    for c in corrs:
+        c.close()
+    return {"value": flops * world / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms,
+            "h2d_bytes_per_step": int(B * N * K), "d2h_bytes_per_step": int(B * P * 8),
+            "steps": steps, "path": "C ABI (ftdx_herk) on pinned host buffers, 2 streams, "
+                                    f"{chunk}-channel chunks"}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    try:
+        return run_ours(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -51,6 +51,9 @@ PROTOTYPES = {
     "ftdx_init_herk": (_i, [_vp, _i, _i, _i, _vp]),
     "ftdx_end_herk": (_i, [_vp]),
     "ftdx_device_status": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32)]),
+    "ftdx_set_profiling": (_i, [_vp, _i]),
+    "ftdx_profile_read": (_i, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i),
+                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i)]),
 }
 
 _lib = None

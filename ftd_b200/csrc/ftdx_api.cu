@@ -61,6 +61,14 @@ struct ftdx_context {
   bool z_reserved = false;    // sized by ftdx_init_herk
   uint32_t* d_status = nullptr;
   std::map<std::tuple<int, int, int>, std::unique_ptr<Plan>> plans;  // (N, kblocks, batch)
+  // kernel timing (ftdx_set_profiling)
+  bool profiling = false;
+  struct Timed {
+    cudaEvent_t a, b;
+    int kind;  // 0 = herk, 1 = prep
+  };
+  std::vector<Timed> timed;
+  std::vector<cudaEvent_t> event_pool;
 };
 
 namespace {
@@ -125,7 +133,7 @@ ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t 
     return fail(h, FTDX_ERR_CAPACITY,
                 "tile plan for N=%d batch=%d built while capturing; call ftdx_init_herk first", N,
                 batch);
-  const int nb = (N + ftdx::kBlockI - 1) / ftdx::kBlockI;
+  const int nb = (N + ftdx::kTile - 1) / ftdx::kTile;
   std::vector<ChanDesc> chans(batch);
   std::vector<TileDesc> tiles;
   tiles.reserve(size_t(batch) * nb * (nb + 1) / 2);
@@ -155,36 +163,56 @@ ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t 
   return FTDX_OK;
 }
 
-// Tensor maps over the operand Z ([rows2][zpitch] bytes):
-//   tmZ: every row (x and y), box 128 B x 256 rows
-//   tmX: even rows only (row stride 2*zpitch), box 128 B x 128 rows
-ftdx_status encode_maps(ftdx_handle h, uint8_t* z, int64_t ant_rows, int64_t zpitch,
-                        CUtensorMap* tmX, CUtensorMap* tmZ) {
+// Tensor map over the operand planes Z[2][rows][Kp] (bytes): box of
+// 128 samples x 128 rows x 1 plane, 128-byte swizzle.
+ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t Kp,
+                              CUtensorMap* tm) {
   auto enc = get_encode_fn();
   if (!enc) return fail(h, FTDX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-  const cuuint32_t estr[2] = {1, 1};
-  {
-    const cuuint64_t dims[2] = {cuuint64_t(zpitch), cuuint64_t(2 * ant_rows)};
-    const cuuint64_t strides[1] = {cuuint64_t(zpitch)};
-    const cuuint32_t box[2] = {cuuint32_t(ftdx::kKBytes), cuuint32_t(ftdx::kUmmaN)};
-    CUresult r = enc(tmZ, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, z, dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return fail(h, FTDX_ERR_CUDA, "tensor map (Z) encode failed: %d", r);
-  }
-  {
-    const cuuint64_t dims[2] = {cuuint64_t(zpitch), cuuint64_t(ant_rows)};
-    const cuuint64_t strides[1] = {cuuint64_t(2 * zpitch)};
-    const cuuint32_t box[2] = {cuuint32_t(ftdx::kKBytes), cuuint32_t(ftdx::kBlockJ)};
-    CUresult r = enc(tmX, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, z, dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return fail(h, FTDX_ERR_CUDA, "tensor map (X) encode failed: %d", r);
-  }
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const cuuint64_t dims[3] = {cuuint64_t(Kp), cuuint64_t(rows), 2};
+  const cuuint64_t strides[2] = {cuuint64_t(Kp), cuuint64_t(rows * Kp)};
+  const cuuint32_t box[3] = {cuuint32_t(ftdx::kStageK), cuuint32_t(ftdx::kTile), 1};
+  CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, z, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(h, FTDX_ERR_CUDA, "tensor map encode failed: %d", int(r));
   return FTDX_OK;
 }
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+cudaEvent_t pool_event(ftdx_handle h) {
+  if (!h->event_pool.empty()) {
+    cudaEvent_t e = h->event_pool.back();
+    h->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Records an event pair around one kernel launch when profiling is on.
+struct ScopedTimer {
+  ftdx_handle h;
+  cudaStream_t s;
+  int kind;
+  cudaEvent_t a = nullptr;
+  ScopedTimer(ftdx_handle h_, cudaStream_t s_, int kind_) : h(h_), s(s_), kind(kind_) {
+    if (h->profiling) {
+      a = pool_event(h);
+      cudaEventRecord(a, s);
+    }
+  }
+  ~ScopedTimer() {
+    if (a) {
+      cudaEvent_t b = pool_event(h);
+      cudaEventRecord(b, s);
+      h->timed.push_back({a, b, kind});
+    }
+  }
+};
 
 }  // namespace
 
@@ -246,6 +274,11 @@ ftdx_status ftdx_destroy(ftdx_handle h) {
   cudaSetDevice(h->device);
   cudaDeviceSynchronize();
   h->plans.clear();
+  for (auto& t : h->timed) {
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  for (auto e : h->event_pool) cudaEventDestroy(e);
   if (h->z) cudaFree(h->z);
   if (h->d_status) cudaFree(h->d_status);
   delete h;
@@ -259,12 +292,12 @@ ftdx_status ftdx_init_herk(ftdx_handle h, int N, int K, int batch, void* stream)
   if (N < 1 || K < 1 || batch < 1) return fail(h, FTDX_ERR_INVALID_ARG, "init_herk: bad sizes");
   cudaSetDevice(h->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int64_t Kp = round_up(K, ftdx::kSamplesPerStage);
-  ftdx_status st = ensure_workspace(h, size_t(2) * N * batch * (2 * Kp), s);
+  const int64_t Kp = round_up(K, ftdx::kStageK);
+  ftdx_status st = ensure_workspace(h, size_t(2) * N * batch * Kp, s);
   if (st != FTDX_OK) return st;
   h->z_reserved = true;
   const Plan* p = nullptr;
-  return get_plan(h, N, int(Kp / ftdx::kSamplesPerStage), batch, s, &p);
+  return get_plan(h, N, int(Kp / ftdx::kStageK), batch, s, &p);
 }
 
 ftdx_status ftdx_end_herk(ftdx_handle h) {
@@ -302,32 +335,33 @@ ftdx_status ftdx_herk(ftdx_handle h, const void* A, void* C, int N, int K, int b
   if (input == FTDX_IN_FP16 && (reinterpret_cast<uintptr_t>(A) & 3) != 0)
     return fail(h, FTDX_ERR_INVALID_ARG, "herk: FP16 A must be 4-byte aligned");
   // Row coordinates of the TMA boxes are 32-bit.
-  if (int64_t(N) * batch * 2 + 512 > (int64_t(1) << 31))
+  if (int64_t(N) * batch + 256 > (int64_t(1) << 31))
     return fail(h, FTDX_ERR_INVALID_ARG, "herk: N*batch too large for one call");
-  if (N > 65535 * ftdx::kBlockI)
+  if (N > 65535 * ftdx::kTile)
     return fail(h, FTDX_ERR_INVALID_ARG, "herk: N too large");
 
   cudaError_t e = cudaSetDevice(h->device);
   if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int64_t Kp = round_up(K, ftdx::kSamplesPerStage);
-  const int64_t zpitch = 2 * Kp;
+  const int64_t Kp = round_up(K, ftdx::kStageK);
   const int64_t rows = int64_t(N) * batch;
-  ftdx_status st = ensure_workspace(h, size_t(2 * rows * zpitch), s);
+  ftdx_status st = ensure_workspace(h, size_t(2 * rows * Kp), s);
   if (st != FTDX_OK) return st;
   const Plan* plan = nullptr;
-  st = get_plan(h, N, int(Kp / ftdx::kSamplesPerStage), batch, s, &plan);
+  st = get_plan(h, N, int(Kp / ftdx::kStageK), batch, s, &plan);
   if (st != FTDX_OK) return st;
 
-  if (input == FTDX_IN_INT4)
-    e = ftdx::launch_qc_to_z(static_cast<const uint8_t*>(A), h->z, rows, K, int(Kp), h->sm_count,
-                             s);
-  else
-    e = ftdx::launch_fp16_to_z(A, h->z, rows, K, int(Kp), h->sm_count, s);
+  {
+    ScopedTimer tm(h, s, 1);
+    if (input == FTDX_IN_INT4)
+      e = ftdx::launch_qc_to_planes(static_cast<const uint8_t*>(A), h->z, rows, K, int(Kp), s);
+    else
+      e = ftdx::launch_fp16_to_planes(A, h->z, rows, K, int(Kp), s);
+  }
   if (e != cudaSuccess) return cuda_fail(h, e, "operand promotion launch");
 
-  CUtensorMap tmX, tmZ;
-  st = encode_maps(h, h->z, rows, zpitch, &tmX, &tmZ);
+  CUtensorMap tmZ;
+  st = encode_planes_map(h, h->z, rows, Kp, &tmZ);
   if (st != FTDX_OK) return st;
   ftdx::HerkArgs args;
   args.tiles = plan->d_tiles;
@@ -339,7 +373,10 @@ ftdx_status ftdx_herk(ftdx_handle h, const void* A, void* C, int N, int K, int b
   args.beta = beta;
   args.status = h->d_status;
   const int grid = plan->num_tiles < h->sm_count ? plan->num_tiles : h->sm_count;
-  e = ftdx::launch_herk_fp8(tmX, tmZ, args, grid, s);
+  {
+    ScopedTimer tm(h, s, 0);
+    e = ftdx::launch_herk_fp8(tmZ, args, grid, s);
+  }
   if (e != cudaSuccess) return cuda_fail(h, e, "HERK kernel launch");
   return FTDX_OK;
 }
@@ -357,6 +394,37 @@ ftdx_status ftdx_device_status(ftdx_handle h, void* stream, uint32_t* bits) {
   if (bits) *bits = v;
   if (v) return fail(h, FTDX_ERR_TIMEOUT, "device status 0x%x", v);
   return FTDX_OK;
+}
+
+ftdx_status ftdx_set_profiling(ftdx_handle h, int enable) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  h->profiling = enable != 0;
+  return FTDX_OK;
+}
+
+ftdx_status ftdx_profile_read(ftdx_handle h, double* herk_ms, int* herk_launches, double* prep_ms,
+                              int* prep_launches) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  cudaSetDevice(h->device);
+  double ms[2] = {0, 0};
+  int n[2] = {0, 0};
+  ftdx_status st = FTDX_OK;
+  for (auto& t : h->timed) {
+    float v = 0.f;
+    cudaError_t e = cudaEventSynchronize(t.b);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&v, t.a, t.b);
+    if (e != cudaSuccess) st = cuda_fail(h, e, "profile event");
+    ms[t.kind] += v;
+    n[t.kind] += 1;
+    h->event_pool.push_back(t.a);
+    h->event_pool.push_back(t.b);
+  }
+  h->timed.clear();
+  if (herk_ms) *herk_ms = ms[0];
+  if (herk_launches) *herk_launches = n[0];
+  if (prep_ms) *prep_ms = ms[1];
+  if (prep_launches) *prep_launches = n[1];
+  return st;
 }
 
 }  // extern "C"

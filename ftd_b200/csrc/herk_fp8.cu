@@ -1,17 +1,18 @@
 // herk_fp8.cu -- B200 (sm_100a) correlator kernels.
 //
-//  * qc_to_z_kernel / fp16_to_z_kernel: promote QC int4 (or interleaved FP16)
-//    voltages to the FP8 E4M3 operand Z (x rows and conjugate-permuted y
-//    rows), zero-padding K to a multiple of 64.  Replaces the reference's
+//  * qc_to_planes_kernel / fp16_to_planes_kernel: promote QC int4 (or
+//    interleaved FP16) voltages to the FP8 E4M3 operand planes Z[Re|Im],
+//    zero-padding K to a multiple of 128.  Replaces the reference's
 //    cast_int4_to_fp8_interleaved (cutlass_interface/cutlass_gemm_api.cu:1566-1623).
 //  * herk_fp8_tc_kernel: persistent, warp-specialised tcgen05 HERK.  Each CTA
 //    walks a list of lower-triangle tiles (128 column antennas j x 128 row
-//    antennas i).  TMA feeds a 4-stage shared-memory ring; one thread issues
-//    tcgen05.mma kind::f8f6f4 (M=128 x N=256 x K=32) into one of two TMEM
-//    accumulators; four epilogue warps drain the other accumulator with
+//    antennas i).  TMA feeds a 3-stage ring of four 128 x 128-byte planes
+//    (Re_j, Im_j, Re_i, Im_i); one thread issues four tcgen05.mma kind::f8f6f4
+//    (M = N = 128, K = 32) per k-step into a Re and an Im accumulator in TMEM
+//    (double-buffered); four epilogue warps drain the other accumulator with
 //    tcgen05.ld and store the packed lower triangle directly.  TMEM lane j
-//    holds (Re, Im) of R_ij in columns (2i, 2i+1), so a warp's 32 lanes write
-//    32 consecutive packed elements of one triangle row per store.
+//    holds R_ij for consecutive i in consecutive columns, so a warp's 32
+//    lanes write 32 consecutive packed elements of one triangle row per store.
 //    Replaces herk_direct_fp8_* (cutlass_interface/shared/herk_kernel_common.hpp:175-2768)
 //    and the CUTLASS baseline + pack kernels
 //    (cutlass_interface/gemm_complex_sm100/api_impl.hpp:1462-1745).
@@ -40,28 +41,21 @@ __device__ __forceinline__ void qc4_to_e4m3(uint32_t w, uint32_t& re, uint32_t& 
   im = __byte_perm(kLo, kHi, si) | ((w << 4) & 0x80808080u);
 }
 
-// Interleave: x = (re0, im0, re1, im1, ...), y = (im0, -re0, im1, -re1, ...).
-__device__ __forceinline__ void make_xy(uint32_t re, uint32_t im, uint32_t& x0, uint32_t& x1,
-                                        uint32_t& y0, uint32_t& y1) {
-  const uint32_t nre = re ^ 0x80808080u;
-  x0 = __byte_perm(re, im, 0x5140);
-  x1 = __byte_perm(re, im, 0x7362);
-  y0 = __byte_perm(im, nre, 0x5140);
-  y1 = __byte_perm(im, nre, 0x7362);
-}
-
-// One thread converts 16 samples of one antenna row.
-__global__ void __launch_bounds__(256) qc_to_z_kernel(const uint8_t* __restrict__ qc,
-                                                      uint8_t* __restrict__ z, int64_t rows,
-                                                      int K, int Kp) {
+// One thread converts 16 samples of one antenna row.  Each block owns
+// `rows_per_block` consecutive rows so that all index math is 32-bit.
+__global__ void __launch_bounds__(256) qc_to_planes_kernel(const uint8_t* __restrict__ qc,
+                                                           uint8_t* __restrict__ z, int64_t rows,
+                                                           int K, int Kp, int rows_per_block) {
   const int chunks = Kp >> 4;
-  const int64_t total = rows * chunks;
-  const int64_t zpitch = 2 * int64_t(Kp);
+  const int64_t r0 = int64_t(blockIdx.x) * rows_per_block;
+  const int64_t nrows64 = rows - r0 < rows_per_block ? rows - r0 : rows_per_block;
+  const int nloc = int(nrows64) * chunks;
+  const int64_t plane = rows * int64_t(Kp);
   const bool vec = ((K & 15) == 0) && ((reinterpret_cast<uintptr_t>(qc) & 15) == 0);
-  for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
-       idx += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t r = idx / chunks;
-    const int t0 = int(idx - r * chunks) << 4;
+  for (int l = threadIdx.x; l < nloc; l += blockDim.x) {
+    const int rl = l / chunks;
+    const int t0 = (l - rl * chunks) << 4;
+    const int64_t r = r0 + rl;
     const uint8_t* src = qc + r * K + t0;
     uint32_t w[4];
     if (vec && t0 + 16 <= K) {
@@ -80,59 +74,52 @@ __global__ void __launch_bounds__(256) qc_to_z_kernel(const uint8_t* __restrict_
         w[q] = acc;
       }
     }
-    uint32_t x[8], y[8];
+    uint32_t re[4], im[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      uint32_t re, im;
-      qc4_to_e4m3(w[q], re, im);
-      make_xy(re, im, x[2 * q], x[2 * q + 1], y[2 * q], y[2 * q + 1]);
-    }
-    uint4* dx = reinterpret_cast<uint4*>(z + (2 * r) * zpitch + 2 * t0);
-    uint4* dy = reinterpret_cast<uint4*>(z + (2 * r + 1) * zpitch + 2 * t0);
-    dx[0] = make_uint4(x[0], x[1], x[2], x[3]);
-    dx[1] = make_uint4(x[4], x[5], x[6], x[7]);
-    dy[0] = make_uint4(y[0], y[1], y[2], y[3]);
-    dy[1] = make_uint4(y[4], y[5], y[6], y[7]);
+    for (int q = 0; q < 4; ++q) qc4_to_e4m3(w[q], re[q], im[q]);
+    uint8_t* dst = z + r * Kp + t0;
+    *reinterpret_cast<uint4*>(dst) = make_uint4(re[0], re[1], re[2], re[3]);
+    *reinterpret_cast<uint4*>(dst + plane) = make_uint4(im[0], im[1], im[2], im[3]);
   }
 }
 
-// Interleaved FP16 complex [rows][K][2] -> Z.  FP16 -> E4M3 rounds to nearest
-// and saturates at +-448 with no scaling, as the reference's FP16 -> FP8 cast
-// (cutlass_interface/shared/cast_kernels_common.hpp:34-37).
+// Interleaved FP16 complex [rows][K][2] -> Z planes.  FP16 -> E4M3 rounds to
+// nearest and saturates at +-448 with no scaling, as the reference's FP16 ->
+// FP8 cast (cutlass_interface/shared/cast_kernels_common.hpp:34-37).
 __device__ __forceinline__ uint32_t h2_to_e4m3x2(__half2 h) {
   return uint32_t(__nv_cvt_halfraw2_to_fp8x2(static_cast<__half2_raw>(h), __NV_SATFINITE,
                                              __NV_E4M3));
 }
 
-__global__ void __launch_bounds__(256) fp16_to_z_kernel(const __half2* __restrict__ a,
-                                                        uint8_t* __restrict__ z, int64_t rows,
-                                                        int K, int Kp) {
+__global__ void __launch_bounds__(256) fp16_to_planes_kernel(const __half2* __restrict__ a,
+                                                             uint8_t* __restrict__ z, int64_t rows,
+                                                             int K, int Kp, int rows_per_block) {
   const int chunks = Kp >> 3;  // 8 samples per thread
-  const int64_t total = rows * chunks;
-  const int64_t zpitch = 2 * int64_t(Kp);
-  for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
-       idx += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t r = idx / chunks;
-    const int t0 = int(idx - r * chunks) << 3;
-    uint32_t x[4], y[4];
+  const int64_t r0 = int64_t(blockIdx.x) * rows_per_block;
+  const int64_t nrows64 = rows - r0 < rows_per_block ? rows - r0 : rows_per_block;
+  const int nloc = int(nrows64) * chunks;
+  const int64_t plane = rows * int64_t(Kp);
+  for (int l = threadIdx.x; l < nloc; l += blockDim.x) {
+    const int rl = l / chunks;
+    const int t0 = (l - rl * chunks) << 3;
+    const int64_t r = r0 + rl;
+    uint32_t re[2], im[2];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      uint32_t pr[2];
+    for (int q = 0; q < 2; ++q) {
+      uint32_t pr[4];
 #pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        const int t = t0 + 2 * q + b;
-        __half2 h = (t < K) ? a[r * K + t] : __floats2half2_rn(0.f, 0.f);
-        pr[b] = h2_to_e4m3x2(h);  // low byte Re, high byte Im
+      for (int b = 0; b < 4; ++b) {
+        const int t = t0 + 4 * q + b;
+        const __half2 h = (t < K) ? a[r * K + t] : __floats2half2_rn(0.f, 0.f);
+        pr[b] = h2_to_e4m3x2(h);  // byte 0 Re, byte 1 Im
       }
-      x[q] = pr[0] | (pr[1] << 16);
-      // y = (im, -re) per sample
-      const uint32_t y0 = ((pr[0] >> 8) & 0xFFu) | (((pr[0] & 0xFFu) ^ 0x80u) << 8);
-      const uint32_t y1 = ((pr[1] >> 8) & 0xFFu) | (((pr[1] & 0xFFu) ^ 0x80u) << 8);
-      y[q] = y0 | (y1 << 16);
+      const uint32_t lo = pr[0] | (pr[1] << 16), hi = pr[2] | (pr[3] << 16);
+      re[q] = __byte_perm(lo, hi, 0x6420);
+      im[q] = __byte_perm(lo, hi, 0x7531);
     }
-    *reinterpret_cast<uint4*>(z + (2 * r) * zpitch + 2 * t0) = make_uint4(x[0], x[1], x[2], x[3]);
-    *reinterpret_cast<uint4*>(z + (2 * r + 1) * zpitch + 2 * t0) =
-        make_uint4(y[0], y[1], y[2], y[3]);
+    uint8_t* dst = z + r * Kp + t0;
+    *reinterpret_cast<uint2*>(dst) = make_uint2(re[0], re[1]);
+    *reinterpret_cast<uint2*>(dst + plane) = make_uint2(im[0], im[1]);
   }
 }
 
@@ -160,24 +147,26 @@ __device__ __forceinline__ void store_elem(__half* out, int64_t idx, float re, f
 
 template <typename OutT>
 __global__ void __launch_bounds__(kHerkThreads, 1)
-    herk_fp8_tc_kernel(const __grid_constant__ CUtensorMap tmX,
-                       const __grid_constant__ CUtensorMap tmZ, const HerkArgs args) {
+    herk_fp8_tc_kernel(const __grid_constant__ CUtensorMap tmZ, const HerkArgs args) {
   extern __shared__ uint8_t smem_dyn[];
   // 128 B swizzled operand tiles must start on 1024 B boundaries of the
   // shared window.
   uint8_t* smem = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
-  uint8_t* sA = smem;
-  uint8_t* sB = smem + kStages * kABytes;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 5);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
+  const uint32_t smem0 = smem_u32(smem);
   const uint32_t bar0 = smem_u32(bars);
   auto full_bar = [&](int s) { return bar0 + 8u * s; };
   auto empty_bar = [&](int s) { return bar0 + 8u * (kStages + s); };
   auto tfull_bar = [&](int b) { return bar0 + 8u * (2 * kStages + b); };
   auto tempty_bar = [&](int b) { return bar0 + 8u * (2 * kStages + 2 + b); };
   const uint32_t done_bar = bar0 + 8u * (2 * kStages + 4);
+  // plane p of stage s: 0 = Re_j, 1 = Im_j, 2 = Re_i, 3 = Im_i
+  auto plane_addr = [&](int s, int p) {
+    return smem0 + uint32_t(s * kStageBytes + p * kPlaneBytes);
+  };
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -195,10 +184,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
     *abort_flag = 0;
     fence_mbar_init();
   }
-  if (warp == 0 && lane == 0) {
-    tma_prefetch_desc(&tmX);
-    tma_prefetch_desc(&tmZ);
-  }
+  if (warp == 0 && lane == 0) tma_prefetch_desc(&tmZ);
   if (warp == 1) {
     tmem_alloc(smem_u32(tmem_slot), 2 * kAccCols);
     tmem_relinquish();
@@ -218,17 +204,23 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
         const TileDesc td = args.tiles[t];
         const ChanDesc cd = args.chans[td.ch];
-        const int32_t rowJ = int32_t(cd.row0 + int64_t(td.tj) * kBlockJ);
-        const int32_t rowZ = int32_t(2 * (cd.row0 + int64_t(td.ti) * kBlockI));
+        const int32_t rowJ = int32_t(cd.row0 + int64_t(td.tj) * kTile);
+        const int32_t rowI = int32_t(cd.row0 + int64_t(td.ti) * kTile);
+        const bool diag = td.ti == td.tj;  // i block == j block: load it once
         for (int kb = 0; kb < cd.kblocks; ++kb) {
           if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
             atomicOr(args.status, kStatusTimeoutProducer);
             ok = false;
             break;
           }
-          mbar_arrive_expect_tx(full_bar(stage), kStageBytes);
-          tma_load_2d(smem_u32(sA + stage * kABytes), &tmX, kb * kKBytes, rowJ, full_bar(stage));
-          tma_load_2d(smem_u32(sB + stage * kBBytes), &tmZ, kb * kKBytes, rowZ, full_bar(stage));
+          const int32_t k0 = kb * kStageK;
+          mbar_arrive_expect_tx(full_bar(stage), diag ? 2 * kPlaneBytes : kStageBytes);
+          tma_load_3d(plane_addr(stage, 0), &tmZ, k0, rowJ, 0, full_bar(stage));
+          tma_load_3d(plane_addr(stage, 1), &tmZ, k0, rowJ, 1, full_bar(stage));
+          if (!diag) {
+            tma_load_3d(plane_addr(stage, 2), &tmZ, k0, rowI, 0, full_bar(stage));
+            tma_load_3d(plane_addr(stage, 3), &tmZ, k0, rowI, 1, full_bar(stage));
+          }
           ++issued;
           if (++stage == kStages) {
             stage = 0;
@@ -246,27 +238,31 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
             ph ^= 1u;
           }
           volatile int never = 0;
-          mbar_wait(full_bar(s), ph, &never);
+          if (!mbar_wait(full_bar(s), ph, &never)) atomicOr(args.status, kStatusTimeoutOther);
         }
       }
     }
   } else if (warp == 1) {
     // ------------------------------------------------ MMA issuer
     if (lane == 0) {
-      constexpr uint32_t idesc = idesc_f32acc(0, 0, kBlockJ, kUmmaN);
+      constexpr uint32_t idesc = idesc_f32acc(0, 0, kTile, kTile);
+      constexpr uint32_t idesc_neg = idesc_f32acc(0, 0, kTile, kTile, 1);
       int stage = 0;
       uint32_t phase = 0;
       int acc = 0;
       uint32_t acc_phase = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
-        const ChanDesc cd = args.chans[args.tiles[t].ch];
+        const TileDesc td = args.tiles[t];
+        const ChanDesc cd = args.chans[td.ch];
+        const int pb = (td.ti == td.tj) ? 0 : 2;  // planes holding the i block
         if (!mbar_wait(tempty_bar(acc), acc_phase ^ 1u, abort_flag)) {
           atomicOr(args.status, kStatusTimeoutMma);
           break;
         }
         tc_fence_after();
-        const uint32_t d_tmem = tmem_base + uint32_t(acc * kAccCols);
+        const uint32_t d_re = tmem_base + uint32_t(acc * kAccCols);
+        const uint32_t d_im = d_re + uint32_t(kTile);
         for (int kb = 0; kb < cd.kblocks; ++kb) {
           if (!mbar_wait(full_bar(stage), phase, abort_flag)) {
             atomicOr(args.status, kStatusTimeoutMma);
@@ -274,12 +270,19 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
             break;
           }
           tc_fence_after();
-          const uint32_t a0 = smem_u32(sA + stage * kABytes);
-          const uint32_t b0 = smem_u32(sB + stage * kBBytes);
+          const uint32_t are = plane_addr(stage, 0), aim = plane_addr(stage, 1);
+          const uint32_t bre = plane_addr(stage, pb), bim = plane_addr(stage, pb + 1);
 #pragma unroll
-          for (int s = 0; s < kKBytes / 32; ++s) {
-            mma_f8f6f4(d_tmem, sdesc_sw128_kmajor(a0 + 32 * s), sdesc_sw128_kmajor(b0 + 32 * s),
-                       idesc, (kb | s) != 0);
+          for (int s = 0; s < kStageK / 32; ++s) {
+            const uint64_t dare = sdesc_sw128_kmajor(are + 32 * s);
+            const uint64_t daim = sdesc_sw128_kmajor(aim + 32 * s);
+            const uint64_t dbre = sdesc_sw128_kmajor(bre + 32 * s);
+            const uint64_t dbim = sdesc_sw128_kmajor(bim + 32 * s);
+            const uint32_t first = (kb | s) != 0;
+            mma_f8f6f4(d_re, dare, dbre, idesc, first);     // Re += Re_j Re_i
+            mma_f8f6f4(d_im, dare, dbim, idesc, first);     // Im += Re_j Im_i
+            mma_f8f6f4(d_re, daim, dbim, idesc, 1);         // Re += Im_j Im_i
+            mma_f8f6f4(d_im, daim, dbre, idesc_neg, 1);     // Im -= Im_j Re_i
           }
           mma_commit(empty_bar(stage));
           if (++stage == kStages) {
@@ -297,7 +300,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       // No MMA may still be writing TMEM when it is released.
       mma_commit(done_bar);
       volatile int never = 0;
-      mbar_wait(done_bar, 0, &never);
+      if (!mbar_wait(done_bar, 0, &never)) atomicOr(args.status, kStatusTimeoutOther);
     }
   } else {
     // ------------------------------------------------ epilogue (warps 2..5)
@@ -315,26 +318,29 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       }
       tc_fence_after();
       const int n = cd.n;
-      const int jw = int(td.tj) * kBlockJ + q * 32;  // first column of this warp
+      const int jw = int(td.tj) * kTile + q * 32;  // first column of this warp
       const int j = jw + lane;
-      const int ib = int(td.ti) * kBlockI;
+      const int ib = int(td.ti) * kTile;
       OutT* outc = out + 2 * cd.out0;
       const uint32_t tb = tmem_base + (uint32_t(q * 32) << 16) + uint32_t(acc * kAccCols);
 #pragma unroll 1
-      for (int c = 0; c < kUmmaN / 32; ++c) {
-        const int i0 = ib + 16 * c;
-        if (i0 + 15 < jw || i0 >= n) continue;  // warp-uniform: nothing to store
-        uint32_t r[32];
+      for (int c = 0; c < kTile / 32; ++c) {
+        const int i0 = ib + 32 * c;
+        if (i0 + 31 < jw || i0 >= n) continue;  // warp-uniform: nothing to store
+        uint32_t re[32], im[32];
         __syncwarp();
-        tmem_ld_32x32b_x32(tb + 32u * c, r);
+        tmem_ld_32x32b_x32(tb + 32u * c, re);
+        tmem_ld_32x32b_x32(tb + uint32_t(kTile) + 32u * c, im);
         tmem_wait_ld();
+        if (j < n) {
 #pragma unroll
-        for (int m = 0; m < 16; ++m) {
-          const int i = i0 + m;
-          if (i < n && j <= i) {
-            float re = __uint_as_float(r[2 * m]) * args.alpha;
-            float im = (i == j) ? 0.f : __uint_as_float(r[2 * m + 1]) * args.alpha;
-            store_elem(outc, int64_t(i) * (i + 1) / 2 + j, re, im, args.beta);
+          for (int m = 0; m < 32; ++m) {
+            const int i = i0 + m;
+            if (i < n && j <= i) {
+              const float vr = __uint_as_float(re[m]) * args.alpha;
+              const float vi = (i == j) ? 0.f : __uint_as_float(im[m]) * args.alpha;
+              store_elem(outc, int64_t(i) * (i + 1) / 2 + j, vr, vi, args.beta);
+            }
           }
         }
       }
@@ -358,52 +364,45 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
 }
 
 // ------------------------------------------------------------------ launchers
-static int grid_for(int64_t work, int threads, int sm_count) {
-  int64_t blocks = (work + threads - 1) / threads;
-  const int64_t cap = int64_t(sm_count) * 8;
-  if (blocks > cap) blocks = cap;
-  if (blocks < 1) blocks = 1;
-  return int(blocks);
+static int rows_per_block(int chunks) {
+  int r = 8192 / (chunks > 0 ? chunks : 1);
+  return r < 1 ? 1 : r;
 }
 
-cudaError_t launch_qc_to_z(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
-                           int sm_count, cudaStream_t s) {
-  const int64_t work = rows * (Kp >> 4);
-  qc_to_z_kernel<<<grid_for(work, 256, sm_count), 256, 0, s>>>(qc, z, rows, K, Kp);
+cudaError_t launch_qc_to_planes(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
+                                cudaStream_t s) {
+  const int rpb = rows_per_block(Kp >> 4);
+  const int64_t blocks = (rows + rpb - 1) / rpb;
+  qc_to_planes_kernel<<<unsigned(blocks), 256, 0, s>>>(qc, z, rows, K, Kp, rpb);
   return cudaGetLastError();
 }
 
-cudaError_t launch_fp16_to_z(const void* a16, uint8_t* z, int64_t rows, int K, int Kp,
-                             int sm_count, cudaStream_t s) {
-  const int64_t work = rows * (Kp >> 3);
-  fp16_to_z_kernel<<<grid_for(work, 256, sm_count), 256, 0, s>>>(
-      static_cast<const __half2*>(a16), z, rows, K, Kp);
+cudaError_t launch_fp16_to_planes(const void* a16, uint8_t* z, int64_t rows, int K, int Kp,
+                                  cudaStream_t s) {
+  const int rpb = rows_per_block(Kp >> 3);
+  const int64_t blocks = (rows + rpb - 1) / rpb;
+  fp16_to_planes_kernel<<<unsigned(blocks), 256, 0, s>>>(static_cast<const __half2*>(a16), z,
+                                                         rows, K, Kp, rpb);
   return cudaGetLastError();
 }
 
-cudaError_t launch_herk_fp8(const CUtensorMap& tmX, const CUtensorMap& tmZ, const HerkArgs& a,
-                            int grid, cudaStream_t s) {
-  static bool attr_done[2] = {false, false};
-  if (a.out_fp16) {
-    if (!attr_done[1]) {
-      cudaError_t e = cudaFuncSetAttribute(herk_fp8_tc_kernel<__half>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           int(kHerkSmem));
-      if (e != cudaSuccess) return e;
-      attr_done[1] = true;
-    }
-    herk_fp8_tc_kernel<__half><<<grid, kHerkThreads, kHerkSmem, s>>>(tmX, tmZ, a);
-  } else {
-    if (!attr_done[0]) {
-      cudaError_t e = cudaFuncSetAttribute(herk_fp8_tc_kernel<float>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           int(kHerkSmem));
-      if (e != cudaSuccess) return e;
-      attr_done[0] = true;
-    }
-    herk_fp8_tc_kernel<float><<<grid, kHerkThreads, kHerkSmem, s>>>(tmX, tmZ, a);
+template <typename OutT>
+static cudaError_t launch_herk_t(const CUtensorMap& tmZ, const HerkArgs& a, int grid,
+                                 cudaStream_t s) {
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(herk_fp8_tc_kernel<OutT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(kHerkSmem));
+    if (e != cudaSuccess) return e;
+    attr_done = true;
   }
+  herk_fp8_tc_kernel<OutT><<<grid, kHerkThreads, kHerkSmem, s>>>(tmZ, a);
   return cudaGetLastError();
+}
+
+cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s) {
+  return a.out_fp16 ? launch_herk_t<__half>(tmZ, a, grid, s) : launch_herk_t<float>(tmZ, a, grid, s);
 }
 
 }  // namespace ftdx

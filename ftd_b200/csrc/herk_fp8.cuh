@@ -1,16 +1,20 @@
 // herk_fp8.cuh -- shared declarations of the correlator (HERK) kernels.
 //
-// Data layout in HBM (per channel c, N_c antennas, K_c time samples):
+// Data layout in HBM (per channel c, N_c inputs, K_c time samples):
 //   QC input   : [N_c][K_c] bytes, one complex sample per byte, high nibble =
 //                Re, low nibble = Im, each sign-magnitude in [-7, 7]
 //                (the reference's QC format, cutlass_interface/test_herk_int4.cu:41-45).
-//   operand Z  : [2*N_c][zpitch] FP8 E4M3 bytes, zpitch = 2*Kp, Kp = K rounded
-//                up to 64.  Row 2a is x_a = (re_t, im_t)_t and row 2a+1 is
-//                y_a = (im_t, -re_t)_t, so that x_j . x_a = Re R_aj and
-//                x_j . y_a = Im R_aj (the conjugate-permutation identity of
-//                cutlass_interface/shared/herk_kernel_common.hpp:8-13).
+//   operand Z  : two FP8 E4M3 planes, Z[p][row][Kp], p = 0 holds Re, p = 1
+//                holds Im, Kp = K rounded up to 128 and zero-padded.  Rows of
+//                all channels are stacked (channel c starts at row0_c).
 //   output     : packed lower triangle, row-major, element (i, j <= i) at
 //                i(i+1)/2 + j, interleaved (re, im) FP32 or FP16.
+//
+// Complex arithmetic on real tensor-core products (per k-step, column
+// antennas j in the MMA's M dimension, row antennas i in its N dimension):
+//   Re R_ij += Re_j . Re_i + Im_j . Im_i
+//   Im R_ij += Re_j . Im_i - Im_j . Re_i      (negate-A bit of the MMA)
+// which is exactly 8 real FLOPs per complex multiply-accumulate.
 #pragma once
 #include <cstdint>
 #include <cuda.h>
@@ -18,16 +22,12 @@
 
 namespace ftdx {
 
-constexpr int kBlockJ = 128;                 // UMMA M: column antennas j (x rows)
-constexpr int kBlockI = 128;                 // row antennas i, two operand rows each
-constexpr int kUmmaN = 2 * kBlockI;          // UMMA N = 256
-constexpr int kKBytes = 128;                 // operand bytes of K per stage = 64 samples
-constexpr int kSamplesPerStage = kKBytes / 2;
-constexpr int kStages = 4;
-constexpr int kABytes = kBlockJ * kKBytes;   // 16 KB
-constexpr int kBBytes = kUmmaN * kKBytes;    // 32 KB
-constexpr int kStageBytes = kABytes + kBBytes;
-constexpr int kAccCols = kUmmaN;             // FP32 TMEM columns per accumulator
+constexpr int kTile = 128;                   // antennas per operand tile (M = N = 128)
+constexpr int kStageK = 128;                 // samples per pipeline stage (= bytes per plane row)
+constexpr int kPlaneBytes = kTile * kStageK; // 16 KB
+constexpr int kStageBytes = 4 * kPlaneBytes; // A_re, A_im, B_re, B_im
+constexpr int kStages = 3;
+constexpr int kAccCols = 2 * kTile;          // FP32 TMEM columns per accumulator: Re | Im
 constexpr int kHerkThreads = 192;            // TMA warp, MMA warp, 4 epilogue warps
 constexpr size_t kHerkSmem = 1024 + size_t(kStages) * kStageBytes + 256;
 
@@ -38,9 +38,8 @@ struct TileDesc {
   uint16_t tj;
 };
 
-// Per-channel geometry.  row0 is the channel's first antenna row in the
-// x-row view of Z (its Z rows start at 2*row0); out0 is the channel's first
-// packed-triangle element in the output.
+// Per-channel geometry.  row0 is the channel's first row in each plane of Z;
+// out0 is the channel's first packed-triangle element in the output.
 struct ChanDesc {
   int32_t n;
   int32_t kblocks;
@@ -61,11 +60,10 @@ struct HerkArgs {
 };
 
 // Host-side launchers (herk_fp8.cu).
-cudaError_t launch_qc_to_z(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
-                           int sm_count, cudaStream_t s);
-cudaError_t launch_fp16_to_z(const void* a16, uint8_t* z, int64_t rows, int K, int Kp,
-                             int sm_count, cudaStream_t s);
-cudaError_t launch_herk_fp8(const CUtensorMap& tmX, const CUtensorMap& tmZ, const HerkArgs& a,
-                            int grid, cudaStream_t s);
+cudaError_t launch_qc_to_planes(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
+                                cudaStream_t s);
+cudaError_t launch_fp16_to_planes(const void* a16, uint8_t* z, int64_t rows, int K, int Kp,
+                                  cudaStream_t s);
+cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s);
 
 }  // namespace ftdx

@@ -97,6 +97,16 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* m, 
       : "memory");
 }
 
+// 3-D tiled load into shared memory, completing on mbarrier `bar`.
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* m, int32_t x,
+                                            int32_t y, int32_t z, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(m)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+
 // ---------------------------------------------------------------- tcgen05
 __device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem),
@@ -176,10 +186,12 @@ __device__ __forceinline__ uint64_t sdesc_sw128_kmajor(uint32_t saddr) {
 // Instruction descriptor for kind::f8f6f4 / kind::f16 dense MMA with FP32
 // accumulation and K-major A and B.
 //   a_fmt/b_fmt: f8f6f4 -> 0 = E4M3; f16 -> 0 = F16, 1 = BF16.
+//   neg_a: negate A (valid for kind::f16 and kind::f8f6f4).
 __host__ __device__ constexpr uint32_t idesc_f32acc(uint32_t a_fmt, uint32_t b_fmt, uint32_t M,
-                                                    uint32_t N) {
+                                                    uint32_t N, uint32_t neg_a = 0) {
   return (1u << 4)                 // D format: F32
          | (a_fmt << 7) | (b_fmt << 10)
+         | (neg_a << 13)
          | ((N >> 3) << 17)        // N / 8
          | ((M >> 4) << 24);       // M / 16
 }

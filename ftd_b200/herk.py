@@ -108,6 +108,19 @@ class Correlator:
     def end_herk(self) -> None:
         check(self._h, self._L.ftdx_end_herk(self._h), "ftdx_end_herk")
 
+    def set_profiling(self, enable: bool) -> None:
+        check(self._h, self._L.ftdx_set_profiling(self._h, int(bool(enable))), "ftdx_set_profiling")
+
+    def profile_read(self) -> dict:
+        """Summed CUDA-event device time (ms) and launch counts per kernel kind."""
+        hm, pm = ctypes.c_double(0), ctypes.c_double(0)
+        hn, pn = ctypes.c_int(0), ctypes.c_int(0)
+        st = self._L.ftdx_profile_read(self._h, ctypes.byref(hm), ctypes.byref(hn),
+                                       ctypes.byref(pm), ctypes.byref(pn))
+        check(self._h, st, "ftdx_profile_read")
+        return {"herk_ms": hm.value, "herk_launches": hn.value,
+                "prep_ms": pm.value, "prep_launches": pn.value}
+
     def device_status(self, stream=None) -> int:
         """Synchronise the stream and return (and clear) the device status bits."""
         bits = ctypes.c_uint32(0)

@@ -108,6 +108,16 @@ FTDX_API ftdx_status ftdx_end_herk(ftdx_handle h);
  * Returns FTDX_ERR_TIMEOUT if any bit was set. */
 FTDX_API ftdx_status ftdx_device_status(ftdx_handle h, void* stream, uint32_t* bits);
 
+/* Kernel timing (no counterpart in the reference; its benches time whole
+ * calls).  While enabled, CUDA events are recorded on the caller's stream
+ * around every kernel this handle launches.  ftdx_profile_read synchronises,
+ * returns the summed device time (ms) and launch count of the correlator
+ * kernel (`herk_*`) and of the operand-promotion kernel (`prep_*`), and resets
+ * the counters.  Any pointer may be NULL. */
+FTDX_API ftdx_status ftdx_set_profiling(ftdx_handle h, int enable);
+FTDX_API ftdx_status ftdx_profile_read(ftdx_handle h, double* herk_ms, int* herk_launches,
+                                       double* prep_ms, int* prep_launches);
+
 #ifdef __cplusplus
 }
 #endif
