@@ -61,6 +61,7 @@ struct ftdx_context {
   bool z_reserved = false;    // sized by ftdx_init_herk
   uint32_t* d_status = nullptr;
   std::map<std::tuple<int, int, int>, std::unique_ptr<Plan>> plans;  // (N, kblocks, batch)
+  int bulk_store = 0;  // epilogue store mode (HerkArgs::bulk_store)
   // kernel timing (ftdx_set_profiling)
   bool profiling = false;
   struct Timed {
@@ -368,6 +369,8 @@ ftdx_status ftdx_herk(ftdx_handle h, const void* A, void* C, int N, int K, int b
   args.chans = plan->d_chans;
   args.num_tiles = plan->num_tiles;
   args.out_fp16 = (output == FTDX_OUT_FP16) ? 1 : 0;
+  args.bulk_store = h->bulk_store;
+  args.reserved = 0;
   args.out = C;
   args.alpha = alpha;
   args.beta = beta;

@@ -124,26 +124,18 @@ __global__ void __launch_bounds__(256) fp16_to_planes_kernel(const __half2* __re
 }
 
 // ------------------------------------------------------------------ HERK
-__device__ __forceinline__ void store_elem(float* out, int64_t idx, float re, float im,
-                                           float beta) {
-  float2* p = reinterpret_cast<float2*>(out) + idx;
-  if (beta != 0.f) {
-    const float2 o = __ldcs(p);
-    re += beta * o.x;
-    im += beta * o.y;
-  }
-  __stcs(p, make_float2(re, im));
-}
-__device__ __forceinline__ void store_elem(__half* out, int64_t idx, float re, float im,
-                                           float beta) {
-  __half2* p = reinterpret_cast<__half2*>(out) + idx;
-  if (beta != 0.f) {
-    const float2 o = __half22float2(*p);
-    re += beta * o.x;
-    im += beta * o.y;
-  }
+// Output element stores.  Streaming (.cs) stores: the triangle is written
+// once and never re-read by this kernel.
+__device__ __forceinline__ void put(float2* p, float re, float im) { __stcs(p, make_float2(re, im)); }
+__device__ __forceinline__ void put(__half2* p, float re, float im) {
   *p = __floats2half2_rn(re, im);
 }
+__device__ __forceinline__ float2 get(const float2* p) { return __ldcs(p); }
+__device__ __forceinline__ float2 get(const __half2* p) { return __half22float2(*p); }
+
+template <typename T> struct Complex2;
+template <> struct Complex2<float> { using type = float2; };
+template <> struct Complex2<__half> { using type = __half2; };
 
 template <typename OutT>
 __global__ void __launch_bounds__(kHerkThreads, 1)
@@ -152,7 +144,8 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   // 128 B swizzled operand tiles must start on 1024 B boundaries of the
   // shared window.
   uint8_t* smem = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+  uint8_t* stg_base = smem + kStages * kStageBytes;  // epilogue staging (kStgBytes)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(stg_base + kStgBytes);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 5);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -178,7 +171,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(tfull_bar(b), 1);
-      mbar_init(tempty_bar(b), 4);
+      mbar_init(tempty_bar(b), kEpiWarps);
     }
     mbar_init(done_bar, 1);
     *abort_flag = 0;
@@ -303,44 +296,104 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       if (!mbar_wait(done_bar, 0, &never)) atomicOr(args.status, kStatusTimeoutOther);
     }
   } else {
-    // ------------------------------------------------ epilogue (warps 2..5)
-    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    // ------------------------------------------------ epilogue warps
+    // Warp w may read TMEM lanes 32*(w%4)..+31 (columns j); the four warps
+    // of a half own rows [64h, 64h+64) of the tile and sync on barrier 1+h.
+    using Out2 = typename Complex2<OutT>::type;
+    constexpr int kChunks = kTile / 32 / (kEpiWarps / 4);
+    constexpr bool kBulkOut = sizeof(Out2) == 8;  // complex64 rows: 1 KB per tile row
+    const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
+    const uint32_t bar_id = 1u + uint32_t(half);
+    const bool plain = (args.alpha == 1.f) && (args.beta == 0.f);
+    const uint32_t stg = smem_u32(stg_base) + uint32_t(half * 2 * kStgRows * kStgRowBytes);
+    const bool issuer = (q == 0) && (lane < kStgRows);  // issues one row copy per sub-chunk
     int acc = 0;
     uint32_t acc_phase = 0;
-    OutT* out = static_cast<OutT*>(args.out);
+    Out2* out = static_cast<Out2*>(args.out);
     for (int t = blockIdx.x; t < args.num_tiles; t += gridDim.x) {
       const TileDesc td = args.tiles[t];
       const ChanDesc cd = args.chans[td.ch];
-      const bool ok = __all_sync(0xffffffffu, mbar_wait(tfull_bar(acc), acc_phase, abort_flag));
+      const bool ok = bar_red_and(bar_id, 128, mbar_wait(tfull_bar(acc), acc_phase, abort_flag));
       if (!ok) {
         if (lane == 0) atomicOr(args.status, kStatusTimeoutEpilogue);
         break;
       }
       tc_fence_after();
       const int n = cd.n;
-      const int jw = int(td.tj) * kTile + q * 32;  // first column of this warp
+      const int j0 = int(td.tj) * kTile;
+      const int jw = j0 + q * 32;  // first column of this warp
       const int j = jw + lane;
       const int ib = int(td.ti) * kTile;
-      OutT* outc = out + 2 * cd.out0;
       const uint32_t tb = tmem_base + (uint32_t(q * 32) << 16) + uint32_t(acc * kAccCols);
+      Out2* outc = out + cd.out0;
+      if (kBulkOut && args.bulk_store && plain && td.ti != td.tj && ib + kTile <= n) {
+        // Interior tile: stage kStgRows row segments (128 consecutive packed
+        // elements each) in shared memory, then one bulk copy per row.  A
+        // row whose global start is 8 mod 16 keeps that phase in shared
+        // memory; its first and last elements are stored directly.
 #pragma unroll 1
-      for (int c = 0; c < kTile / 32; ++c) {
-        const int i0 = ib + 32 * c;
-        if (i0 + 31 < jw || i0 >= n) continue;  // warp-uniform: nothing to store
-        uint32_t re[32], im[32];
-        __syncwarp();
-        tmem_ld_32x32b_x32(tb + 32u * c, re);
-        tmem_ld_32x32b_x32(tb + uint32_t(kTile) + 32u * c, im);
-        tmem_wait_ld();
-        if (j < n) {
+        for (int sc = 0; sc < (kTile / 2) / kStgRows; ++sc) {
+          const int is = ib + half * (kTile / 2) + sc * kStgRows;
+          const uint32_t col = uint32_t(half * (kTile / 2) + sc * kStgRows);
+          uint32_t re[kStgRows], im[kStgRows];
+          __syncwarp();
+          tmem_ld_32x32b_x8(tb + col, re);
+          tmem_ld_32x32b_x8(tb + uint32_t(kTile) + col, im);
+          tmem_wait_ld();
+          const uint32_t buf = stg + uint32_t((sc & 1) * kStgRows * kStgRowBytes);
+#pragma unroll
+          for (int m = 0; m < kStgRows; ++m) {
+            const int i = is + m;
+            Out2* g = outc + int64_t(i) * (i + 1) / 2 + j0;
+            const uint32_t ph = uint32_t(reinterpret_cast<uintptr_t>(g) & 8u);
+            st_shared_v2(buf + uint32_t(m * kStgRowBytes) + ph + 8u * uint32_t(q * 32 + lane),
+                         re[m], im[m]);
+            if (ph && ((q == 0 && lane == 0) || (q == 3 && lane == 31)))
+              put(outc + int64_t(i) * (i + 1) / 2 + j, __uint_as_float(re[m]),
+                  __uint_as_float(im[m]));
+          }
+          fence_proxy_async_smem();
+          named_bar_sync(bar_id, 128);
+          if (issuer) {
+            const int i = is + lane;
+            Out2* g = outc + int64_t(i) * (i + 1) / 2 + j0;
+            const bool odd = (reinterpret_cast<uintptr_t>(g) & 8u) != 0;
+            const uint32_t src = buf + uint32_t(lane * kStgRowBytes) + (odd ? 16u : 0u);
+            bulk_store(odd ? static_cast<void*>(g + 1) : static_cast<void*>(g), src,
+                       odd ? uint32_t((kTile - 2) * 8) : uint32_t(kTile * 8));
+            bulk_commit();
+            bulk_wait_read<1>();  // the other buffer is free again
+          }
+          named_bar_sync(bar_id, 128);
+        }
+      } else {
+#pragma unroll 1
+        for (int cc = 0; cc < kChunks; ++cc) {
+          const int c = half * kChunks + cc;
+          const int i0 = ib + 32 * c;
+          if (i0 + 31 < jw || i0 >= n) continue;  // warp-uniform: nothing to store
+          uint32_t re[32], im[32];
+          __syncwarp();
+          tmem_ld_32x32b_x32(tb + 32u * c, re);
+          tmem_ld_32x32b_x32(tb + uint32_t(kTile) + 32u * c, im);
+          tmem_wait_ld();
+          // element (i, j) lives at i(i+1)/2 + j; row i+1 starts i+1 later
+          Out2* p = outc + int64_t(i0) * (i0 + 1) / 2 + j;
 #pragma unroll
           for (int m = 0; m < 32; ++m) {
             const int i = i0 + m;
             if (i < n && j <= i) {
-              const float vr = __uint_as_float(re[m]) * args.alpha;
-              const float vi = (i == j) ? 0.f : __uint_as_float(im[m]) * args.alpha;
-              store_elem(outc, int64_t(i) * (i + 1) / 2 + j, vr, vi, args.beta);
+              float vr = __uint_as_float(re[m]) * args.alpha;
+              float vi = (i == j) ? 0.f : __uint_as_float(im[m]) * args.alpha;
+              if (args.beta != 0.f) {
+                const float2 o = get(p);
+                vr += args.beta * o.x;
+                vi += args.beta * o.y;
+              }
+              put(p, vr, vi);
             }
+            p += i + 1;
           }
         }
       }
@@ -352,6 +405,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
         acc_phase ^= 1u;
       }
     }
+    if (issuer) bulk_wait<0>();  // bulk stores complete before the CTA exits
   }
 
   tc_fence_before();

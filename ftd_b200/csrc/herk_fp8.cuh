@@ -28,8 +28,15 @@ constexpr int kPlaneBytes = kTile * kStageK; // 16 KB
 constexpr int kStageBytes = 4 * kPlaneBytes; // A_re, A_im, B_re, B_im
 constexpr int kStages = 3;
 constexpr int kAccCols = 2 * kTile;          // FP32 TMEM columns per accumulator: Re | Im
-constexpr int kHerkThreads = 192;            // TMA warp, MMA warp, 4 epilogue warps
-constexpr size_t kHerkSmem = 1024 + size_t(kStages) * kStageBytes + 256;
+constexpr int kEpiWarps = 8;                 // two per TMEM lane quarter
+constexpr int kHerkThreads = 64 + 32 * kEpiWarps;  // TMA warp, MMA warp, epilogue warps
+// Epilogue staging for bulk stores: per half of the epilogue warps, two
+// buffers of kStgRows triangle-row segments (128 complex64 = 1 KB each, plus
+// 16 B so a row can keep the 16-byte phase of its global address).
+constexpr int kStgRows = 8;
+constexpr int kStgRowBytes = kTile * 8 + 16;
+constexpr int kStgBytes = 2 /*halves*/ * 2 /*buffers*/ * kStgRows * kStgRowBytes;
+constexpr size_t kHerkSmem = 1024 + size_t(kStages) * kStageBytes + kStgBytes + 256;
 
 // One lower-triangle tile: channel, row block ti (i), column block tj (j), tj <= ti.
 struct TileDesc {
@@ -53,6 +60,8 @@ struct HerkArgs {
   const ChanDesc* chans;
   int32_t num_tiles;
   int32_t out_fp16;
+  int32_t bulk_store;  // 1: interior tiles leave through shared memory + bulk copies
+  int32_t reserved;
   void* out;
   float alpha;
   float beta;

@@ -58,7 +58,7 @@ def test_small_config_bit_exact(corr):
     assert np.array_equal(C, oracle.herk_qc(qc, N, K, B).astype(np.float32))
 
 
-@pytest.mark.parametrize("N,K,B", [(256, 1024, 2), (300, 100, 2), (129, 64, 3), (2, 1, 5),
+@pytest.mark.parametrize("N,K,B", [(256, 1024, 2), (300, 100, 2), (129, 64, 3), (2, 1, 5), (257, 96, 3),
                                    (384, 63, 1), (513, 200, 1)])
 def test_ragged_shapes_bit_exact(corr, N, K, B):
     qc = oracle.gaussian_qc(N * 1000 + K, B, N, K)
