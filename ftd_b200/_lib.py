@@ -52,6 +52,13 @@ PROTOTYPES = {
     "ftdx_end_herk": (_i, [_vp]),
     "ftdx_device_status": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32)]),
     "ftdx_set_profiling": (_i, [_vp, _i]),
+    "ftdx_set_tune_cache": (_i, [_vp, ctypes.c_char_p]),
+    "ftdx_tune": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, ctypes.POINTER(_i),
+                       ctypes.POINTER(_i), ctypes.POINTER(_f)]),
+    "ftdx_lookup_tuned": (_i, [_vp, _i, _i, _i, _i, _i, ctypes.POINTER(_i), ctypes.POINTER(_i),
+                               ctypes.POINTER(_f)]),
+    "ftdx_set_graph_mode": (_i, [_vp, _i]),
+    "ftdx_graph_count": (_i, [_vp]),
     "ftdx_profile_read": (_i, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i),
                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i)]),
 }

@@ -1,0 +1,129 @@
+// context.h -- internal state behind an ftdx_handle, shared by the C-ABI
+// translation units (ftdx_api.cu, herk_api.cu, ...).
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <list>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/ftdx.h"
+#include "herk_fp8.cuh"
+
+namespace ftdx {
+
+// Device-resident tile list + channel table for one problem shape.
+struct Plan {
+  TileDesc* d_tiles = nullptr;
+  ChanDesc* d_chans = nullptr;
+  int num_tiles = 0;
+  int num_chans = 0;
+  ~Plan();
+};
+
+// Launch strategy of the correlator kernel; chosen by the autotuner.
+struct Strategy {
+  int store_mode = 0;  // 0: direct stores, 1: shared-memory staging + bulk copies
+  int grid = 0;        // persistent CTAs (0: one per SM)
+  bool operator==(const Strategy& o) const {
+    return store_mode == o.store_mode && grid == o.grid;
+  }
+};
+
+// Autotune cache key: device, problem shape and precisions.
+struct TuneKey {
+  std::string device;
+  int n, kp, batch, input, output;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(device, n, kp, batch, input, output) <
+           std::tie(o.device, o.n, o.kp, o.batch, o.input, o.output);
+  }
+};
+struct TuneEntry {
+  Strategy st;
+  float ms = 0.f;
+};
+
+// One captured launch sequence (promotion + correlator) for graph replay.
+struct GraphKey {
+  const void* a;
+  void* c;
+  int n, k, batch, input, output;
+  float alpha, beta;
+  int store_mode, grid;
+  bool operator==(const GraphKey& o) const {
+    return a == o.a && c == o.c && n == o.n && k == o.k && batch == o.batch &&
+           input == o.input && output == o.output && alpha == o.alpha && beta == o.beta &&
+           store_mode == o.store_mode && grid == o.grid;
+  }
+};
+struct GraphEntry {
+  GraphKey key;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+}  // namespace ftdx
+
+struct ftdx_context {
+  int device = 0;
+  int sm_count = 148;
+  int verbosity = 0;
+  std::string device_name;
+  std::string last_error;
+  // FP8 operand workspace (grown on demand, or pre-sized by ftdx_init_herk)
+  uint8_t* z = nullptr;
+  size_t z_cap = 0;
+  uint32_t* d_status = nullptr;
+  std::map<std::tuple<int, int, int>, std::unique_ptr<ftdx::Plan>> plans;  // (N, kblocks, batch)
+  // autotuner
+  std::string tune_cache;
+  std::map<ftdx::TuneKey, ftdx::TuneEntry> tuned;
+  int cache_bad_lines = 0;
+  // graph replay (most recently used first)
+  bool graph_mode = false;
+  cudaStream_t capture_stream = nullptr;
+  std::list<ftdx::GraphEntry> graphs;
+  // kernel timing (ftdx_set_profiling)
+  bool profiling = false;
+  struct Timed {
+    cudaEvent_t a, b;
+    int kind;  // 0 = correlator, 1 = promotion
+  };
+  std::vector<Timed> timed;
+  std::vector<cudaEvent_t> event_pool;
+};
+
+namespace ftdx {
+
+constexpr size_t kGraphCacheSize = 4;
+
+ftdx_status fail(ftdx_handle h, ftdx_status s, const char* fmt, ...);
+ftdx_status cuda_fail(ftdx_handle h, cudaError_t e, const char* what);
+bool stream_capturing(cudaStream_t s);
+ftdx_status ensure_workspace(ftdx_handle h, size_t bytes, cudaStream_t s);
+ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
+                     const Plan** out);
+ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t Kp,
+                              CUtensorMap* tm);
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// Event pair around one kernel launch when profiling is on (never during capture).
+struct ScopedTimer {
+  ftdx_handle h;
+  cudaStream_t s;
+  int kind;
+  cudaEvent_t a = nullptr;
+  ScopedTimer(ftdx_handle h_, cudaStream_t s_, int kind_);
+  ~ScopedTimer();
+};
+
+void release_graphs(ftdx_handle h);
+void load_tune_cache(ftdx_handle h);
+
+}  // namespace ftdx

@@ -1,27 +1,23 @@
-// ftdx_api.cu -- C ABI of the correlator: handles, workspace, tile plans,
-// tensor-map encoding and kernel dispatch.  See include/ftdx.h.
-#include "../../include/ftdx.h"
-#include "herk_fp8.cuh"
-
-#include <cuda.h>
+// ftdx_api.cu -- C ABI core: handles, workspace, tile plans, tensor maps,
+// device status and kernel timing.  The correlator entry points are in
+// herk_api.cu.  See include/ftdx.h.
 #include <cudaTypedefs.h>
-#include <cuda_runtime.h>
 
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
-#include <map>
-#include <memory>
-#include <string>
-#include <tuple>
-#include <vector>
 
-namespace {
+#include "context.h"
 
-using ftdx::ChanDesc;
-using ftdx::TileDesc;
+namespace ftdx {
 
-PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
+Plan::~Plan() {
+  if (d_tiles) cudaFree(d_tiles);
+  if (d_chans) cudaFree(d_chans);
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static bool tried = false;
   if (!tried) {
@@ -35,44 +31,6 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
   }
   return fn;
 }
-
-// Device-resident tile list + channel table for one problem shape.
-struct Plan {
-  TileDesc* d_tiles = nullptr;
-  ChanDesc* d_chans = nullptr;
-  int num_tiles = 0;
-  int num_chans = 0;
-  ~Plan() {
-    if (d_tiles) cudaFree(d_tiles);
-    if (d_chans) cudaFree(d_chans);
-  }
-};
-
-}  // namespace
-
-struct ftdx_context {
-  int device = 0;
-  int sm_count = 148;
-  int verbosity = 0;
-  std::string tune_cache;
-  std::string last_error;
-  uint8_t* z = nullptr;       // FP8 operand workspace
-  size_t z_cap = 0;
-  bool z_reserved = false;    // sized by ftdx_init_herk
-  uint32_t* d_status = nullptr;
-  std::map<std::tuple<int, int, int>, std::unique_ptr<Plan>> plans;  // (N, kblocks, batch)
-  int bulk_store = 0;  // epilogue store mode (HerkArgs::bulk_store)
-  // kernel timing (ftdx_set_profiling)
-  bool profiling = false;
-  struct Timed {
-    cudaEvent_t a, b;
-    int kind;  // 0 = herk, 1 = prep
-  };
-  std::vector<Timed> timed;
-  std::vector<cudaEvent_t> event_pool;
-};
-
-namespace {
 
 ftdx_status fail(ftdx_handle h, ftdx_status s, const char* fmt, ...) {
   if (h) {
@@ -93,7 +51,10 @@ ftdx_status cuda_fail(ftdx_handle h, cudaError_t e, const char* what) {
 
 bool stream_capturing(cudaStream_t s) {
   cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
-  if (cudaStreamIsCapturing(s, &st) != cudaSuccess) return false;
+  if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
   return st != cudaStreamCaptureStatusNone;
 }
 
@@ -105,10 +66,11 @@ ftdx_status ensure_workspace(ftdx_handle h, size_t bytes, cudaStream_t s) {
                 "first",
                 bytes, h->z_cap);
   if (h->z) {
-    cudaStreamSynchronize(s);
+    cudaDeviceSynchronize();  // every queued user of the old buffer is done
     cudaFree(h->z);
     h->z = nullptr;
     h->z_cap = 0;
+    release_graphs(h);  // captured graphs point at the old buffer
   }
   cudaError_t e = cudaMalloc(&h->z, bytes);
   if (e != cudaSuccess) {
@@ -121,7 +83,7 @@ ftdx_status ensure_workspace(ftdx_handle h, size_t bytes, cudaStream_t s) {
 }
 
 // Lower-triangle tile list for `batch` channels of N inputs, channel-major so
-// that consecutive CTAs share a channel's operand in L2.
+// that concurrently running CTAs share a channel's operand in L2.
 ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
                      const Plan** out) {
   auto key = std::make_tuple(N, kblocks, batch);
@@ -134,7 +96,7 @@ ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t 
     return fail(h, FTDX_ERR_CAPACITY,
                 "tile plan for N=%d batch=%d built while capturing; call ftdx_init_herk first", N,
                 batch);
-  const int nb = (N + ftdx::kTile - 1) / ftdx::kTile;
+  const int nb = (N + kTile - 1) / kTile;
   std::vector<ChanDesc> chans(batch);
   std::vector<TileDesc> tiles;
   tiles.reserve(size_t(batch) * nb * (nb + 1) / 2);
@@ -173,7 +135,7 @@ ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t K
   const cuuint32_t estr[3] = {1, 1, 1};
   const cuuint64_t dims[3] = {cuuint64_t(Kp), cuuint64_t(rows), 2};
   const cuuint64_t strides[2] = {cuuint64_t(Kp), cuuint64_t(rows * Kp)};
-  const cuuint32_t box[3] = {cuuint32_t(ftdx::kStageK), cuuint32_t(ftdx::kTile), 1};
+  const cuuint32_t box[3] = {cuuint32_t(kStageK), cuuint32_t(kTile), 1};
   CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, z, dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -181,9 +143,7 @@ ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t K
   return FTDX_OK;
 }
 
-inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
-
-cudaEvent_t pool_event(ftdx_handle h) {
+static cudaEvent_t pool_event(ftdx_handle h) {
   if (!h->event_pool.empty()) {
     cudaEvent_t e = h->event_pool.back();
     h->event_pool.pop_back();
@@ -194,28 +154,24 @@ cudaEvent_t pool_event(ftdx_handle h) {
   return e;
 }
 
-// Records an event pair around one kernel launch when profiling is on.
-struct ScopedTimer {
-  ftdx_handle h;
-  cudaStream_t s;
-  int kind;
-  cudaEvent_t a = nullptr;
-  ScopedTimer(ftdx_handle h_, cudaStream_t s_, int kind_) : h(h_), s(s_), kind(kind_) {
-    if (h->profiling) {
-      a = pool_event(h);
-      cudaEventRecord(a, s);
-    }
+ScopedTimer::ScopedTimer(ftdx_handle h_, cudaStream_t s_, int kind_) : h(h_), s(s_), kind(kind_) {
+  if (h->profiling && !stream_capturing(s)) {
+    a = pool_event(h);
+    cudaEventRecord(a, s);
   }
-  ~ScopedTimer() {
-    if (a) {
-      cudaEvent_t b = pool_event(h);
-      cudaEventRecord(b, s);
-      h->timed.push_back({a, b, kind});
-    }
-  }
-};
+}
 
-}  // namespace
+ScopedTimer::~ScopedTimer() {
+  if (a) {
+    cudaEvent_t b = pool_event(h);
+    cudaEventRecord(b, s);
+    h->timed.push_back({a, b, kind});
+  }
+}
+
+}  // namespace ftdx
+
+using namespace ftdx;
 
 extern "C" {
 
@@ -247,25 +203,30 @@ ftdx_status ftdx_create(ftdx_handle* out, const ftdx_config* cfg) {
   int dev = (cfg && cfg->device >= 0) ? cfg->device : -1;
   if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return FTDX_ERR_NO_DEVICE;
   if (dev >= ndev) return FTDX_ERR_INVALID_ARG;
-  int major = 0, minor = 0, sms = 0;
-  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
-  cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (major != 10 || minor != 0) return FTDX_ERR_NO_DEVICE;
+  cudaDeviceProp prop{};
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return FTDX_ERR_NO_DEVICE;
+  if (prop.major != 10 || prop.minor != 0) return FTDX_ERR_NO_DEVICE;
   if (cudaSetDevice(dev) != cudaSuccess) return FTDX_ERR_NO_DEVICE;
   auto* h = new ftdx_context();
   h->device = dev;
-  h->sm_count = sms;
-  if (cfg) {
-    h->verbosity = cfg->verbosity;
-    if (cfg->tune_cache) h->tune_cache = cfg->tune_cache;
-  }
+  h->sm_count = prop.multiProcessorCount;
+  h->device_name = prop.name;
+  for (char& c : h->device_name)
+    if (c == ' ' || c == '\t') c = '_';
+  if (cfg) h->verbosity = cfg->verbosity;
+  if (cfg && cfg->tune_cache)
+    h->tune_cache = cfg->tune_cache;
+  else if (const char* env = getenv("FTDX_TUNE_CACHE"))
+    h->tune_cache = env;
   if (cudaMalloc(&h->d_status, sizeof(uint32_t)) != cudaSuccess ||
-      cudaMemset(h->d_status, 0, sizeof(uint32_t)) != cudaSuccess) {
+      cudaMemset(h->d_status, 0, sizeof(uint32_t)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->capture_stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
+    if (h->d_status) cudaFree(h->d_status);
     delete h;
     return FTDX_ERR_ALLOC;
   }
+  load_tune_cache(h);
   *out = h;
   return FTDX_OK;
 }
@@ -274,6 +235,7 @@ ftdx_status ftdx_destroy(ftdx_handle h) {
   if (!h) return FTDX_ERR_INVALID_ARG;
   cudaSetDevice(h->device);
   cudaDeviceSynchronize();
+  release_graphs(h);
   h->plans.clear();
   for (auto& t : h->timed) {
     cudaEventDestroy(t.a);
@@ -282,107 +244,12 @@ ftdx_status ftdx_destroy(ftdx_handle h) {
   for (auto e : h->event_pool) cudaEventDestroy(e);
   if (h->z) cudaFree(h->z);
   if (h->d_status) cudaFree(h->d_status);
+  if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
   delete h;
   return FTDX_OK;
 }
 
 const char* ftdx_last_error(ftdx_handle h) { return h ? h->last_error.c_str() : "null handle"; }
-
-ftdx_status ftdx_init_herk(ftdx_handle h, int N, int K, int batch, void* stream) {
-  if (!h) return FTDX_ERR_INVALID_ARG;
-  if (N < 1 || K < 1 || batch < 1) return fail(h, FTDX_ERR_INVALID_ARG, "init_herk: bad sizes");
-  cudaSetDevice(h->device);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int64_t Kp = round_up(K, ftdx::kStageK);
-  ftdx_status st = ensure_workspace(h, size_t(2) * N * batch * Kp, s);
-  if (st != FTDX_OK) return st;
-  h->z_reserved = true;
-  const Plan* p = nullptr;
-  return get_plan(h, N, int(Kp / ftdx::kStageK), batch, s, &p);
-}
-
-ftdx_status ftdx_end_herk(ftdx_handle h) {
-  if (!h) return FTDX_ERR_INVALID_ARG;
-  cudaSetDevice(h->device);
-  cudaDeviceSynchronize();
-  if (h->z) cudaFree(h->z);
-  h->z = nullptr;
-  h->z_cap = 0;
-  h->z_reserved = false;
-  h->plans.clear();
-  return FTDX_OK;
-}
-
-ftdx_status ftdx_herk(ftdx_handle h, const void* A, void* C, int N, int K, int batch,
-                      ftdx_input input, ftdx_compute compute, ftdx_output output,
-                      ftdx_format format, float alpha, float beta, void* stream, int tune) {
-  (void)tune;
-  if (!h) return FTDX_ERR_INVALID_ARG;
-  if (!A || !C) return fail(h, FTDX_ERR_INVALID_ARG, "herk: null A or C");
-  if (N < 1 || K < 1 || batch < 1)
-    return fail(h, FTDX_ERR_INVALID_ARG, "herk: N, K and batch must be >= 1 (got %d, %d, %d)", N,
-                K, batch);
-  if (input != FTDX_IN_INT4 && input != FTDX_IN_FP16)
-    return fail(h, FTDX_ERR_INVALID_ARG, "herk: bad input precision %d", int(input));
-  if (output != FTDX_OUT_FP32 && output != FTDX_OUT_FP16)
-    return fail(h, FTDX_ERR_INVALID_ARG, "herk: bad output precision %d", int(output));
-  if (format != FTDX_FORMAT_PACKED_TRIANGLE)
-    return fail(h, FTDX_ERR_INVALID_ARG, "herk: only the packed triangle format exists");
-  if (compute != FTDX_COMPUTE_FP8)
-    return fail(h, FTDX_ERR_UNSUPPORTED, "herk: compute precision %d not implemented",
-                int(compute));
-  if ((reinterpret_cast<uintptr_t>(C) & (output == FTDX_OUT_FP32 ? 7 : 3)) != 0)
-    return fail(h, FTDX_ERR_INVALID_ARG, "herk: C is not aligned to one complex element");
-  if (input == FTDX_IN_FP16 && (reinterpret_cast<uintptr_t>(A) & 3) != 0)
-    return fail(h, FTDX_ERR_INVALID_ARG, "herk: FP16 A must be 4-byte aligned");
-  // Row coordinates of the TMA boxes are 32-bit.
-  if (int64_t(N) * batch + 256 > (int64_t(1) << 31))
-    return fail(h, FTDX_ERR_INVALID_ARG, "herk: N*batch too large for one call");
-  if (N > 65535 * ftdx::kTile)
-    return fail(h, FTDX_ERR_INVALID_ARG, "herk: N too large");
-
-  cudaError_t e = cudaSetDevice(h->device);
-  if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int64_t Kp = round_up(K, ftdx::kStageK);
-  const int64_t rows = int64_t(N) * batch;
-  ftdx_status st = ensure_workspace(h, size_t(2 * rows * Kp), s);
-  if (st != FTDX_OK) return st;
-  const Plan* plan = nullptr;
-  st = get_plan(h, N, int(Kp / ftdx::kStageK), batch, s, &plan);
-  if (st != FTDX_OK) return st;
-
-  {
-    ScopedTimer tm(h, s, 1);
-    if (input == FTDX_IN_INT4)
-      e = ftdx::launch_qc_to_planes(static_cast<const uint8_t*>(A), h->z, rows, K, int(Kp), s);
-    else
-      e = ftdx::launch_fp16_to_planes(A, h->z, rows, K, int(Kp), s);
-  }
-  if (e != cudaSuccess) return cuda_fail(h, e, "operand promotion launch");
-
-  CUtensorMap tmZ;
-  st = encode_planes_map(h, h->z, rows, Kp, &tmZ);
-  if (st != FTDX_OK) return st;
-  ftdx::HerkArgs args;
-  args.tiles = plan->d_tiles;
-  args.chans = plan->d_chans;
-  args.num_tiles = plan->num_tiles;
-  args.out_fp16 = (output == FTDX_OUT_FP16) ? 1 : 0;
-  args.bulk_store = h->bulk_store;
-  args.reserved = 0;
-  args.out = C;
-  args.alpha = alpha;
-  args.beta = beta;
-  args.status = h->d_status;
-  const int grid = plan->num_tiles < h->sm_count ? plan->num_tiles : h->sm_count;
-  {
-    ScopedTimer tm(h, s, 0);
-    e = ftdx::launch_herk_fp8(tmZ, args, grid, s);
-  }
-  if (e != cudaSuccess) return cuda_fail(h, e, "HERK kernel launch");
-  return FTDX_OK;
-}
 
 ftdx_status ftdx_device_status(ftdx_handle h, void* stream, uint32_t* bits) {
   if (!h) return FTDX_ERR_INVALID_ARG;

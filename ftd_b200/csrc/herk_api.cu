@@ -1,0 +1,369 @@
+// herk_api.cu -- correlator entry points of the C ABI: ftdx_herk, workspace
+// pre-sizing, the strategy autotuner with its disk cache, and CUDA-graph
+// replay.  Mirrors CutlassComplexGemm::herk (cutlass_interface/cutlass_gemm_api.cu:1707-1878),
+// tune_herk / strategy_cache::run_autotune (cutlass_gemm_api.cu:1389-1409,
+// strategy_cache.hpp:504-721) and the direct-HERK graph cache
+// (cutlass_gemm_api.cu:200-315, 1738-1807) of the reference.
+#include <cerrno>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+#include "context.h"
+
+namespace ftdx {
+namespace {
+
+struct HerkCall {
+  const void* A;
+  void* C;
+  int N, K, batch;
+  ftdx_input input;
+  ftdx_output output;
+  float alpha, beta;
+};
+
+ftdx_status validate(ftdx_handle h, const HerkCall& c, ftdx_compute compute, ftdx_format format) {
+  if (!c.A || !c.C) return fail(h, FTDX_ERR_INVALID_ARG, "herk: null A or C");
+  if (c.N < 1 || c.K < 1 || c.batch < 1)
+    return fail(h, FTDX_ERR_INVALID_ARG, "herk: N, K and batch must be >= 1 (got %d, %d, %d)",
+                c.N, c.K, c.batch);
+  if (c.input != FTDX_IN_INT4 && c.input != FTDX_IN_FP16)
+    return fail(h, FTDX_ERR_INVALID_ARG, "herk: bad input precision %d", int(c.input));
+  if (c.output != FTDX_OUT_FP32 && c.output != FTDX_OUT_FP16)
+    return fail(h, FTDX_ERR_INVALID_ARG, "herk: bad output precision %d", int(c.output));
+  if (format != FTDX_FORMAT_PACKED_TRIANGLE)
+    return fail(h, FTDX_ERR_INVALID_ARG, "herk: only the packed triangle format exists");
+  if (compute != FTDX_COMPUTE_FP8)
+    return fail(h, FTDX_ERR_UNSUPPORTED, "herk: compute precision %d not implemented for "
+                "this entry point", int(compute));
+  if ((reinterpret_cast<uintptr_t>(c.C) & (c.output == FTDX_OUT_FP32 ? 7 : 3)) != 0)
+    return fail(h, FTDX_ERR_INVALID_ARG, "herk: C is not aligned to one complex element");
+  if (c.input == FTDX_IN_FP16 && (reinterpret_cast<uintptr_t>(c.A) & 3) != 0)
+    return fail(h, FTDX_ERR_INVALID_ARG, "herk: FP16 A must be 4-byte aligned");
+  // Row coordinates of the TMA boxes are 32-bit.
+  if (int64_t(c.N) * c.batch + 256 > (int64_t(1) << 31))
+    return fail(h, FTDX_ERR_INVALID_ARG, "herk: N*batch too large for one call");
+  if (c.N > 65535 * kTile) return fail(h, FTDX_ERR_INVALID_ARG, "herk: N too large");
+  if (int64_t(c.K) > (int64_t(1) << 30)) return fail(h, FTDX_ERR_INVALID_ARG, "herk: K too large");
+  return FTDX_OK;
+}
+
+// Workspace and tile plan for a call; allocates, so never while capturing.
+ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan** plan) {
+  const int64_t Kp = round_up(c.K, kStageK);
+  const int64_t rows = int64_t(c.N) * c.batch;
+  ftdx_status st = ensure_workspace(h, size_t(2 * rows * Kp), s);
+  if (st != FTDX_OK) return st;
+  return get_plan(h, c.N, int(Kp / kStageK), c.batch, s, plan);
+}
+
+// Promotion kernel + correlator kernel on stream s.
+ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, cudaStream_t s) {
+  const Plan* plan = nullptr;
+  ftdx_status st = prepare(h, c, s, &plan);
+  if (st != FTDX_OK) return st;
+  const int64_t Kp = round_up(c.K, kStageK);
+  const int64_t rows = int64_t(c.N) * c.batch;
+  cudaError_t e;
+  {
+    ScopedTimer tm(h, s, 1);
+    if (c.input == FTDX_IN_INT4)
+      e = launch_qc_to_planes(static_cast<const uint8_t*>(c.A), h->z, rows, c.K, int(Kp), s);
+    else
+      e = launch_fp16_to_planes(c.A, h->z, rows, c.K, int(Kp), s);
+  }
+  if (e != cudaSuccess) return cuda_fail(h, e, "operand promotion launch");
+  CUtensorMap tmZ;
+  st = encode_planes_map(h, h->z, rows, Kp, &tmZ);
+  if (st != FTDX_OK) return st;
+  HerkArgs args;
+  args.tiles = plan->d_tiles;
+  args.chans = plan->d_chans;
+  args.num_tiles = plan->num_tiles;
+  args.out_fp16 = (c.output == FTDX_OUT_FP16) ? 1 : 0;
+  args.bulk_store = strat.store_mode == 1 ? 1 : 0;
+  args.reserved = 0;
+  args.out = c.C;
+  args.alpha = c.alpha;
+  args.beta = c.beta;
+  args.status = h->d_status;
+  int grid = strat.grid > 0 ? strat.grid : h->sm_count;
+  if (grid > h->sm_count) grid = h->sm_count;  // persistent: at most one CTA per SM
+  if (grid > plan->num_tiles) grid = plan->num_tiles;
+  {
+    ScopedTimer tm(h, s, 0);
+    e = launch_herk_fp8(tmZ, args, grid, s);
+  }
+  if (e != cudaSuccess) return cuda_fail(h, e, "correlator kernel launch");
+  return FTDX_OK;
+}
+
+TuneKey tune_key(ftdx_handle h, const HerkCall& c) {
+  return TuneKey{h->device_name, c.N, int(round_up(c.K, kStageK)), c.batch, int(c.input),
+                 int(c.output)};
+}
+
+std::vector<Strategy> candidates(ftdx_handle h, const HerkCall& c) {
+  std::vector<Strategy> v;
+  const int grids[2] = {h->sm_count, h->sm_count - h->sm_count / 8};
+  for (int g : grids) {
+    v.push_back(Strategy{0, g});
+    if (c.output == FTDX_OUT_FP32) v.push_back(Strategy{1, g});
+  }
+  return v;
+}
+
+void append_tune_cache(ftdx_handle h, const TuneKey& k, const TuneEntry& e) {
+  if (h->tune_cache.empty()) return;
+  FILE* f = fopen(h->tune_cache.c_str(), "a");
+  if (!f) {
+    fail(h, FTDX_ERR_CACHE, "cannot append to tune cache %s: %s", h->tune_cache.c_str(),
+         strerror(errno));
+    return;
+  }
+  fprintf(f, "ftdx-tune 1 %s %d %d %d %d %d %d %d %.6f\n", k.device.c_str(), k.n, k.kp, k.batch,
+          k.input, k.output, e.st.store_mode, e.st.grid, e.ms);
+  fclose(f);
+}
+
+// Times every candidate strategy on the caller's buffers (beta must be 0, so
+// repeated runs leave C as one run would) and records the fastest.
+ftdx_status run_tune(ftdx_handle h, const HerkCall& c, cudaStream_t s, TuneEntry* out) {
+  if (c.beta != 0.f)
+    return fail(h, FTDX_ERR_INVALID_ARG, "tuning needs beta == 0 (C is overwritten)");
+  const Plan* plan = nullptr;
+  ftdx_status st = prepare(h, c, s, &plan);
+  if (st != FTDX_OK) return st;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    return fail(h, FTDX_ERR_CUDA, "tuner events");
+  const bool prof = h->profiling;
+  h->profiling = false;
+  TuneEntry best;
+  best.ms = -1.f;
+  for (const Strategy& cand : candidates(h, c)) {
+    for (int w = 0; w < 2 && st == FTDX_OK; ++w) st = launch_all(h, c, cand, s);
+    if (st != FTDX_OK) break;
+    cudaEventRecord(e0, s);
+    const int reps = 3;
+    for (int r = 0; r < reps && st == FTDX_OK; ++r) st = launch_all(h, c, cand, s);
+    cudaEventRecord(e1, s);
+    if (st != FTDX_OK) break;
+    float ms = 0.f;
+    cudaError_t ce = cudaEventSynchronize(e1);
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+    if (ce != cudaSuccess) {
+      st = cuda_fail(h, ce, "tuner timing");
+      break;
+    }
+    ms /= reps;
+    if (h->verbosity > 1)
+      fprintf(stderr, "ftdx tune N=%d K=%d batch=%d: store=%d grid=%d %.4f ms\n", c.N, c.K,
+              c.batch, cand.store_mode, cand.grid, ms);
+    if (best.ms < 0.f || ms < best.ms) best = TuneEntry{cand, ms};
+  }
+  h->profiling = prof;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != FTDX_OK) return st;
+  const TuneKey k = tune_key(h, c);
+  h->tuned[k] = best;
+  append_tune_cache(h, k, best);
+  if (h->verbosity > 0)
+    fprintf(stderr, "ftdx tuned N=%d K=%d batch=%d -> store=%d grid=%d (%.4f ms)\n", c.N, c.K,
+            c.batch, best.st.store_mode, best.st.grid, best.ms);
+  if (out) *out = best;
+  return FTDX_OK;
+}
+
+// Replays {promotion, correlator} as one CUDA graph per call signature
+// (least-recently-used cache of kGraphCacheSize entries).
+ftdx_status run_graph(ftdx_handle h, const HerkCall& c, const Strategy& strat, cudaStream_t s) {
+  const GraphKey key{c.A, c.C, c.N, c.K, c.batch, int(c.input), int(c.output), c.alpha, c.beta,
+                     strat.store_mode, strat.grid};
+  for (auto it = h->graphs.begin(); it != h->graphs.end(); ++it) {
+    if (it->key == key) {
+      h->graphs.splice(h->graphs.begin(), h->graphs, it);
+      cudaError_t e = cudaGraphLaunch(h->graphs.front().exec, s);
+      return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "cudaGraphLaunch");
+    }
+  }
+  const Plan* plan = nullptr;
+  ftdx_status st = prepare(h, c, s, &plan);  // allocate before capturing
+  if (st != FTDX_OK) return st;
+  GraphEntry ge;
+  ge.key = key;
+  cudaError_t e = cudaStreamBeginCapture(h->capture_stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamBeginCapture");
+  st = launch_all(h, c, strat, h->capture_stream);
+  e = cudaStreamEndCapture(h->capture_stream, &ge.graph);
+  if (st != FTDX_OK) {
+    if (ge.graph) cudaGraphDestroy(ge.graph);
+    return st;
+  }
+  if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&ge.exec, ge.graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(ge.graph);
+    return cuda_fail(h, e, "cudaGraphInstantiate");
+  }
+  h->graphs.push_front(ge);
+  while (h->graphs.size() > kGraphCacheSize) {
+    cudaGraphExecDestroy(h->graphs.back().exec);
+    cudaGraphDestroy(h->graphs.back().graph);
+    h->graphs.pop_back();
+  }
+  e = cudaGraphLaunch(h->graphs.front().exec, s);
+  return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "cudaGraphLaunch");
+}
+
+}  // namespace
+
+void release_graphs(ftdx_handle h) {
+  for (auto& g : h->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+  }
+  h->graphs.clear();
+}
+
+// Text cache, one entry per line:
+//   ftdx-tune 1 <device> <N> <Kp> <batch> <input> <output> <store_mode> <grid> <ms>
+// Unreadable or malformed lines are skipped and counted.
+void load_tune_cache(ftdx_handle h) {
+  h->cache_bad_lines = 0;
+  if (h->tune_cache.empty()) return;
+  std::ifstream f(h->tune_cache);
+  if (!f) return;  // a cache that does not exist yet is not an error
+  std::string line;
+  while (std::getline(f, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream is(line);
+    std::string magic, dev;
+    int ver = 0;
+    TuneKey k;
+    TuneEntry e;
+    if (!(is >> magic >> ver >> dev >> k.n >> k.kp >> k.batch >> k.input >> k.output >>
+          e.st.store_mode >> e.st.grid >> e.ms) ||
+        magic != "ftdx-tune" || ver != 1 || k.n < 1 || k.kp < 1 || k.batch < 1 ||
+        e.st.store_mode < 0 || e.st.store_mode > 1 || e.st.grid < 0 || !(e.ms >= 0.f)) {
+      ++h->cache_bad_lines;
+      continue;
+    }
+    k.device = dev;
+    h->tuned[k] = e;
+  }
+}
+
+}  // namespace ftdx
+
+using namespace ftdx;
+
+extern "C" {
+
+ftdx_status ftdx_herk(ftdx_handle h, const void* A, void* C, int N, int K, int batch,
+                      ftdx_input input, ftdx_compute compute, ftdx_output output,
+                      ftdx_format format, float alpha, float beta, void* stream, int tune) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  const HerkCall c{A, C, N, K, batch, input, output, alpha, beta};
+  ftdx_status st = validate(h, c, compute, format);
+  if (st != FTDX_OK) return st;
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool capturing = stream_capturing(s);
+  Strategy strat;
+  if (tune) {
+    auto it = h->tuned.find(tune_key(h, c));
+    if (it != h->tuned.end()) {
+      strat = it->second.st;
+    } else if (beta == 0.f && !capturing) {
+      TuneEntry te;
+      st = run_tune(h, c, s, &te);
+      if (st != FTDX_OK) return st;
+      strat = te.st;
+    }
+  }
+  if (h->graph_mode && !capturing) return run_graph(h, c, strat, s);
+  return launch_all(h, c, strat, s);
+}
+
+ftdx_status ftdx_init_herk(ftdx_handle h, int N, int K, int batch, void* stream) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  if (N < 1 || K < 1 || batch < 1) return fail(h, FTDX_ERR_INVALID_ARG, "init_herk: bad sizes");
+  cudaSetDevice(h->device);
+  const HerkCall c{reinterpret_cast<const void*>(16), reinterpret_cast<void*>(16), N, K, batch,
+                   FTDX_IN_INT4, FTDX_OUT_FP32, 1.f, 0.f};
+  const Plan* p = nullptr;
+  return prepare(h, c, static_cast<cudaStream_t>(stream), &p);
+}
+
+ftdx_status ftdx_end_herk(ftdx_handle h) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  cudaSetDevice(h->device);
+  cudaDeviceSynchronize();
+  release_graphs(h);
+  if (h->z) cudaFree(h->z);
+  h->z = nullptr;
+  h->z_cap = 0;
+  h->plans.clear();
+  return FTDX_OK;
+}
+
+ftdx_status ftdx_set_tune_cache(ftdx_handle h, const char* path) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  h->tune_cache = path ? path : "";
+  load_tune_cache(h);
+  if (h->cache_bad_lines)
+    return fail(h, FTDX_ERR_CACHE, "tune cache %s: %d malformed line(s) skipped",
+                h->tune_cache.c_str(), h->cache_bad_lines);
+  return FTDX_OK;
+}
+
+ftdx_status ftdx_tune(ftdx_handle h, const void* A, void* C, int N, int K, int batch,
+                      ftdx_input input, ftdx_output output, void* stream, int* store_mode,
+                      int* grid, float* ms) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  const HerkCall c{A, C, N, K, batch, input, output, 1.f, 0.f};
+  ftdx_status st = validate(h, c, FTDX_COMPUTE_FP8, FTDX_FORMAT_PACKED_TRIANGLE);
+  if (st != FTDX_OK) return st;
+  cudaSetDevice(h->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (stream_capturing(s)) return fail(h, FTDX_ERR_CAPACITY, "cannot tune while capturing");
+  TuneEntry te;
+  st = run_tune(h, c, s, &te);
+  if (st != FTDX_OK) return st;
+  if (store_mode) *store_mode = te.st.store_mode;
+  if (grid) *grid = te.st.grid;
+  if (ms) *ms = te.ms;
+  return FTDX_OK;
+}
+
+ftdx_status ftdx_lookup_tuned(ftdx_handle h, int N, int K, int batch, ftdx_input input,
+                              ftdx_output output, int* store_mode, int* grid, float* ms) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  const HerkCall c{nullptr, nullptr, N, K, batch, input, output, 1.f, 0.f};
+  auto it = h->tuned.find(tune_key(h, c));
+  if (it == h->tuned.end()) return fail(h, FTDX_ERR_CACHE, "no tuned entry for this shape");
+  if (store_mode) *store_mode = it->second.st.store_mode;
+  if (grid) *grid = it->second.st.grid;
+  if (ms) *ms = it->second.ms;
+  return FTDX_OK;
+}
+
+ftdx_status ftdx_set_graph_mode(ftdx_handle h, int enable) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  h->graph_mode = enable != 0;
+  if (!h->graph_mode) {
+    cudaSetDevice(h->device);
+    cudaDeviceSynchronize();
+    release_graphs(h);
+  }
+  return FTDX_OK;
+}
+
+int ftdx_graph_count(ftdx_handle h) { return h ? int(h->graphs.size()) : -1; }
+
+}  // extern "C"

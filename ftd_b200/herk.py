@@ -108,6 +108,38 @@ class Correlator:
     def end_herk(self) -> None:
         check(self._h, self._L.ftdx_end_herk(self._h), "ftdx_end_herk")
 
+    # ------------------------------------------------------------ tuning / graphs
+    def set_tune_cache(self, path: str | None) -> None:
+        check(self._h, self._L.ftdx_set_tune_cache(self._h, path.encode() if path else None),
+              "ftdx_set_tune_cache")
+
+    def tune(self, A, C, N: int, K: int, batch: int, input: int = IN_INT4,
+             output: int = OUT_FP32, stream=None) -> dict:
+        """Time every launch strategy for this shape; returns the winner."""
+        sm, g, ms = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_float(0)
+        st = self._L.ftdx_tune(self._h, _ptr(A), _ptr(C), N, K, batch, input, output,
+                               _stream(stream), ctypes.byref(sm), ctypes.byref(g),
+                               ctypes.byref(ms))
+        check(self._h, st, "ftdx_tune")
+        return {"store_mode": sm.value, "grid": g.value, "ms": ms.value}
+
+    def lookup_tuned(self, N: int, K: int, batch: int, input: int = IN_INT4,
+                     output: int = OUT_FP32):
+        """The cached strategy for a shape, or None."""
+        sm, g, ms = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_float(0)
+        st = self._L.ftdx_lookup_tuned(self._h, N, K, batch, input, output, ctypes.byref(sm),
+                                       ctypes.byref(g), ctypes.byref(ms))
+        if st != _lib.FTDX_OK:
+            return None
+        return {"store_mode": sm.value, "grid": g.value, "ms": ms.value}
+
+    def set_graph_mode(self, enable: bool) -> None:
+        check(self._h, self._L.ftdx_set_graph_mode(self._h, int(bool(enable))),
+              "ftdx_set_graph_mode")
+
+    def graph_count(self) -> int:
+        return int(self._L.ftdx_graph_count(self._h))
+
     def set_profiling(self, enable: bool) -> None:
         check(self._h, self._L.ftdx_set_profiling(self._h, int(bool(enable))), "ftdx_set_profiling")
 

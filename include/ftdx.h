@@ -108,6 +108,37 @@ FTDX_API ftdx_status ftdx_end_herk(ftdx_handle h);
  * Returns FTDX_ERR_TIMEOUT if any bit was set. */
 FTDX_API ftdx_status ftdx_device_status(ftdx_handle h, void* stream, uint32_t* bits);
 
+/* ---- autotuning and graph replay ------------------------------------------
+ * Replace tune_herk / strategy_cache::run_autotune and the direct-HERK graph
+ * cache of the reference (cutlass_gemm_api.cu:1389-1409, 200-315, 1738-1807;
+ * strategy_cache.hpp:504-721).
+ *
+ * The autotuner times every launch strategy (epilogue store mode x number
+ * of persistent CTAs) for a problem shape on the caller's buffers and keeps
+ * the fastest, in memory and appended to a text cache file (one line per
+ * entry: "ftdx-tune 1 <device> <N> <Kp> <batch> <input> <output> <store>
+ * <grid> <ms>").  ftdx_herk(..., tune=1) looks the shape up and tunes on a
+ * miss (only when beta == 0 and the stream is not capturing). */
+
+/* Set the cache file and load its entries.  Malformed lines are skipped and
+ * reported as FTDX_ERR_CACHE (the valid entries are still loaded). */
+FTDX_API ftdx_status ftdx_set_tune_cache(ftdx_handle h, const char* path);
+
+/* Run the strategy sweep now for this shape (C is overwritten; beta = 0). */
+FTDX_API ftdx_status ftdx_tune(ftdx_handle h, const void* A, void* C, int N, int K, int batch,
+                               ftdx_input input, ftdx_output output, void* stream,
+                               int* store_mode, int* grid, float* ms);
+
+/* Query the tuned strategy of a shape (FTDX_ERR_CACHE when there is none). */
+FTDX_API ftdx_status ftdx_lookup_tuned(ftdx_handle h, int N, int K, int batch, ftdx_input input,
+                                       ftdx_output output, int* store_mode, int* grid, float* ms);
+
+/* Graph mode: each distinct call (pointers, sizes, precisions, alpha, beta,
+ * strategy) is captured once into a CUDA graph and replayed afterwards
+ * (4-entry LRU).  Disabling releases the graphs. */
+FTDX_API ftdx_status ftdx_set_graph_mode(ftdx_handle h, int enable);
+FTDX_API int ftdx_graph_count(ftdx_handle h);
+
 /* Kernel timing (no counterpart in the reference; its benches time whole
  * calls).  While enabled, CUDA events are recorded on the caller's stream
  * around every kernel this handle launches.  ftdx_profile_read synchronises,
