@@ -59,6 +59,7 @@ PROTOTYPES = {
                                ctypes.POINTER(_f)]),
     "ftdx_set_graph_mode": (_i, [_vp, _i]),
     "ftdx_graph_count": (_i, [_vp]),
+    "ftdx_set_strategy": (_i, [_vp, _i, _i]),
     "ftdx_profile_read": (_i, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i),
                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i)]),
 }

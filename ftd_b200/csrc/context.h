@@ -29,7 +29,7 @@ struct Plan {
 // Launch strategy of the correlator kernel; chosen by the autotuner.
 struct Strategy {
   int store_mode = 0;  // 0: direct stores, 1: shared-memory staging + bulk copies
-  int grid = 0;        // persistent CTAs (0: one per SM)
+  int grid = 0;        // persistent CTAs (0: one per SM); -1: one CTA per tile (not persistent)
   bool operator==(const Strategy& o) const {
     return store_mode == o.store_mode && grid == o.grid;
   }
@@ -81,6 +81,8 @@ struct ftdx_context {
   size_t z_cap = 0;
   uint32_t* d_status = nullptr;
   std::map<std::tuple<int, int, int>, std::unique_ptr<ftdx::Plan>> plans;  // (N, kblocks, batch)
+  // strategy of untuned calls (ftdx_set_strategy)
+  ftdx::Strategy default_strategy;
   // autotuner
   std::string tune_cache;
   std::map<ftdx::TuneKey, ftdx::TuneEntry> tuned;

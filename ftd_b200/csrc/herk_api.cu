@@ -91,6 +91,7 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   args.status = h->d_status;
   int grid = strat.grid > 0 ? strat.grid : h->sm_count;
   if (grid > h->sm_count) grid = h->sm_count;  // persistent: at most one CTA per SM
+  if (strat.grid < 0) grid = plan->num_tiles;   // one tile per CTA
   if (grid > plan->num_tiles) grid = plan->num_tiles;
   {
     ScopedTimer tm(h, s, 0);
@@ -274,7 +275,7 @@ ftdx_status ftdx_herk(ftdx_handle h, const void* A, void* C, int N, int K, int b
   if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const bool capturing = stream_capturing(s);
-  Strategy strat;
+  Strategy strat = h->default_strategy;
   if (tune) {
     auto it = h->tuned.find(tune_key(h, c));
     if (it != h->tuned.end()) {
@@ -365,5 +366,14 @@ ftdx_status ftdx_set_graph_mode(ftdx_handle h, int enable) {
 }
 
 int ftdx_graph_count(ftdx_handle h) { return h ? int(h->graphs.size()) : -1; }
+
+ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  if (store_mode < 0 || store_mode > 1 || grid < -1)
+    return fail(h, FTDX_ERR_INVALID_ARG, "set_strategy: store_mode %d / grid %d", store_mode,
+                grid);
+  h->default_strategy = Strategy{store_mode, grid};
+  return FTDX_OK;
+}
 
 }  // extern "C"

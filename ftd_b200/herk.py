@@ -133,6 +133,10 @@ class Correlator:
             return None
         return {"store_mode": sm.value, "grid": g.value, "ms": ms.value}
 
+    def set_strategy(self, store_mode: int = 0, grid: int = 0) -> None:
+        """Strategy of untuned calls; grid=-1 is a plain one-tile-per-CTA launch."""
+        check(self._h, self._L.ftdx_set_strategy(self._h, store_mode, grid), "ftdx_set_strategy")
+
     def set_graph_mode(self, enable: bool) -> None:
         check(self._h, self._L.ftdx_set_graph_mode(self._h, int(bool(enable))),
               "ftdx_set_graph_mode")

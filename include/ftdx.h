@@ -139,6 +139,12 @@ FTDX_API ftdx_status ftdx_lookup_tuned(ftdx_handle h, int N, int K, int batch, f
 FTDX_API ftdx_status ftdx_set_graph_mode(ftdx_handle h, int enable);
 FTDX_API int ftdx_graph_count(ftdx_handle h);
 
+/* Strategy for calls that are not tuned (tune = 0, or no cache entry):
+ * store_mode 0 = direct stores, 1 = shared-memory staging + bulk copies;
+ * grid > 0 = that many persistent CTAs (capped at one per SM), 0 = one per
+ * SM, -1 = one CTA per tile (a plain, non-persistent launch). */
+FTDX_API ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid);
+
 /* Kernel timing (no counterpart in the reference; its benches time whole
  * calls).  While enabled, CUDA events are recorded on the caller's stream
  * around every kernel this handle launches.  ftdx_profile_read synchronises,
