@@ -145,6 +145,32 @@ FTDX_API int ftdx_graph_count(ftdx_handle h);
  * SM, -1 = one CTA per tile (a plain, non-persistent launch). */
 FTDX_API ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid);
 
+/* ---- correlation without any allocation -----------------------------------
+ * No counterpart in the reference.  For callers that must not have the
+ * library allocate GPU memory once they run: real-time pipelines that size
+ * every buffer up front and cannot afford a cudaMalloc stalling or failing
+ * mid-observation, and host frameworks whose device memory all comes from
+ * their own pool.  Same result as
+ *   ftdx_herk(h, A, C, N, K, batch, FTDX_IN_INT4, FTDX_COMPUTE_FP8,
+ *             FTDX_OUT_FP32, FTDX_FORMAT_PACKED_TRIANGLE, 1, 0, stream, 0)
+ * (QC int4 in, complex64 packed lower triangles out), but no handle and no
+ * workspace: all scratch lives in one static device array of
+ * FTDX_STATIC_SCRATCH_BYTES that every GPU loading this library holds until
+ * the process exits.  Needed: 1 KiB + 2*N*batch*Kp bytes (Kp = K rounded up
+ * to 128) + 8 bytes per lower-triangle tile of 128 x 128 inputs; larger
+ * problems return FTDX_ERR_CAPACITY (and print the sizes to stderr), e.g.
+ * N = 1024 inputs, K = 1024 samples fits 15 channels per call.  The first
+ * call on a device looks up the array's device address (a one-time set-up);
+ * make that first call before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (other streams, other threads) race
+ * and corrupt each other's results; serialise them.  If status_out is not
+ * NULL the call synchronises `stream` and stores the device status bits
+ * there (FTDX_ERR_TIMEOUT if any is set).  scratch_used (may be NULL)
+ * receives the bytes this problem needs. */
+#define FTDX_STATIC_SCRATCH_BYTES (32u << 20)
+FTDX_API ftdx_status ftdx_herk_static(const void* A, void* C, int N, int K, int batch,
+                                      void* stream, uint32_t* status_out, size_t* scratch_used);
+
 /* Kernel timing (no counterpart in the reference; its benches time whole
  * calls).  While enabled, CUDA events are recorded on the caller's stream
  * around every kernel this handle launches.  ftdx_profile_read synchronises,
