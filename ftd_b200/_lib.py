@@ -31,6 +31,11 @@ class FtdxError(RuntimeError):
         self.status = status
 
 
+class ChannelDesc(ctypes.Structure):
+    _fields_ = [("A", ctypes.c_void_p), ("C", ctypes.c_void_p), ("n_inputs", ctypes.c_int),
+                ("K", ctypes.c_int), ("lda", ctypes.c_int64), ("active", ctypes.c_void_p)]
+
+
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("verbosity", ctypes.c_int),
                 ("tune_cache", ctypes.c_char_p), ("reserved", ctypes.c_int * 8)]
@@ -49,6 +54,7 @@ PROTOTYPES = {
     "ftdx_last_error": (ctypes.c_char_p, [_vp]),
     "ftdx_herk": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _f, _f, _vp, _i]),
     "ftdx_init_herk": (_i, [_vp, _i, _i, _i, _vp]),
+    "ftdx_herk_batched_v": (_i, [_vp, ctypes.c_void_p, _i, _i, _f, _f, _vp, _i]),
     "ftdx_end_herk": (_i, [_vp]),
     "ftdx_device_status": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32)]),
     "ftdx_set_profiling": (_i, [_vp, _i]),

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <list>
 #include <map>
 #include <memory>
@@ -81,6 +82,7 @@ struct ftdx_context {
   size_t z_cap = 0;
   uint32_t* d_status = nullptr;
   std::map<std::tuple<int, int, int>, std::unique_ptr<ftdx::Plan>> plans;  // (N, kblocks, batch)
+  std::map<uint64_t, std::shared_ptr<void>> vplans;  // batched-call plans by fingerprint
   // strategy of untuned calls (ftdx_set_strategy)
   ftdx::Strategy default_strategy;
   // autotuner
@@ -127,5 +129,14 @@ struct ScopedTimer {
 
 void release_graphs(ftdx_handle h);
 void load_tune_cache(ftdx_handle h);
+
+// Autotuning and graph replay shared by the correlator entry points.
+using LaunchFn = std::function<ftdx_status(const Strategy&, cudaStream_t)>;
+std::vector<Strategy> default_candidates(ftdx_handle h, bool fp32_out);
+ftdx_status tune_sweep(ftdx_handle h, const LaunchFn& launch, const std::vector<Strategy>& cands,
+                       cudaStream_t s, TuneEntry* best);
+void record_tuned(ftdx_handle h, const TuneKey& k, const TuneEntry& e);
+ftdx_status graph_launch(ftdx_handle h, const GraphKey& key,
+                         const std::function<ftdx_status(cudaStream_t)>& launch, cudaStream_t s);
 
 }  // namespace ftdx

@@ -105,7 +105,7 @@ ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t 
     chans[c].kblocks = kblocks;
     chans[c].row0 = int64_t(c) * N;
     chans[c].out0 = int64_t(c) * (int64_t(N) * (N + 1) / 2);
-    chans[c].reserved = 0;
+    chans[c].out_ptr = 0;
     for (int ti = 0; ti < nb; ++ti)
       for (int tj = 0; tj <= ti; ++tj) tiles.push_back(TileDesc{c, uint16_t(ti), uint16_t(tj)});
   }
@@ -237,6 +237,7 @@ ftdx_status ftdx_destroy(ftdx_handle h) {
   cudaDeviceSynchronize();
   release_graphs(h);
   h->plans.clear();
+  h->vplans.clear();
   for (auto& t : h->timed) {
     cudaEventDestroy(t.a);
     cudaEventDestroy(t.b);

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <sstream>
 
 #include "context.h"
@@ -106,17 +107,90 @@ TuneKey tune_key(ftdx_handle h, const HerkCall& c) {
                  int(c.output)};
 }
 
-std::vector<Strategy> candidates(ftdx_handle h, const HerkCall& c) {
+// Times every candidate strategy on the caller's buffers (beta must be 0, so
+// repeated runs leave C as one run would) and records the fastest.
+ftdx_status run_tune(ftdx_handle h, const HerkCall& c, cudaStream_t s, TuneEntry* out) {
+  if (c.beta != 0.f)
+    return fail(h, FTDX_ERR_INVALID_ARG, "tuning needs beta == 0 (C is overwritten)");
+  const Plan* plan = nullptr;
+  ftdx_status st = prepare(h, c, s, &plan);
+  if (st != FTDX_OK) return st;
+  TuneEntry best;
+  st = tune_sweep(
+      h, [&](const Strategy& cand, cudaStream_t ss) { return launch_all(h, c, cand, ss); },
+      default_candidates(h, c.output == FTDX_OUT_FP32), s, &best);
+  if (st != FTDX_OK) return st;
+  record_tuned(h, tune_key(h, c), best);
+  if (out) *out = best;
+  return FTDX_OK;
+}
+
+ftdx_status run_graph(ftdx_handle h, const HerkCall& c, const Strategy& strat, cudaStream_t s) {
+  const GraphKey key{c.A, c.C, c.N, c.K, c.batch, int(c.input), int(c.output), c.alpha, c.beta,
+                     strat.store_mode, strat.grid};
+  return graph_launch(
+      h, key,
+      [&](cudaStream_t ss) {
+        const Plan* plan = nullptr;
+        return ss == h->capture_stream ? launch_all(h, c, strat, ss) : prepare(h, c, ss, &plan);
+      },
+      s);
+}
+
+}  // namespace
+
+std::vector<Strategy> default_candidates(ftdx_handle h, bool fp32_out) {
   std::vector<Strategy> v;
   const int grids[2] = {h->sm_count, h->sm_count - h->sm_count / 8};
   for (int g : grids) {
     v.push_back(Strategy{0, g});
-    if (c.output == FTDX_OUT_FP32) v.push_back(Strategy{1, g});
+    if (fp32_out) v.push_back(Strategy{1, g});
   }
   return v;
 }
 
-void append_tune_cache(ftdx_handle h, const TuneKey& k, const TuneEntry& e) {
+ftdx_status tune_sweep(ftdx_handle h, const LaunchFn& launch, const std::vector<Strategy>& cands,
+                       cudaStream_t s, TuneEntry* best_out) {
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    return fail(h, FTDX_ERR_CUDA, "tuner events");
+  const bool prof = h->profiling;
+  h->profiling = false;
+  ftdx_status st = FTDX_OK;
+  TuneEntry best;
+  best.ms = -1.f;
+  for (const Strategy& cand : cands) {
+    for (int w = 0; w < 2 && st == FTDX_OK; ++w) st = launch(cand, s);
+    if (st != FTDX_OK) break;
+    cudaEventRecord(e0, s);
+    const int reps = 3;
+    for (int r = 0; r < reps && st == FTDX_OK; ++r) st = launch(cand, s);
+    cudaEventRecord(e1, s);
+    if (st != FTDX_OK) break;
+    float ms = 0.f;
+    cudaError_t ce = cudaEventSynchronize(e1);
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+    if (ce != cudaSuccess) {
+      st = cuda_fail(h, ce, "tuner timing");
+      break;
+    }
+    ms /= reps;
+    if (h->verbosity > 1)
+      fprintf(stderr, "ftdx tune: store=%d grid=%d %.4f ms\n", cand.store_mode, cand.grid, ms);
+    if (best.ms < 0.f || ms < best.ms) best = TuneEntry{cand, ms};
+  }
+  h->profiling = prof;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st == FTDX_OK && best_out) *best_out = best;
+  return st;
+}
+
+void record_tuned(ftdx_handle h, const TuneKey& k, const TuneEntry& e) {
+  h->tuned[k] = e;
+  if (h->verbosity > 0)
+    fprintf(stderr, "ftdx tuned n=%d kp=%d batch=%d -> store=%d grid=%d (%.4f ms)\n", k.n, k.kp,
+            k.batch, e.st.store_mode, e.st.grid, e.ms);
   if (h->tune_cache.empty()) return;
   FILE* f = fopen(h->tune_cache.c_str(), "a");
   if (!f) {
@@ -129,61 +203,12 @@ void append_tune_cache(ftdx_handle h, const TuneKey& k, const TuneEntry& e) {
   fclose(f);
 }
 
-// Times every candidate strategy on the caller's buffers (beta must be 0, so
-// repeated runs leave C as one run would) and records the fastest.
-ftdx_status run_tune(ftdx_handle h, const HerkCall& c, cudaStream_t s, TuneEntry* out) {
-  if (c.beta != 0.f)
-    return fail(h, FTDX_ERR_INVALID_ARG, "tuning needs beta == 0 (C is overwritten)");
-  const Plan* plan = nullptr;
-  ftdx_status st = prepare(h, c, s, &plan);
-  if (st != FTDX_OK) return st;
-  cudaEvent_t e0, e1;
-  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
-    return fail(h, FTDX_ERR_CUDA, "tuner events");
-  const bool prof = h->profiling;
-  h->profiling = false;
-  TuneEntry best;
-  best.ms = -1.f;
-  for (const Strategy& cand : candidates(h, c)) {
-    for (int w = 0; w < 2 && st == FTDX_OK; ++w) st = launch_all(h, c, cand, s);
-    if (st != FTDX_OK) break;
-    cudaEventRecord(e0, s);
-    const int reps = 3;
-    for (int r = 0; r < reps && st == FTDX_OK; ++r) st = launch_all(h, c, cand, s);
-    cudaEventRecord(e1, s);
-    if (st != FTDX_OK) break;
-    float ms = 0.f;
-    cudaError_t ce = cudaEventSynchronize(e1);
-    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
-    if (ce != cudaSuccess) {
-      st = cuda_fail(h, ce, "tuner timing");
-      break;
-    }
-    ms /= reps;
-    if (h->verbosity > 1)
-      fprintf(stderr, "ftdx tune N=%d K=%d batch=%d: store=%d grid=%d %.4f ms\n", c.N, c.K,
-              c.batch, cand.store_mode, cand.grid, ms);
-    if (best.ms < 0.f || ms < best.ms) best = TuneEntry{cand, ms};
-  }
-  h->profiling = prof;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (st != FTDX_OK) return st;
-  const TuneKey k = tune_key(h, c);
-  h->tuned[k] = best;
-  append_tune_cache(h, k, best);
-  if (h->verbosity > 0)
-    fprintf(stderr, "ftdx tuned N=%d K=%d batch=%d -> store=%d grid=%d (%.4f ms)\n", c.N, c.K,
-            c.batch, best.st.store_mode, best.st.grid, best.ms);
-  if (out) *out = best;
-  return FTDX_OK;
-}
-
-// Replays {promotion, correlator} as one CUDA graph per call signature
-// (least-recently-used cache of kGraphCacheSize entries).
-ftdx_status run_graph(ftdx_handle h, const HerkCall& c, const Strategy& strat, cudaStream_t s) {
-  const GraphKey key{c.A, c.C, c.N, c.K, c.batch, int(c.input), int(c.output), c.alpha, c.beta,
-                     strat.store_mode, strat.grid};
+// Replays a launch sequence as one CUDA graph per key (least-recently-used
+// cache of kGraphCacheSize entries).  `launch` is first called on the
+// caller's stream outside capture to allocate what it needs, then on the
+// capture stream.
+ftdx_status graph_launch(ftdx_handle h, const GraphKey& key,
+                         const std::function<ftdx_status(cudaStream_t)>& launch, cudaStream_t s) {
   for (auto it = h->graphs.begin(); it != h->graphs.end(); ++it) {
     if (it->key == key) {
       h->graphs.splice(h->graphs.begin(), h->graphs, it);
@@ -191,14 +216,13 @@ ftdx_status run_graph(ftdx_handle h, const HerkCall& c, const Strategy& strat, c
       return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "cudaGraphLaunch");
     }
   }
-  const Plan* plan = nullptr;
-  ftdx_status st = prepare(h, c, s, &plan);  // allocate before capturing
+  ftdx_status st = launch(s == h->capture_stream ? nullptr : s);  // allocation pass
   if (st != FTDX_OK) return st;
   GraphEntry ge;
   ge.key = key;
   cudaError_t e = cudaStreamBeginCapture(h->capture_stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamBeginCapture");
-  st = launch_all(h, c, strat, h->capture_stream);
+  st = launch(h->capture_stream);
   e = cudaStreamEndCapture(h->capture_stream, &ge.graph);
   if (st != FTDX_OK) {
     if (ge.graph) cudaGraphDestroy(ge.graph);
@@ -219,8 +243,6 @@ ftdx_status run_graph(ftdx_handle h, const HerkCall& c, const Strategy& strat, c
   e = cudaGraphLaunch(h->graphs.front().exec, s);
   return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "cudaGraphLaunch");
 }
-
-}  // namespace
 
 void release_graphs(ftdx_handle h) {
   for (auto& g : h->graphs) {
@@ -248,7 +270,7 @@ void load_tune_cache(ftdx_handle h) {
     TuneEntry e;
     if (!(is >> magic >> ver >> dev >> k.n >> k.kp >> k.batch >> k.input >> k.output >>
           e.st.store_mode >> e.st.grid >> e.ms) ||
-        magic != "ftdx-tune" || ver != 1 || k.n < 1 || k.kp < 1 || k.batch < 1 ||
+        magic != "ftdx-tune" || ver != 1 || (k.n < 1 && k.n != -1) || k.kp < 1 || k.batch < 1 ||
         e.st.store_mode < 0 || e.st.store_mode > 1 || e.st.grid < 0 || !(e.ms >= 0.f)) {
       ++h->cache_bad_lines;
       continue;
@@ -310,6 +332,7 @@ ftdx_status ftdx_end_herk(ftdx_handle h) {
   h->z = nullptr;
   h->z_cap = 0;
   h->plans.clear();
+  h->vplans.clear();
   return FTDX_OK;
 }
 

@@ -123,6 +123,53 @@ __global__ void __launch_bounds__(256) fp16_to_planes_kernel(const __half2* __re
   }
 }
 
+// Batched promotion with row gathering (flagged inputs) and per-channel K.
+// Block (x, y): channel y, rows [x * rows_per_block, ...).  One thread
+// converts 16 samples of one row.
+__global__ void __launch_bounds__(256) gather_qc_to_planes_kernel(const GatherDesc* __restrict__ gd,
+                                                                  uint8_t* __restrict__ z,
+                                                                  int64_t total_rows, int Kp,
+                                                                  int rows_per_block) {
+  const GatherDesc g = gd[blockIdx.y];
+  const int r0 = blockIdx.x * rows_per_block;
+  if (r0 >= g.n) return;
+  const int nrows = min(rows_per_block, g.n - r0);
+  const int kpc = (g.k + kStageK - 1) / kStageK * kStageK;  // this channel's padded K
+  const int chunks = kpc >> 4;
+  const int64_t plane = total_rows * int64_t(Kp);
+  const bool vec = ((g.lda & 15) == 0) && ((reinterpret_cast<uintptr_t>(g.a) & 15) == 0);
+  for (int l = threadIdx.x; l < nrows * chunks; l += blockDim.x) {
+    const int rl = l / chunks;
+    const int t0 = (l - rl * chunks) << 4;
+    const int r = r0 + rl;
+    const int64_t src_row = g.active ? int64_t(__ldg(g.active + r)) : int64_t(r);
+    const uint8_t* src = g.a + src_row * g.lda + t0;
+    uint32_t w[4];
+    if (vec && t0 + 16 <= g.k) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(src));
+      w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        uint32_t acc = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int t = t0 + 4 * q + b;
+          const uint32_t byte = (t < g.k) ? uint32_t(__ldg(src + 4 * q + b)) : 0u;
+          acc |= byte << (8 * b);
+        }
+        w[q] = acc;
+      }
+    }
+    uint32_t re[4], im[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) qc4_to_e4m3(w[q], re[q], im[q]);
+    uint8_t* dst = z + (g.row0 + r) * int64_t(Kp) + t0;
+    *reinterpret_cast<uint4*>(dst) = make_uint4(re[0], re[1], re[2], re[3]);
+    *reinterpret_cast<uint4*>(dst + plane) = make_uint4(im[0], im[1], im[2], im[3]);
+  }
+}
+
 // ------------------------------------------------------------------ HERK
 // Output element stores.  Streaming (.cs) stores: the triangle is written
 // once and never re-read by this kernel.
@@ -326,7 +373,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       const int j = jw + lane;
       const int ib = int(td.ti) * kTile;
       const uint32_t tb = tmem_base + (uint32_t(q * 32) << 16) + uint32_t(acc * kAccCols);
-      Out2* outc = out + cd.out0;
+      Out2* outc = cd.out_ptr ? reinterpret_cast<Out2*>(cd.out_ptr) : out + cd.out0;
       if (kBulkOut && args.bulk_store && plain && td.ti != td.tj && ib + kTile <= n) {
         // Interior tile: stage kStgRows row segments (128 consecutive packed
         // elements each) in shared memory, then one bulk copy per row.  A
@@ -437,6 +484,14 @@ cudaError_t launch_fp16_to_planes(const void* a16, uint8_t* z, int64_t rows, int
   const int64_t blocks = (rows + rpb - 1) / rpb;
   fp16_to_planes_kernel<<<unsigned(blocks), 256, 0, s>>>(static_cast<const __half2*>(a16), z,
                                                          rows, K, Kp, rpb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_qc_to_planes(const GatherDesc* g, int nch, int max_n, uint8_t* z,
+                                       int64_t total_rows, int Kp, cudaStream_t s) {
+  const int rpb = rows_per_block(Kp >> 4);
+  const dim3 grid(unsigned((max_n + rpb - 1) / rpb), unsigned(nch));
+  gather_qc_to_planes_kernel<<<grid, 256, 0, s>>>(g, z, total_rows, Kp, rpb);
   return cudaGetLastError();
 }
 

@@ -46,13 +46,25 @@ struct TileDesc {
 };
 
 // Per-channel geometry.  row0 is the channel's first row in each plane of Z;
-// out0 is the channel's first packed-triangle element in the output.
+// the channel's packed triangle starts at out_ptr when it is non-zero (a
+// device address), else at element out0 of HerkArgs::out.
 struct ChanDesc {
   int32_t n;
   int32_t kblocks;
   int64_t row0;
   int64_t out0;
-  int64_t reserved;
+  int64_t out_ptr;
+};
+
+// One channel of a batched call with its own input geometry: the promotion
+// pass gathers rows active[0..n) (or rows 0..n) of a [rows][lda] QC block.
+struct GatherDesc {
+  const uint8_t* a;
+  const int32_t* active;  // nullptr: all rows
+  int64_t lda;
+  int64_t row0;           // first row in each plane of Z
+  int32_t n;
+  int32_t k;
 };
 
 struct HerkArgs {
@@ -73,6 +85,11 @@ cudaError_t launch_qc_to_planes(const uint8_t* qc, uint8_t* z, int64_t rows, int
                                 cudaStream_t s);
 cudaError_t launch_fp16_to_planes(const void* a16, uint8_t* z, int64_t rows, int K, int Kp,
                                   cudaStream_t s);
+// Gathered promotion for `nch` channels with a common plane pitch Kp
+// (>= every channel's K rounded up to 128); each channel's rows are
+// zero-padded from its K up to its own K rounded up to 128.
+cudaError_t launch_gather_qc_to_planes(const GatherDesc* g, int nch, int max_n, uint8_t* z,
+                                       int64_t total_rows, int Kp, cudaStream_t s);
 cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s);
 
 }  // namespace ftdx

@@ -101,6 +101,23 @@ class Correlator:
                                format, float(alpha), float(beta), _stream(stream), int(bool(tune)))
         check(self._h, st, "ftdx_herk")
 
+    def herk_batched_v(self, channels, output: int = OUT_FP32, alpha: float = 1.0,
+                       beta: float = 0.0, stream=None, tune: bool = False) -> None:
+        """Uneven / flagged channels in one launch.  `channels` is a list of dicts
+        with keys A, C, n_inputs, K and optionally lda, active (device buffers)."""
+        arr = (_lib.ChannelDesc * len(channels))()
+        for k, ch in enumerate(channels):
+            arr[k].A = _ptr(ch["A"])
+            arr[k].C = _ptr(ch["C"])
+            arr[k].n_inputs = int(ch["n_inputs"])
+            arr[k].K = int(ch["K"])
+            arr[k].lda = int(ch.get("lda", 0))
+            arr[k].active = _ptr(ch.get("active"))
+        st = self._L.ftdx_herk_batched_v(self._h, ctypes.cast(arr, ctypes.c_void_p), len(channels),
+                                         output, float(alpha), float(beta), _stream(stream),
+                                         int(bool(tune)))
+        check(self._h, st, "ftdx_herk_batched_v")
+
     def init_herk(self, N: int, K: int, batch: int, stream=None) -> None:
         check(self._h, self._L.ftdx_init_herk(self._h, N, K, batch, _stream(stream)),
               "ftdx_init_herk")

@@ -97,6 +97,31 @@ FTDX_API ftdx_status ftdx_herk(ftdx_handle h, const void* A, void* C, int N, int
                       ftdx_input input, ftdx_compute compute, ftdx_output output,
                       ftdx_format format, float alpha, float beta, void* stream, int tune);
 
+/* ---- uneven, flagged channels in one launch --------------------------------
+ * No single counterpart in the reference, which batches only uniform
+ * (N, K, batch) problems and loops over channel groups in its callers
+ * (lib/visibility_pipeline.cu:268-277).  One call correlates n_chans
+ * channels, each with its own QC rows, integration length and output:
+ * channel c's output (packed lower triangle over its n_inputs active inputs,
+ * in the order of `active`) is
+ *   C_c = alpha * A_c A_c^H + beta * C_c,  A_c = rows active[0..n_inputs) of
+ *   the [rows][lda] QC block at A (rows 0..n_inputs-1 when active == NULL).
+ * All channels run in one persistent correlator launch (longest K first).
+ * A plan is built on the first call with a given descriptor set (pointers
+ * and sizes; the contents of `active` are read on every call) and cached. */
+typedef struct ftdx_channel_desc {
+  const void* A;           /* QC int4 bytes of this channel (device) */
+  void* C;                 /* its packed triangle, n_inputs*(n_inputs+1)/2 complex (device) */
+  int n_inputs;            /* inputs correlated (active inputs after flagging) */
+  int K;                   /* time samples, >= 1 */
+  int64_t lda;             /* row pitch of A in bytes (0: K) */
+  const int32_t* active;   /* device array of n_inputs row indices, or NULL */
+} ftdx_channel_desc;
+
+FTDX_API ftdx_status ftdx_herk_batched_v(ftdx_handle h, const ftdx_channel_desc* chans,
+                                         int n_chans, ftdx_output output, float alpha,
+                                         float beta, void* stream, int tune);
+
 /* Pre-size the workspace for problems up to (N, K, batch) so that later
  * ftdx_herk calls allocate nothing (required before graph capture).
  * Replaces CutlassComplexGemm::init_herk / end_herk (cutlass_gemm_api.h:617-624). */
