@@ -19,8 +19,8 @@ STATUS_NAMES = {
 }
 
 # enum values (include/ftdx.h)
-IN_FP16, IN_INT4 = 0, 1
-COMPUTE_FP8, COMPUTE_FP6, COMPUTE_FP4 = 0, 1, 2
+IN_FP16, IN_INT4, IN_FP32 = 0, 1, 2
+COMPUTE_FP8, COMPUTE_FP6, COMPUTE_FP4, COMPUTE_FP8_SPLIT = 0, 1, 2, 3
 OUT_FP16, OUT_FP32 = 0, 1
 FORMAT_PACKED_TRIANGLE = 0
 
@@ -54,6 +54,7 @@ PROTOTYPES = {
     "ftdx_last_error": (ctypes.c_char_p, [_vp]),
     "ftdx_herk": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _f, _f, _vp, _i]),
     "ftdx_init_herk": (_i, [_vp, _i, _i, _i, _vp]),
+    "ftdx_herk_kahan": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
     "ftdx_herk_batched_v": (_i, [_vp, ctypes.c_void_p, _i, _i, _f, _f, _vp, _i]),
     "ftdx_end_herk": (_i, [_vp]),
     "ftdx_device_status": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32)]),

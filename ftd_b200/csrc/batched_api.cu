@@ -142,7 +142,7 @@ ftdx_status launch_v(ftdx_handle h, const VCall& c, const Strategy& strat, cudaS
   CUtensorMap tmZ;
   st = encode_planes_map(h, h->z, p->rows, p->kp, &tmZ);
   if (st != FTDX_OK) return st;
-  HerkArgs args;
+  HerkArgs args = herk_args_default();
   args.tiles = p->d_tiles;
   args.chans = p->d_chans;
   args.num_tiles = p->num_tiles;

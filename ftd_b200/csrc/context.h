@@ -80,6 +80,9 @@ struct ftdx_context {
   // FP8 operand workspace (grown on demand, or pre-sized by ftdx_init_herk)
   uint8_t* z = nullptr;
   size_t z_cap = 0;
+  // per-channel scales of float inputs: qscale[batch], out_scale[batch], amax[batch]
+  uint8_t* aux = nullptr;
+  size_t aux_cap = 0;
   uint32_t* d_status = nullptr;
   std::map<std::tuple<int, int, int>, std::unique_ptr<ftdx::Plan>> plans;  // (N, kblocks, batch)
   std::map<uint64_t, std::shared_ptr<void>> vplans;  // batched-call plans by fingerprint
@@ -111,6 +114,7 @@ ftdx_status fail(ftdx_handle h, ftdx_status s, const char* fmt, ...);
 ftdx_status cuda_fail(ftdx_handle h, cudaError_t e, const char* what);
 bool stream_capturing(cudaStream_t s);
 ftdx_status ensure_workspace(ftdx_handle h, size_t bytes, cudaStream_t s);
+ftdx_status ensure_aux(ftdx_handle h, size_t bytes, cudaStream_t s);
 ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
                      const Plan** out);
 ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t Kp,

@@ -82,6 +82,27 @@ ftdx_status ensure_workspace(ftdx_handle h, size_t bytes, cudaStream_t s) {
   return FTDX_OK;
 }
 
+ftdx_status ensure_aux(ftdx_handle h, size_t bytes, cudaStream_t s) {
+  if (bytes <= h->aux_cap) return FTDX_OK;
+  if (stream_capturing(s))
+    return fail(h, FTDX_ERR_CAPACITY, "scale buffer needed while capturing; call once first");
+  if (h->aux) {
+    cudaDeviceSynchronize();
+    cudaFree(h->aux);
+    h->aux = nullptr;
+    h->aux_cap = 0;
+    release_graphs(h);
+  }
+  cudaError_t e = cudaMalloc(&h->aux, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(h, FTDX_ERR_ALLOC, "cudaMalloc(%zu) for channel scales: %s", bytes,
+                cudaGetErrorString(e));
+  }
+  h->aux_cap = bytes;
+  return FTDX_OK;
+}
+
 // Lower-triangle tile list for `batch` channels of N inputs, channel-major so
 // that concurrently running CTAs share a channel's operand in L2.
 ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
@@ -244,6 +265,7 @@ ftdx_status ftdx_destroy(ftdx_handle h) {
   }
   for (auto e : h->event_pool) cudaEventDestroy(e);
   if (h->z) cudaFree(h->z);
+  if (h->aux) cudaFree(h->aux);
   if (h->d_status) cudaFree(h->d_status);
   if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
   delete h;

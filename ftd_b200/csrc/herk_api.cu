@@ -23,22 +23,30 @@ struct HerkCall {
   ftdx_input input;
   ftdx_output output;
   float alpha, beta;
+  ftdx_compute compute = FTDX_COMPUTE_FP8;
+  void* comp = nullptr;  // Kahan compensation buffer (ftdx_herk_kahan)
 };
+
+bool is_split(const HerkCall& c) { return c.compute == FTDX_COMPUTE_FP8_SPLIT; }
 
 ftdx_status validate(ftdx_handle h, const HerkCall& c, ftdx_compute compute, ftdx_format format) {
   if (!c.A || !c.C) return fail(h, FTDX_ERR_INVALID_ARG, "herk: null A or C");
   if (c.N < 1 || c.K < 1 || c.batch < 1)
     return fail(h, FTDX_ERR_INVALID_ARG, "herk: N, K and batch must be >= 1 (got %d, %d, %d)",
                 c.N, c.K, c.batch);
-  if (c.input != FTDX_IN_INT4 && c.input != FTDX_IN_FP16)
+  if (c.input != FTDX_IN_INT4 && c.input != FTDX_IN_FP16 && c.input != FTDX_IN_FP32)
     return fail(h, FTDX_ERR_INVALID_ARG, "herk: bad input precision %d", int(c.input));
   if (c.output != FTDX_OUT_FP32 && c.output != FTDX_OUT_FP16)
     return fail(h, FTDX_ERR_INVALID_ARG, "herk: bad output precision %d", int(c.output));
   if (format != FTDX_FORMAT_PACKED_TRIANGLE)
     return fail(h, FTDX_ERR_INVALID_ARG, "herk: only the packed triangle format exists");
-  if (compute != FTDX_COMPUTE_FP8)
+  if (compute == FTDX_COMPUTE_FP8_SPLIT && c.input != FTDX_IN_FP32)
+    return fail(h, FTDX_ERR_INVALID_ARG, "herk: split FP8 needs FP32 input");
+  if (compute != FTDX_COMPUTE_FP8 && compute != FTDX_COMPUTE_FP8_SPLIT)
     return fail(h, FTDX_ERR_UNSUPPORTED, "herk: compute precision %d not implemented for "
                 "this entry point", int(compute));
+  if (c.input == FTDX_IN_FP32 && (reinterpret_cast<uintptr_t>(c.A) & 7) != 0)
+    return fail(h, FTDX_ERR_INVALID_ARG, "herk: FP32 complex A must be 8-byte aligned");
   if ((reinterpret_cast<uintptr_t>(c.C) & (c.output == FTDX_OUT_FP32 ? 7 : 3)) != 0)
     return fail(h, FTDX_ERR_INVALID_ARG, "herk: C is not aligned to one complex element");
   if (c.input == FTDX_IN_FP16 && (reinterpret_cast<uintptr_t>(c.A) & 3) != 0)
@@ -54,9 +62,14 @@ ftdx_status validate(ftdx_handle h, const HerkCall& c, ftdx_compute compute, ftd
 // Workspace and tile plan for a call; allocates, so never while capturing.
 ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan** plan) {
   const int64_t Kp = round_up(c.K, kStageK);
+  const int64_t zpitch = is_split(c) ? 2 * Kp : Kp;
   const int64_t rows = int64_t(c.N) * c.batch;
-  ftdx_status st = ensure_workspace(h, size_t(2 * rows * Kp), s);
+  ftdx_status st = ensure_workspace(h, size_t(2 * rows * zpitch), s);
   if (st != FTDX_OK) return st;
+  if (c.input == FTDX_IN_FP32) {
+    st = ensure_aux(h, size_t(12) * size_t(c.batch) + 256, s);
+    if (st != FTDX_OK) return st;
+  }
   return get_plan(h, c.N, int(Kp / kStageK), c.batch, s, plan);
 }
 
@@ -66,20 +79,27 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   ftdx_status st = prepare(h, c, s, &plan);
   if (st != FTDX_OK) return st;
   const int64_t Kp = round_up(c.K, kStageK);
+  const int64_t zpitch = is_split(c) ? 2 * Kp : Kp;
   const int64_t rows = int64_t(c.N) * c.batch;
+  float* qscale = reinterpret_cast<float*>(h->aux);
+  float* out_scale = qscale + c.batch;
+  uint32_t* amax = reinterpret_cast<uint32_t*>(out_scale + c.batch);
   cudaError_t e;
   {
     ScopedTimer tm(h, s, 1);
     if (c.input == FTDX_IN_INT4)
       e = launch_qc_to_planes(static_cast<const uint8_t*>(c.A), h->z, rows, c.K, int(Kp), s);
-    else
+    else if (c.input == FTDX_IN_FP16)
       e = launch_fp16_to_planes(c.A, h->z, rows, c.K, int(Kp), s);
+    else
+      e = launch_float_to_planes(c.A, h->z, rows, c.K, int(Kp), int(zpitch), c.N, c.batch,
+                                 is_split(c) ? 1 : 0, qscale, out_scale, amax, h->sm_count, s);
   }
   if (e != cudaSuccess) return cuda_fail(h, e, "operand promotion launch");
   CUtensorMap tmZ;
-  st = encode_planes_map(h, h->z, rows, Kp, &tmZ);
+  st = encode_planes_map(h, h->z, rows, zpitch, &tmZ);
   if (st != FTDX_OK) return st;
-  HerkArgs args;
+  HerkArgs args = herk_args_default();
   args.tiles = plan->d_tiles;
   args.chans = plan->d_chans;
   args.num_tiles = plan->num_tiles;
@@ -90,6 +110,17 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   args.alpha = c.alpha;
   args.beta = c.beta;
   args.status = h->d_status;
+  if (c.input == FTDX_IN_FP32) args.chan_scale = out_scale;
+  if (is_split(c)) {  // (hi, hi) + (hi, lo) + (lo, hi)
+    const int kb = int(Kp / kStageK);
+    args.nseg = 3;
+    args.seg_a[0] = 0, args.seg_a[1] = 0, args.seg_a[2] = kb;
+    args.seg_b[0] = 0, args.seg_b[1] = kb, args.seg_b[2] = 0;
+  }
+  if (c.comp) {
+    args.kahan = 1;
+    args.out2 = c.comp;
+  }
   int grid = strat.grid > 0 ? strat.grid : h->sm_count;
   if (grid > h->sm_count) grid = h->sm_count;  // persistent: at most one CTA per SM
   if (strat.grid < 0) grid = plan->num_tiles;   // one tile per CTA
@@ -103,8 +134,8 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
 }
 
 TuneKey tune_key(ftdx_handle h, const HerkCall& c) {
-  return TuneKey{h->device_name, c.N, int(round_up(c.K, kStageK)), c.batch, int(c.input),
-                 int(c.output)};
+  return TuneKey{h->device_name, c.N, int(round_up(c.K, kStageK)), c.batch,
+                 int(c.input) | (int(c.compute) << 4) | (c.comp ? 256 : 0), int(c.output)};
 }
 
 // Times every candidate strategy on the caller's buffers (beta must be 0, so
@@ -126,8 +157,9 @@ ftdx_status run_tune(ftdx_handle h, const HerkCall& c, cudaStream_t s, TuneEntry
 }
 
 ftdx_status run_graph(ftdx_handle h, const HerkCall& c, const Strategy& strat, cudaStream_t s) {
-  const GraphKey key{c.A, c.C, c.N, c.K, c.batch, int(c.input), int(c.output), c.alpha, c.beta,
-                     strat.store_mode, strat.grid};
+  const GraphKey key{c.A, c.C, c.N, c.K, c.batch,
+                     int(c.input) | (int(c.compute) << 4) | (c.comp ? 256 : 0), int(c.output),
+                     c.alpha, c.beta, strat.store_mode, strat.grid};
   return graph_launch(
       h, key,
       [&](cudaStream_t ss) {
@@ -290,7 +322,8 @@ ftdx_status ftdx_herk(ftdx_handle h, const void* A, void* C, int N, int K, int b
                       ftdx_input input, ftdx_compute compute, ftdx_output output,
                       ftdx_format format, float alpha, float beta, void* stream, int tune) {
   if (!h) return FTDX_ERR_INVALID_ARG;
-  const HerkCall c{A, C, N, K, batch, input, output, alpha, beta};
+  HerkCall c{A, C, N, K, batch, input, output, alpha, beta};
+  c.compute = compute;
   ftdx_status st = validate(h, c, compute, format);
   if (st != FTDX_OK) return st;
   cudaError_t e = cudaSetDevice(h->device);
@@ -389,6 +422,27 @@ ftdx_status ftdx_set_graph_mode(ftdx_handle h, int enable) {
 }
 
 int ftdx_graph_count(ftdx_handle h) { return h ? int(h->graphs.size()) : -1; }
+
+ftdx_status ftdx_herk_kahan(ftdx_handle h, const void* A, void* sum, void* comp, int N, int K,
+                            int batch, ftdx_input input, ftdx_compute compute, void* stream) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  if (!comp || comp == sum)
+    return fail(h, FTDX_ERR_INVALID_ARG, "kahan: need a separate compensation buffer");
+  if ((reinterpret_cast<uintptr_t>(comp) & 7) != 0)
+    return fail(h, FTDX_ERR_INVALID_ARG, "kahan: compensation buffer misaligned");
+  HerkCall c{A, sum, N, K, batch, input, FTDX_OUT_FP32, 1.f, 0.f};
+  c.compute = compute;
+  c.comp = comp;
+  ftdx_status st = validate(h, c, compute, FTDX_FORMAT_PACKED_TRIANGLE);
+  if (st != FTDX_OK) return st;
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+  // Read-modify-write of sum and compensation: no tuning sweep (it would
+  // accumulate the same dump several times); direct stores only.
+  Strategy strat = h->default_strategy;
+  strat.store_mode = 0;
+  return launch_all(h, c, strat, static_cast<cudaStream_t>(stream));
+}
 
 ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid) {
   if (!h) return FTDX_ERR_INVALID_ARG;

@@ -247,19 +247,25 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
         const int32_t rowJ = int32_t(cd.row0 + int64_t(td.tj) * kTile);
         const int32_t rowI = int32_t(cd.row0 + int64_t(td.ti) * kTile);
         const bool diag = td.ti == td.tj;  // i block == j block: load it once
-        for (int kb = 0; kb < cd.kblocks; ++kb) {
+        const int nkb = cd.kblocks * args.nseg;
+        for (int kb = 0; kb < nkb; ++kb) {
           if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
             atomicOr(args.status, kStatusTimeoutProducer);
             ok = false;
             break;
           }
-          const int32_t k0 = kb * kStageK;
-          mbar_arrive_expect_tx(full_bar(stage), diag ? 2 * kPlaneBytes : kStageBytes);
-          tma_load_3d(plane_addr(stage, 0), &tmZ, k0, rowJ, 0, full_bar(stage));
-          tma_load_3d(plane_addr(stage, 1), &tmZ, k0, rowJ, 1, full_bar(stage));
-          if (!diag) {
-            tma_load_3d(plane_addr(stage, 2), &tmZ, k0, rowI, 0, full_bar(stage));
-            tma_load_3d(plane_addr(stage, 3), &tmZ, k0, rowI, 1, full_bar(stage));
+          const int seg = kb / cd.kblocks;
+          const int kk = kb - seg * cd.kblocks;
+          const int sa = seg == 0 ? args.seg_a[0] : (seg == 1 ? args.seg_a[1] : args.seg_a[2]);
+          const int sb = seg == 0 ? args.seg_b[0] : (seg == 1 ? args.seg_b[1] : args.seg_b[2]);
+          const int32_t kA = (sa + kk) * kStageK, kB = (sb + kk) * kStageK;
+          const bool share = diag && sa == sb;
+          mbar_arrive_expect_tx(full_bar(stage), share ? 2 * kPlaneBytes : kStageBytes);
+          tma_load_3d(plane_addr(stage, 0), &tmZ, kA, rowJ, 0, full_bar(stage));
+          tma_load_3d(plane_addr(stage, 1), &tmZ, kA, rowJ, 1, full_bar(stage));
+          if (!share) {
+            tma_load_3d(plane_addr(stage, 2), &tmZ, kB, rowI, 0, full_bar(stage));
+            tma_load_3d(plane_addr(stage, 3), &tmZ, kB, rowI, 1, full_bar(stage));
           }
           ++issued;
           if (++stage == kStages) {
@@ -295,7 +301,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
         const TileDesc td = args.tiles[t];
         const ChanDesc cd = args.chans[td.ch];
-        const int pb = (td.ti == td.tj) ? 0 : 2;  // planes holding the i block
+        const bool diag = td.ti == td.tj;
         if (!mbar_wait(tempty_bar(acc), acc_phase ^ 1u, abort_flag)) {
           atomicOr(args.status, kStatusTimeoutMma);
           break;
@@ -303,13 +309,18 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
         tc_fence_after();
         const uint32_t d_re = tmem_base + uint32_t(acc * kAccCols);
         const uint32_t d_im = d_re + uint32_t(kTile);
-        for (int kb = 0; kb < cd.kblocks; ++kb) {
+        const int nkb = cd.kblocks * args.nseg;
+        for (int kb = 0; kb < nkb; ++kb) {
           if (!mbar_wait(full_bar(stage), phase, abort_flag)) {
             atomicOr(args.status, kStatusTimeoutMma);
             ok = false;
             break;
           }
           tc_fence_after();
+          const int seg = kb / cd.kblocks;
+          const int sa = seg == 0 ? args.seg_a[0] : (seg == 1 ? args.seg_a[1] : args.seg_a[2]);
+          const int sb = seg == 0 ? args.seg_b[0] : (seg == 1 ? args.seg_b[1] : args.seg_b[2]);
+          const int pb = (diag && sa == sb) ? 0 : 2;  // planes holding the i block
           const uint32_t are = plane_addr(stage, 0), aim = plane_addr(stage, 1);
           const uint32_t bre = plane_addr(stage, pb), bim = plane_addr(stage, pb + 1);
 #pragma unroll
@@ -352,7 +363,8 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
     const int q = warp & 3;
     const int half = (warp - 2) >> 2;
     const uint32_t bar_id = 1u + uint32_t(half);
-    const bool plain = (args.alpha == 1.f) && (args.beta == 0.f);
+    const bool plain = (args.alpha == 1.f) && (args.beta == 0.f) && !args.kahan &&
+                       args.chan_scale == nullptr;
     const uint32_t stg = smem_u32(stg_base) + uint32_t(half * 2 * kStgRows * kStgRowBytes);
     const bool issuer = (q == 0) && (lane < kStgRows);  // issues one row copy per sub-chunk
     int acc = 0;
@@ -427,13 +439,27 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
           tmem_wait_ld();
           // element (i, j) lives at i(i+1)/2 + j; row i+1 starts i+1 later
           Out2* p = outc + int64_t(i0) * (i0 + 1) / 2 + j;
+          // compensation buffer: same layout as the output (uniform calls only)
+          float2* pc = args.kahan ? static_cast<float2*>(args.out2) + cd.out0 +
+                                        int64_t(i0) * (i0 + 1) / 2 + j
+                                  : nullptr;
+          const float sc = args.alpha * (args.chan_scale ? args.chan_scale[td.ch] : 1.f);
 #pragma unroll
           for (int m = 0; m < 32; ++m) {
             const int i = i0 + m;
             if (i < n && j <= i) {
-              float vr = __uint_as_float(re[m]) * args.alpha;
-              float vi = (i == j) ? 0.f : __uint_as_float(im[m]) * args.alpha;
-              if (args.beta != 0.f) {
+              float vr = __uint_as_float(re[m]) * sc;
+              float vi = (i == j) ? 0.f : __uint_as_float(im[m]) * sc;
+              if (args.kahan) {
+                // sum += v with the rounding error carried in the compensation
+                const float2 sum = get(p), cmp = *pc;
+                const float yr = __fsub_rn(vr, cmp.x), yi = __fsub_rn(vi, cmp.y);
+                const float tr = __fadd_rn(sum.x, yr), ti = __fadd_rn(sum.y, yi);
+                *pc = make_float2(__fsub_rn(__fsub_rn(tr, sum.x), yr),
+                                  __fsub_rn(__fsub_rn(ti, sum.y), yi));
+                vr = tr;
+                vi = ti;
+              } else if (args.beta != 0.f) {
                 const float2 o = get(p);
                 vr += args.beta * o.x;
                 vi += args.beta * o.y;
@@ -441,6 +467,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
               put(p, vr, vi);
             }
             p += i + 1;
+            if (args.kahan) pc += i + 1;
           }
         }
       }

@@ -78,7 +78,24 @@ struct HerkArgs {
   float alpha;
   float beta;
   uint32_t* status;
+  // K segments: segment s pairs the A (j) operand's k-blocks seg_a[s] + kk
+  // with the B (i) operand's k-blocks seg_b[s] + kk, kk < kblocks, all
+  // accumulated into one result (nseg = 1, offsets 0: a plain HERK).
+  int32_t nseg;
+  int32_t seg_a[3];
+  int32_t seg_b[3];
+  int32_t kahan;            // 1: Kahan-accumulate into out (sum) and out2 (compensation)
+  const float* chan_scale;  // per-channel result multiplier (nullptr: 1)
+  void* out2;
 };
+
+// A plain single-segment argument block.
+inline HerkArgs herk_args_default() {
+  HerkArgs a{};
+  a.nseg = 1;
+  a.alpha = 1.f;
+  return a;
+}
 
 // Host-side launchers (herk_fp8.cu).
 cudaError_t launch_qc_to_planes(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
@@ -91,5 +108,10 @@ cudaError_t launch_fp16_to_planes(const void* a16, uint8_t* z, int64_t rows, int
 cudaError_t launch_gather_qc_to_planes(const GatherDesc* g, int nch, int max_n, uint8_t* z,
                                        int64_t total_rows, int Kp, cudaStream_t s);
 cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s);
+// Float complex [rows][K] -> scaled E4M3 planes of pitch zpitch (precision.cu).
+cudaError_t launch_float_to_planes(const void* a, uint8_t* z, int64_t rows, int K, int Kp,
+                                   int zpitch, int n, int batch, int split, float* qscale,
+                                   float* out_scale, uint32_t* amax_bits, int sm_count,
+                                   cudaStream_t s);
 
 }  // namespace ftdx

@@ -147,7 +147,7 @@ extern "C" ftdx_status ftdx_herk_static(const void* A, void* C, int N, int K, in
           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return FTDX_ERR_CUDA;
 
-  HerkArgs args;
+  HerkArgs args = herk_args_default();
   args.tiles = tiles;
   args.chans = chans;
   args.num_tiles = int(ntiles);

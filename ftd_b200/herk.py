@@ -15,8 +15,8 @@ from __future__ import annotations
 import ctypes
 
 from . import _lib
-from ._lib import (COMPUTE_FP8, FORMAT_PACKED_TRIANGLE, IN_FP16, IN_INT4, OUT_FP16, OUT_FP32,
-                   FtdxError, check, load)
+from ._lib import (COMPUTE_FP8, COMPUTE_FP8_SPLIT, FORMAT_PACKED_TRIANGLE, IN_FP16, IN_FP32,  # noqa: F401
+                   IN_INT4, OUT_FP16, OUT_FP32, FtdxError, check, load)
 
 __all__ = ["Correlator", "herk_batched_cutlass_qc", "herk_batched_cutlass_qc_fp16",
            "herk_batched_cutlass_fp16", "init_cutlass_api", "tri_size", "FtdxError",
@@ -117,6 +117,13 @@ class Correlator:
                                          output, float(alpha), float(beta), _stream(stream),
                                          int(bool(tune)))
         check(self._h, st, "ftdx_herk_batched_v")
+
+    def herk_kahan(self, A, S, comp, N: int, K: int, batch: int, input: int = IN_INT4,
+                   compute: int = COMPUTE_FP8, stream=None) -> None:
+        """S += A A^H with Kahan compensation kept in `comp` (both packed complex64)."""
+        st = self._L.ftdx_herk_kahan(self._h, _ptr(A), _ptr(S), _ptr(comp), N, K, batch, input,
+                                     compute, _stream(stream))
+        check(self._h, st, "ftdx_herk_kahan")
 
     def init_herk(self, N: int, K: int, batch: int, stream=None) -> None:
         check(self._h, self._L.ftdx_init_herk(self._h, N, K, batch, _stream(stream)),

@@ -52,11 +52,17 @@ typedef enum ftdx_status {
 
 /* Values equal the reference's enum class ordinals
  * (cutlass_interface/cutlass_gemm_api.h:37-59). */
-typedef enum ftdx_input { FTDX_IN_FP16 = 0, FTDX_IN_INT4 = 1 } ftdx_input;
+typedef enum ftdx_input {
+  FTDX_IN_FP16 = 0,
+  FTDX_IN_INT4 = 1,
+  FTDX_IN_FP32 = 2   /* interleaved complex64 [batch][N][K][2] float (this library only) */
+} ftdx_input;
 typedef enum ftdx_compute {
-  FTDX_COMPUTE_FP8 = 0,
+  FTDX_COMPUTE_FP8 = 0,        /* INT4: exact; FP16: unscaled E4M3 (as the reference);
+                                  FP32: E4M3 with a per-channel scale */
   FTDX_COMPUTE_FP6 = 1,
-  FTDX_COMPUTE_FP4 = 2
+  FTDX_COMPUTE_FP4 = 2,        /* NVFP4: E2M1 with one E4M3 scale per 16 values (FP32 input) */
+  FTDX_COMPUTE_FP8_SPLIT = 3   /* FP32 input: hi + lo E4M3, hi.hi^H + hi.lo^H + lo.hi^H */
 } ftdx_compute;
 typedef enum ftdx_output { FTDX_OUT_FP16 = 0, FTDX_OUT_FP32 = 1 } ftdx_output;
 typedef enum ftdx_format { FTDX_FORMAT_PACKED_TRIANGLE = 0 } ftdx_format;
@@ -121,6 +127,16 @@ typedef struct ftdx_channel_desc {
 FTDX_API ftdx_status ftdx_herk_batched_v(ftdx_handle h, const ftdx_channel_desc* chans,
                                          int n_chans, ftdx_output output, float alpha,
                                          float beta, void* stream, int tune);
+
+/* Kahan-compensated accumulation across integration dumps (no counterpart
+ * in the reference): sum += A A^H with the FP32 rounding error of every
+ * addition carried in `comp` (same packed layout and size as `sum`, complex64,
+ * zero it before the first dump).  After n dumps, sum + comp holds the total
+ * to about FP32 precision independently of n.  Both buffers are read and
+ * written by every call; FP32 output only. */
+FTDX_API ftdx_status ftdx_herk_kahan(ftdx_handle h, const void* A, void* sum, void* comp, int N,
+                                     int K, int batch, ftdx_input input, ftdx_compute compute,
+                                     void* stream);
 
 /* Pre-size the workspace for problems up to (N, K, batch) so that later
  * ftdx_herk calls allocate nothing (required before graph capture).

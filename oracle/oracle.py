@@ -163,3 +163,40 @@ def gaussian_qc(seed: int, batch: int, N: int, K: int, sigma: float = 2.5) -> np
     rng = np.random.default_rng(seed)
     re, im = gaussian_int4(rng, (batch, N, K), sigma)
     return encode_qc(re, im)
+
+
+# ----------------------------------------------------------------- precision study
+def workload4_voltages(seed: int, batch: int, N: int, K: int, rfi_time_frac: float = 0.01,
+                       rfi_input_frac: float = 0.05, rfi_sigma: float = 20.0) -> np.ndarray:
+    """Complex Gaussian voltages [batch, N, K] (complex64): per-channel RMS
+    log-uniform in [0.1, 10]; on `rfi_input_frac` of the inputs, a fraction
+    `rfi_time_frac` of the time samples carries a burst of `rfi_sigma` sigma."""
+    rng = np.random.default_rng(seed)
+    rms = np.exp(rng.uniform(np.log(0.1), np.log(10.0), size=batch))
+    v = (rng.normal(size=(batch, N, K)) + 1j * rng.normal(size=(batch, N, K))) / np.sqrt(2.0)
+    v *= rms[:, None, None]
+    for b in range(batch):
+        ins = rng.choice(N, size=max(1, int(round(rfi_input_frac * N))), replace=False)
+        ts = rng.choice(K, size=max(1, int(round(rfi_time_frac * K))), replace=False)
+        phase = np.exp(2j * np.pi * rng.uniform(size=(len(ins), len(ts))))
+        v[b][np.ix_(ins, ts)] = rfi_sigma * rms[b] * phase
+    return v.astype(np.complex64)
+
+
+def correlation_errors(got: np.ndarray, ref: np.ndarray, N: int) -> dict:
+    """Errors of packed triangles [batch, P, 2] against an FP64 reference:
+    elementwise |dR_ij| / sqrt(R_ii R_jj) (normalised by the autocorrelations,
+    the scale-free measure for correlation products) -- max and RMS -- and the
+    relative error of the autocorrelations R_ii themselves."""
+    g = got[..., 0].astype(np.float64) + 1j * got[..., 1].astype(np.float64)
+    r = ref[..., 0] + 1j * ref[..., 1]
+    i, j = np.tril_indices(N)
+    order = np.lexsort((j, i))
+    i, j = i[order], j[order]
+    diag = np.arange(N) * (np.arange(N) + 1) // 2 + np.arange(N)
+    auto = r[:, diag].real
+    norm = np.sqrt(np.maximum(auto[:, i] * auto[:, j], 1e-300))
+    e = np.abs(g - r) / norm
+    de = np.abs(g[:, diag].real - auto) / np.maximum(auto, 1e-300)
+    return {"max_norm": float(e.max()), "rms_norm": float(np.sqrt(np.mean(e ** 2))),
+            "max_auto_rel": float(de.max()), "rms_auto_rel": float(np.sqrt(np.mean(de ** 2)))}

@@ -77,11 +77,11 @@ def test_uneven_flagged_medium_tuned_and_graph():
         assert c.graph_count() == 1
         check(chans, host)
         # new flag lists written into the same device arrays are honoured
-        for ch, hb in zip(chans, host):
-            block, rows_used, n, K = hb
+        for k, ch in enumerate(chans):
+            block, rows_used, n, K = host[k]
             new = np.sort(rng.choice(768, size=n, replace=False)).astype(np.int32)
             ch["active"].copy_(torch.from_numpy(new))
-            host[host.index(hb)] = (block, new, n, K)
+            host[k] = (block, new, n, K)
         c.herk_batched_v(chans, tune=True)
         check(chans, host)
         assert c.device_status() == 0
@@ -120,3 +120,42 @@ def test_batched_bad_descriptor_rejected():
         C = torch.zeros(20, 2, device=DEV)
         with pytest.raises(FtdxError):  # lda < K
             c.herk_batched_v([{"A": A, "C": C, "n_inputs": 4, "K": 16, "lda": 8}])
+
+
+def make_workload3(seed, n_chans=96, inputs=4096):
+    """96 channels; K ~ U{128, 192, ..., 2048}; active inputs ~ U[1536, 4096]
+    after seeded random flagging of a 4096-input array; Gaussian int4 (sigma 2.5)."""
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=DEV).manual_seed(seed)
+    chans = []
+    for _ in range(n_chans):
+        K = int(rng.integers(2, 33)) * 64
+        n = int(rng.integers(1536, inputs + 1))
+        active = np.sort(rng.choice(inputs, size=n, replace=False)).astype(np.int32)
+        re = torch.clamp(torch.round(torch.randn(inputs, K, device=DEV, generator=g) * 2.5), -7, 7).to(torch.int32)
+        im = torch.clamp(torch.round(torch.randn(inputs, K, device=DEV, generator=g) * 2.5), -7, 7).to(torch.int32)
+        qc = ((torch.where(re < 0, 8 | (-re), re) << 4) | torch.where(im < 0, 8 | (-im), im)).to(torch.uint8)
+        chans.append({"A": qc, "C": torch.empty(tri_size(n), 2, device=DEV), "n_inputs": n, "K": K,
+                      "active": torch.from_numpy(active).to(DEV), "re": re, "im": im})
+    return chans
+
+
+def test_workload3_full_size_properties():
+    chans = make_workload3(2027)
+    with Correlator() as c:
+        c.herk_batched_v(chans, tune=True)
+        assert c.device_status() == 0
+    torch.cuda.synchronize()
+    for k, ch in enumerate(chans):
+        n = ch["n_inputs"]
+        act = ch["active"].long()
+        # diagonal: sum |v|^2 of each active input, exactly
+        power = (ch["re"][act] ** 2 + ch["im"][act] ** 2).sum(-1).float()
+        idx = torch.arange(n, device=DEV, dtype=torch.int64)
+        assert torch.equal(ch["C"][idx * (idx + 1) // 2 + idx, 0], power), k
+        if k % 24 == 0:  # exact rows against the oracle for a few channels
+            qc = ch["A"][act].cpu().numpy()[None]
+            i0 = n - 40
+            ref = oracle.herk_qc_rows(qc, n, ch["K"], 0, i0, n).astype(np.float32)
+            got = ch["C"][tri_size(i0):tri_size(n)].cpu().numpy()
+            assert np.array_equal(got, ref), k

@@ -1,0 +1,89 @@
+"""Precision modes on float complex voltages (per-channel-scaled FP8 and the
+hi+lo split-FP8 mode) against the FP64 oracle, and Kahan accumulation across
+integration dumps.  Errors are measured as |dR_ij| / sqrt(R_ii R_jj) (scale
+free; the bound is written in each test)."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+from oracle import oracle  # noqa: E402
+
+from ftd_b200 import Correlator, tri_size  # noqa: E402
+from ftd_b200._lib import (COMPUTE_FP8, COMPUTE_FP8_SPLIT, IN_FP32, IN_INT4,  # noqa: E402
+                           OUT_FP32)
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+
+
+def run_float(v, compute):
+    B, N, K = v.shape
+    A = torch.from_numpy(np.ascontiguousarray(v).view(np.float32).reshape(B, N, K, 2)).to(DEV)
+    C = torch.full((B, tri_size(N), 2), float("nan"), device=DEV)
+    with Correlator() as c:
+        c.herk(A, C, N, K, B, input=IN_FP32, compute=compute, output=OUT_FP32)
+        assert c.device_status() == 0
+    torch.cuda.synchronize()
+    return C.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def workload():
+    B, N, K = 4, 256, 1024
+    v = oracle.workload4_voltages(404, B, N, K)
+    return v, oracle.herk_c128(v.astype(np.complex128), N, K, B)
+
+
+def test_fp8_scaled_error(workload):
+    v, ref = workload
+    err = oracle.correlation_errors(run_float(v, COMPUTE_FP8), ref, v.shape[1])
+    print("fp8", err)
+    # E4M3 keeps 4 significant bits: ~3% per sample, averaged over K samples
+    assert err["max_norm"] < 3e-2 and err["rms_norm"] < 3e-3
+    assert err["max_auto_rel"] < 3e-2
+
+
+def test_split_fp8_error(workload):
+    v, ref = workload
+    err = oracle.correlation_errors(run_float(v, COMPUTE_FP8_SPLIT), ref, v.shape[1])
+    print("split", err)
+    # hi + lo carries ~8 significant bits; the dropped lo.lo^H term biases R_ii by ~3e-4
+    assert err["max_norm"] < 3e-3 and err["rms_norm"] < 3e-4
+    err8 = oracle.correlation_errors(run_float(v, COMPUTE_FP8), ref, v.shape[1])
+    assert err["rms_norm"] < err8["rms_norm"] / 8
+
+
+def test_scale_invariance():
+    # per-channel scaling: channels differing only by a power-of-two factor give
+    # results differing by exactly that factor squared
+    B, N, K = 2, 130, 256
+    v = oracle.workload4_voltages(405, 1, N, K)
+    v2 = np.concatenate([v, v * np.float32(8.0)], axis=0)
+    out = run_float(v2, COMPUTE_FP8)
+    assert np.array_equal(out[1], out[0] * 64.0)
+
+
+def test_kahan_accumulation_across_dumps():
+    N, K, B, dumps = 128, 1024, 2, 800
+    rng = np.random.default_rng(9)
+    S = torch.zeros(B, tri_size(N), 2, device=DEV)
+    comp = torch.zeros_like(S)
+    naive = torch.zeros_like(S)
+    exact = np.zeros((B, tri_size(N), 2), dtype=np.int64)
+    with Correlator() as c:
+        for d in range(dumps):
+            qc = oracle.gaussian_qc(int(rng.integers(1 << 30)), B, N, K, sigma=5.0)
+            exact += oracle.herk_qc(qc, N, K, B)
+            dq = torch.from_numpy(qc.reshape(-1)).to(DEV)
+            c.herk_kahan(dq, S, comp, N, K, B, input=IN_INT4, compute=COMPUTE_FP8)
+            c.herk(dq, naive, N, K, B, input=IN_INT4, output=OUT_FP32, beta=1.0, tune=False)
+        assert c.device_status() == 0
+    torch.cuda.synchronize()
+    # the compensation holds minus the low-order part lost from the sum
+    tot = S.double().cpu().numpy() - comp.double().cpu().numpy()
+    err_k = np.abs(tot - exact).max()
+    err_n = np.abs(naive.double().cpu().numpy() - exact).max()
+    print("kahan max abs err", err_k, "naive", err_n, "max |total|", np.abs(exact).max())
+    assert np.abs(exact).max() > 2 ** 24          # beyond FP32's exact-integer range
+    assert err_k <= 2.0                            # compensated: ~exact
+    assert err_n > 4 * max(err_k, 0.5)             # plain FP32 accumulation drifts
