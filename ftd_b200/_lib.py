@@ -54,6 +54,8 @@ PROTOTYPES = {
     "ftdx_last_error": (ctypes.c_char_p, [_vp]),
     "ftdx_herk": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _f, _f, _vp, _i]),
     "ftdx_init_herk": (_i, [_vp, _i, _i, _i, _vp]),
+    "ftdx_herk_adjoint": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _vp]),
+    "ftdx_gain_gradient": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp]),
     "ftdx_herk_kahan": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
     "ftdx_herk_batched_v": (_i, [_vp, ctypes.c_void_p, _i, _i, _f, _f, _vp, _i]),
     "ftdx_end_herk": (_i, [_vp]),

@@ -120,6 +120,7 @@ ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t 
 ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t Kp,
                               CUtensorMap* tm);
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+void* tensor_map_encoder();  // cuTensorMapEncodeTiled through the runtime
 
 // Event pair around one kernel launch when profiling is on (never during capture).
 struct ScopedTimer {

@@ -32,6 +32,8 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
   return fn;
 }
 
+void* tensor_map_encoder() { return reinterpret_cast<void*>(get_encode_fn()); }
+
 ftdx_status fail(ftdx_handle h, ftdx_status s, const char* fmt, ...) {
   if (h) {
     char buf[512];

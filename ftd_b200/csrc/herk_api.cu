@@ -423,6 +423,49 @@ ftdx_status ftdx_set_graph_mode(ftdx_handle h, int enable) {
 
 int ftdx_graph_count(ftdx_handle h) { return h ? int(h->graphs.size()) : -1; }
 
+ftdx_status ftdx_herk_adjoint(ftdx_handle h, const void* G, const void* V, void* dV, int N, int K,
+                              int batch, ftdx_input input, void* stream) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  if (!G || !V || !dV || N < 8 || K < 1 || batch < 1 || batch > 65535 || (N % 8) != 0 ||
+      N > (1 << 17) || K > (1 << 20) || int64_t(batch) * K > (int64_t(1) << 30))
+    return fail(h, FTDX_ERR_INVALID_ARG, "adjoint: bad sizes (N a multiple of 8, >= 8)");
+  if (input != FTDX_IN_INT4)
+    return fail(h, FTDX_ERR_UNSUPPORTED, "adjoint: only QC int4 voltages are implemented");
+  if (((reinterpret_cast<uintptr_t>(G) | reinterpret_cast<uintptr_t>(dV)) & 7) != 0)
+    return fail(h, FTDX_ERR_INVALID_ARG, "adjoint: misaligned G or dV");
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  ftdx_status st = ensure_workspace(h, adjoint_workspace_bytes(N, K, batch), s);
+  if (st != FTDX_OK) return st;
+  {
+    ScopedTimer tm(h, s, 0);
+    e = launch_adjoint(G, static_cast<const uint8_t*>(V), dV, N, K, batch, h->z, h->sm_count,
+                       h->d_status, tensor_map_encoder(), s);
+  }
+  return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "adjoint launch");
+}
+
+ftdx_status ftdx_gain_gradient(ftdx_handle h, const void* R_obs, const void* R_mod,
+                               const float* W, const void* g, int N, int n_chans, double* grad,
+                               double* loss, void* stream) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  if (!R_obs || !R_mod || !W || !g || !grad || !loss || N < 1 || n_chans < 1 ||
+      n_chans > 65535 || N > (1 << 20))
+    return fail(h, FTDX_ERR_INVALID_ARG, "gain_gradient: bad arguments");
+  if (((reinterpret_cast<uintptr_t>(R_obs) | reinterpret_cast<uintptr_t>(R_mod) |
+        reinterpret_cast<uintptr_t>(g) | reinterpret_cast<uintptr_t>(grad) |
+        reinterpret_cast<uintptr_t>(loss)) & 7) != 0 ||
+      (reinterpret_cast<uintptr_t>(W) & 3) != 0)
+    return fail(h, FTDX_ERR_INVALID_ARG, "gain_gradient: misaligned pointer");
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e == cudaSuccess)
+    e = launch_gain_grad(static_cast<const float2*>(R_obs), static_cast<const float2*>(R_mod), W,
+                         static_cast<const float2*>(g), N, n_chans, grad, loss,
+                         static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "gain gradient launch");
+}
+
 ftdx_status ftdx_herk_kahan(ftdx_handle h, const void* A, void* sum, void* comp, int N, int K,
                             int batch, ftdx_input input, ftdx_compute compute, void* stream) {
   if (!h) return FTDX_ERR_INVALID_ARG;

@@ -108,6 +108,15 @@ cudaError_t launch_fp16_to_planes(const void* a16, uint8_t* z, int64_t rows, int
 cudaError_t launch_gather_qc_to_planes(const GatherDesc* g, int nch, int max_n, uint8_t* z,
                                        int64_t total_rows, int Kp, cudaStream_t s);
 cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s);
+// Gain-calibration loss and gradient over packed triangles (gain_grad.cu).
+cudaError_t launch_gain_grad(const float2* robs, const float2* rmod, const float* w,
+                             const float2* g, int n, int nchan, double* grad, double* loss,
+                             cudaStream_t s);
+// Adjoint dV = (G + G^H) V (adjoint.cu); n must be a multiple of 8.
+size_t adjoint_workspace_bytes(int n, int K, int batch);
+cudaError_t launch_adjoint(const void* G, const uint8_t* V, void* dV, int n, int K, int batch,
+                           uint8_t* ws, int sm_count, uint32_t* status, void* encode_fn,
+                           cudaStream_t s);
 // Float complex [rows][K] -> scaled E4M3 planes of pitch zpitch (precision.cu).
 cudaError_t launch_float_to_planes(const void* a, uint8_t* z, int64_t rows, int K, int Kp,
                                    int zpitch, int n, int batch, int split, float* qscale,

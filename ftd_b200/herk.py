@@ -125,6 +125,20 @@ class Correlator:
                                      compute, _stream(stream))
         check(self._h, st, "ftdx_herk_kahan")
 
+    def herk_adjoint(self, G, V, dV, N: int, K: int, batch: int, input: int = IN_INT4,
+                     stream=None) -> None:
+        """dV = (G + G^H) V per channel (G complex64 [batch][N][N], V QC int4)."""
+        st = self._L.ftdx_herk_adjoint(self._h, _ptr(G), _ptr(V), _ptr(dV), N, K, batch, input,
+                                       _stream(stream))
+        check(self._h, st, "ftdx_herk_adjoint")
+
+    def gain_gradient(self, R_obs, R_mod, W, g, N: int, n_chans: int, grad, loss,
+                      stream=None) -> None:
+        """Gain-calibration loss (double) and gradient (complex128 [N]) on the device."""
+        st = self._L.ftdx_gain_gradient(self._h, _ptr(R_obs), _ptr(R_mod), _ptr(W), _ptr(g), N,
+                                        n_chans, _ptr(grad), _ptr(loss), _stream(stream))
+        check(self._h, st, "ftdx_gain_gradient")
+
     def init_herk(self, N: int, K: int, batch: int, stream=None) -> None:
         check(self._h, self._L.ftdx_init_herk(self._h, N, K, batch, _stream(stream)),
               "ftdx_init_herk")

@@ -212,6 +212,33 @@ FTDX_API ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid);
 FTDX_API ftdx_status ftdx_herk_static(const void* A, void* C, int N, int K, int batch,
                                       void* stream, uint32_t* status_out, size_t* scratch_used);
 
+/* ---- differentiation -------------------------------------------------------
+ * No counterpart in the reference.
+ *
+ * Adjoint of the correlator: for visibilities R = V V^H and an upstream
+ * gradient G = dL/dR (N x N complex64 per channel, row-major, batch back to
+ * back; any matrix, not only Hermitian), dV = (G + G^H) V (N x K complex64
+ * per channel, row-major).  V is QC int4 [batch][N][K] (FTDX_IN_INT4).
+ * G + G^H is carried as bf16 hi + lo on the tensor cores with FP32
+ * accumulation (relative error ~1e-5 of max|dV|).  N must be a multiple of 8.
+ * Uses the handle's workspace (2 bytes x (4 N^2 + 2 N K) per channel). */
+FTDX_API ftdx_status ftdx_herk_adjoint(ftdx_handle h, const void* G, const void* V, void* dV,
+                                       int N, int K, int batch, ftdx_input input, void* stream);
+
+/*
+ * Gain calibration: for per-input complex gains g[N] shared by all channels,
+ * observed and model visibilities R_obs, R_mod (packed lower triangles of
+ * complex64, n_chans back to back, as ftdx_herk writes them) and real
+ * weights W (packed, float, same layout),
+ *   L = sum_f sum_{i,j} W_ij |R_obs,ij - g_i R_mod,ij conj(g_j)|^2
+ * over the full Hermitian matrices (off-diagonal entries of the triangle
+ * count twice), and grad[k] = dL/dRe(g_k) + i dL/dIm(g_k).  grad is
+ * complex128 [N] (two doubles per input), loss one double; both are device
+ * pointers, overwritten (not accumulated) by the call. */
+FTDX_API ftdx_status ftdx_gain_gradient(ftdx_handle h, const void* R_obs, const void* R_mod,
+                                        const float* W, const void* g, int N, int n_chans,
+                                        double* grad, double* loss, void* stream);
+
 /* Kernel timing (no counterpart in the reference; its benches time whole
  * calls).  While enabled, CUDA events are recorded on the caller's stream
  * around every kernel this handle launches.  ftdx_profile_read synchronises,

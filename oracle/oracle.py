@@ -200,3 +200,43 @@ def correlation_errors(got: np.ndarray, ref: np.ndarray, N: int) -> dict:
     de = np.abs(g[:, diag].real - auto) / np.maximum(auto, 1e-300)
     return {"max_norm": float(e.max()), "rms_norm": float(np.sqrt(np.mean(e ** 2))),
             "max_auto_rel": float(de.max()), "rms_auto_rel": float(np.sqrt(np.mean(de ** 2)))}
+
+
+# ----------------------------------------------------------------- gain calibration
+def unpack_tri(tri: np.ndarray, N: int) -> np.ndarray:
+    """Packed lower triangle [P, 2] (or complex [P]) -> full Hermitian N x N complex128."""
+    t = np.asarray(tri)
+    if t.ndim == 2 and t.shape[-1] == 2:
+        t = t[..., 0].astype(np.float64) + 1j * t[..., 1].astype(np.float64)
+    i, j = np.tril_indices(N)
+    order = np.lexsort((j, i))
+    i, j = i[order], j[order]
+    M = np.zeros((N, N), dtype=np.complex128)
+    M[i, j] = t
+    M[j, i] = np.conj(t)
+    return M
+
+
+def unpack_tri_real(tri: np.ndarray, N: int) -> np.ndarray:
+    i, j = np.tril_indices(N)
+    order = np.lexsort((j, i))
+    i, j = i[order], j[order]
+    M = np.zeros((N, N), dtype=np.float64)
+    M[i, j] = tri
+    M[j, i] = tri
+    return M
+
+
+def gain_loss_grad(robs: np.ndarray, rmod: np.ndarray, w: np.ndarray, g: np.ndarray, N: int):
+    """FP64 loss and gradient of sum_f ||W o (R_obs - g R_mod g^H)||_F^2 over
+    full Hermitian matrices; grad_k = dL/dRe g_k + i dL/dIm g_k
+    = -4 sum_f sum_j W_kj E_kj conj(R_mod,kj) g_j."""
+    g = np.asarray(g, dtype=np.complex128)
+    L = 0.0
+    grad = np.zeros(N, dtype=np.complex128)
+    for f in range(robs.shape[0]):
+        Ro, Rm, W = unpack_tri(robs[f], N), unpack_tri(rmod[f], N), unpack_tri_real(w[f], N)
+        E = Ro - g[:, None] * Rm * np.conj(g)[None, :]
+        L += float(np.sum(W * np.abs(E) ** 2))
+        grad += -4.0 * (W * E * np.conj(Rm)) @ g
+    return L, grad
