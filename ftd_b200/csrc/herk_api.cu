@@ -28,6 +28,7 @@ struct HerkCall {
 };
 
 bool is_split(const HerkCall& c) { return c.compute == FTDX_COMPUTE_FP8_SPLIT; }
+bool is_fp4(const HerkCall& c) { return c.compute == FTDX_COMPUTE_FP4; }
 
 ftdx_status validate(ftdx_handle h, const HerkCall& c, ftdx_compute compute, ftdx_format format) {
   if (!c.A || !c.C) return fail(h, FTDX_ERR_INVALID_ARG, "herk: null A or C");
@@ -42,7 +43,11 @@ ftdx_status validate(ftdx_handle h, const HerkCall& c, ftdx_compute compute, ftd
     return fail(h, FTDX_ERR_INVALID_ARG, "herk: only the packed triangle format exists");
   if (compute == FTDX_COMPUTE_FP8_SPLIT && c.input != FTDX_IN_FP32)
     return fail(h, FTDX_ERR_INVALID_ARG, "herk: split FP8 needs FP32 input");
-  if (compute != FTDX_COMPUTE_FP8 && compute != FTDX_COMPUTE_FP8_SPLIT)
+  if (compute == FTDX_COMPUTE_FP4 &&
+      (c.input != FTDX_IN_FP32 || c.output != FTDX_OUT_FP32 || c.comp != nullptr))
+    return fail(h, FTDX_ERR_UNSUPPORTED, "herk: NVFP4 needs FP32 input and FP32 output");
+  if (compute != FTDX_COMPUTE_FP8 && compute != FTDX_COMPUTE_FP8_SPLIT &&
+      compute != FTDX_COMPUTE_FP4)
     return fail(h, FTDX_ERR_UNSUPPORTED, "herk: compute precision %d not implemented for "
                 "this entry point", int(compute));
   if (c.input == FTDX_IN_FP32 && (reinterpret_cast<uintptr_t>(c.A) & 7) != 0)
@@ -57,6 +62,65 @@ ftdx_status validate(ftdx_handle h, const HerkCall& c, ftdx_compute compute, ftd
   if (c.N > 65535 * kTile) return fail(h, FTDX_ERR_INVALID_ARG, "herk: N too large");
   if (int64_t(c.K) > (int64_t(1) << 30)) return fail(h, FTDX_ERR_INVALID_ARG, "herk: K too large");
   return FTDX_OK;
+}
+
+// Tile plan of the NVFP4 kernel: ti over 64 row inputs, tj over 128 column
+// inputs, tiles holding at least one j <= i.  Cached with a negative kblocks
+// key so it never collides with the FP8 plans.
+ftdx_status get_fp4_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
+                         const Plan** out) {
+  const auto key = std::make_tuple(N, -1 - kblocks, batch);
+  auto it = h->plans.find(key);
+  if (it != h->plans.end()) {
+    *out = it->second.get();
+    return FTDX_OK;
+  }
+  if (stream_capturing(s))
+    return fail(h, FTDX_ERR_CAPACITY, "NVFP4 tile plan built while capturing; call once first");
+  const int ni = (N + 63) / 64, nj = (N + 127) / 128;
+  std::vector<ChanDesc> chans(batch);
+  std::vector<TileDesc> tiles;
+  for (int c = 0; c < batch; ++c) {
+    chans[c] = ChanDesc{N, kblocks, int64_t(c) * N, int64_t(c) * (int64_t(N) * (N + 1) / 2), 0};
+    for (int ti = 0; ti < ni; ++ti)
+      for (int tj = 0; tj < nj && tj * 128 <= ti * 64 + 63; ++tj)
+        tiles.push_back(TileDesc{c, uint16_t(ti), uint16_t(tj)});
+  }
+  auto p = std::make_unique<Plan>();
+  p->num_tiles = int(tiles.size());
+  p->num_chans = batch;
+  cudaError_t e = cudaMalloc(&p->d_tiles, tiles.size() * sizeof(TileDesc));
+  if (e == cudaSuccess) e = cudaMalloc(&p->d_chans, chans.size() * sizeof(ChanDesc));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(p->d_tiles, tiles.data(), tiles.size() * sizeof(TileDesc),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(p->d_chans, chans.data(), chans.size() * sizeof(ChanDesc),
+                   cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(h, e, "NVFP4 plan upload");
+  *out = p.get();
+  h->plans.emplace(key, std::move(p));
+  return FTDX_OK;
+}
+
+ftdx_status launch_fp4(ftdx_handle h, const HerkCall& c, cudaStream_t s) {
+  const int64_t rows = int64_t(c.N) * c.batch;
+  ftdx_status st = ensure_workspace(h, nvfp4_workspace_bytes(rows, c.K), s);
+  if (st == FTDX_OK) st = ensure_aux(h, size_t(12) * size_t(c.batch) + 256, s);
+  const Plan* plan = nullptr;
+  if (st == FTDX_OK) st = get_fp4_plan(h, c.N, nvfp4_kblocks(c.K), c.batch, s, &plan);
+  if (st != FTDX_OK) return st;
+  float* gscale = reinterpret_cast<float*>(h->aux);
+  float* out_scale = gscale + c.batch;
+  uint32_t* amax = reinterpret_cast<uint32_t*>(out_scale + c.batch);
+  cudaError_t e;
+  {
+    ScopedTimer tm(h, s, 0);
+    e = launch_nvfp4(c.A, rows, c.K, c.N, c.batch, h->z, gscale, out_scale, amax,
+                     plan->d_tiles, plan->d_chans, plan->num_tiles, c.C, c.alpha, c.beta,
+                     h->d_status, h->sm_count, tensor_map_encoder(), s);
+  }
+  return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "NVFP4 launch");
 }
 
 // Workspace and tile plan for a call; allocates, so never while capturing.
@@ -75,6 +139,7 @@ ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan
 
 // Promotion kernel + correlator kernel on stream s.
 ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, cudaStream_t s) {
+  if (is_fp4(c)) return launch_fp4(h, c, s);
   const Plan* plan = nullptr;
   ftdx_status st = prepare(h, c, s, &plan);
   if (st != FTDX_OK) return st;

@@ -1,0 +1,438 @@
+// herk_fp4.cu -- NVFP4 correlator for float complex voltages.
+//
+// Quantisation (nvfp4_quantize_kernel): per channel a global FP32 scale
+// g_c = amax_c / (6 * 448); per row and block of 16 values along K (8
+// complex samples, Re/Im interleaved) a UE4M3 block scale b >= amax_blk /
+// (6 g_c) (rounded up, so no element saturates); elements E2M1(v / (g_c b)),
+// round to nearest even.  Each input row a becomes two operand rows with the
+// same block scales: x_a = (re, im)_t and y_a = (im, -re)_t, so that
+//   x_j . x_i = Re R_ij and x_j . y_i = Im R_ij
+// (the FP4 MMA has no negate bit; the sign lives in the y row).  The result
+// is multiplied by g_c^2 in the epilogue.
+//
+// herk_fp4_tc_kernel: persistent tcgen05 kernel, tile = 128 column inputs j
+// (MMA M, x rows) x 64 row inputs i (MMA N = 128: their x and y rows).  TMA
+// brings per stage 128 B of K (256 E2M1 values) of A and B plus their 16
+// scale bytes per row; four scale-factor warps copy the scales into TMEM in
+// the layout tcgen05.mma kind::mxf4nvf4.block_scale expects (row m of a
+// 128-row operand at lane m%32 of every lane quarter, column m/32, byte = the
+// 16-element block within the 64-element k-step); one thread issues the
+// MMAs (M=128, N=128, K=64); four epilogue warps store the packed triangle.
+#include <cuda_fp4.h>
+#include <cudaTypedefs.h>
+#include <cuda_fp8.h>
+
+#include "herk_fp8.cuh"
+#include "sm100.cuh"
+
+namespace ftdx {
+using namespace dev;
+namespace {
+
+constexpr int k4J = 128;                      // j inputs per tile (A rows)
+constexpr int k4I = 64;                       // i inputs per tile (B rows = 128)
+constexpr int k4KB = 128;                     // operand bytes of K per stage (256 E2M1)
+constexpr int k4Op = 128 * k4KB;              // 16 KB per operand per stage
+constexpr int k4Sf = 128 * 16;                // 2 KB of scales per operand per stage
+constexpr int k4StageBytes = 2 * k4Op + 2 * k4Sf;  // 36 KB (multiple of 1 KB)
+constexpr int k4Stages = 5;
+constexpr int k4AccCols = 128;                // (Re, Im) column pairs of 64 inputs
+constexpr int k4SfCol0 = 2 * k4AccCols;       // TMEM columns of the scale-factor slots
+constexpr int k4SfColsPerStage = 32;          // 4 k-steps x (4 SFA + 4 SFB) columns
+constexpr int k4Threads = 320;                // TMA, MMA, 4 epilogue, 4 scale-factor warps
+constexpr size_t k4Smem = 1024 + size_t(k4Stages) * k4StageBytes + 256;
+
+// E4M3 bits of a non-negative float, rounded up to the next representable
+// value (the block scale must not let any element saturate).
+__device__ __forceinline__ uint32_t ue4m3_ceil(float v) {
+  if (!(v > 0.f)) return 0u;
+  uint32_t c = uint32_t(__nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3)) & 0x7Fu;
+  const __half_raw h = __nv_cvt_fp8_to_halfraw(__nv_fp8_storage_t(c), __NV_E4M3);
+  if (__half2float(__half(h)) < v && c < 0x7Eu) ++c;
+  return c;
+}
+__device__ __forceinline__ float ue4m3_value(uint32_t c) {
+  const __half_raw h = __nv_cvt_fp8_to_halfraw(__nv_fp8_storage_t(c), __NV_E4M3);
+  return __half2float(__half(h));
+}
+__device__ __forceinline__ uint32_t fp4x2(float a, float b) {
+  return uint32_t(__nv_cvt_float2_to_fp4x2(make_float2(a, b), __NV_E2M1, cudaRoundNearest));
+}
+
+__global__ void fp4_scale_kernel(const uint32_t* __restrict__ amax_bits, int batch,
+                                 float* __restrict__ gscale, float* __restrict__ out_scale) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= batch) return;
+  const float m = __uint_as_float(amax_bits[c]);
+  const float g = (m > 0.f && m < 3.0e38f) ? m / (6.f * 448.f) : 1.f;
+  gscale[c] = g;
+  out_scale[c] = g * g;
+}
+
+// One thread: one 16-value block (8 complex samples) of one input row.
+__global__ void __launch_bounds__(256) nvfp4_quantize_kernel(
+    const float2* __restrict__ a, uint8_t* __restrict__ z, uint8_t* __restrict__ sf,
+    int64_t rows, int K, int pitch, int sfpitch, int n, const float* __restrict__ gscale) {
+  const int blocks_per_row = pitch / 8;  // 8 bytes of E2M1 per block
+  const int64_t total = rows * blocks_per_row;
+  for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = idx / blocks_per_row;
+    const int b = int(idx - r * blocks_per_row);
+    const int t0 = 8 * b;
+    float x[16];
+    float amax = 0.f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int t = t0 + q;
+      const float2 v = (t < K) ? __ldg(a + r * K + t) : make_float2(0.f, 0.f);
+      x[2 * q] = v.x;
+      x[2 * q + 1] = v.y;
+      amax = fmaxf(amax, fmaxf(fabsf(v.x), fabsf(v.y)));
+    }
+    const float g = gscale[r / n];
+    const uint32_t bc = ue4m3_ceil(amax / (6.f * g));
+    const float inv = bc ? 1.f / (g * ue4m3_value(bc)) : 0.f;
+    uint32_t xw[2] = {0u, 0u}, yw[2] = {0u, 0u};
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float re = x[2 * q] * inv, im = x[2 * q + 1] * inv;
+      xw[q >> 2] |= fp4x2(re, im) << (8 * (q & 3));
+      yw[q >> 2] |= fp4x2(im, -re) << (8 * (q & 3));
+    }
+    *reinterpret_cast<uint2*>(z + (2 * r) * pitch + 8 * b) = make_uint2(xw[0], xw[1]);
+    *reinterpret_cast<uint2*>(z + (2 * r + 1) * pitch + 8 * b) = make_uint2(yw[0], yw[1]);
+    sf[(2 * r) * sfpitch + b] = uint8_t(bc);
+    sf[(2 * r + 1) * sfpitch + b] = uint8_t(bc);
+  }
+}
+
+// Block-scaled instruction descriptor: E2M1 x E2M1, UE4M3 scales, FP32
+// accumulate, K-major A and B, K = 64.
+constexpr uint32_t idesc_nvf4(uint32_t M, uint32_t N) {
+  return (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+struct Fp4Args {
+  const TileDesc* tiles;
+  const ChanDesc* chans;
+  int num_tiles;
+  void* out;
+  float alpha, beta;
+  const float* chan_scale;
+  uint32_t* status;
+};
+
+__global__ void __launch_bounds__(k4Threads, 1)
+    herk_fp4_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                       const __grid_constant__ CUtensorMap tmSa, const __grid_constant__ CUtensorMap tmSb,
+                       const Fp4Args args) {
+  extern __shared__ uint8_t smem_dyn[];
+  uint8_t* smem = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + k4Stages * k4StageBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * k4Stages + 5);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const uint32_t smem0 = smem_u32(smem);
+  const uint32_t bar0 = smem_u32(bars);
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (k4Stages + s); };
+  auto sf_bar = [&](int s) { return bar0 + 8u * (2 * k4Stages + s); };
+  auto tfull_bar = [&](int b) { return bar0 + 8u * (3 * k4Stages + b); };
+  auto tempty_bar = [&](int b) { return bar0 + 8u * (3 * k4Stages + 2 + b); };
+  const uint32_t done_bar = bar0 + 8u * (3 * k4Stages + 4);
+  auto a_addr = [&](int s) { return smem0 + uint32_t(s * k4StageBytes); };
+  auto b_addr = [&](int s) { return smem0 + uint32_t(s * k4StageBytes + k4Op); };
+  auto sfa_addr = [&](int s) { return smem0 + uint32_t(s * k4StageBytes + 2 * k4Op); };
+  auto sfb_addr = [&](int s) { return smem0 + uint32_t(s * k4StageBytes + 2 * k4Op + k4Sf); };
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < k4Stages; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+      mbar_init(sf_bar(s), 4);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(tfull_bar(b), 1);
+      mbar_init(tempty_bar(b), 4);
+    }
+    mbar_init(done_bar, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    tma_prefetch_desc(&tmA);
+    tma_prefetch_desc(&tmB);
+    tma_prefetch_desc(&tmSa);
+    tma_prefetch_desc(&tmSb);
+  }
+  if (warp == 1) {
+    tmem_alloc(smem_u32(tmem_slot), 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------------------------ TMA producer
+    if (lane == 0) {
+      int stage = 0, issued = 0;
+      uint32_t phase = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
+        const TileDesc td = args.tiles[t];
+        const ChanDesc cd = args.chans[td.ch];
+        const int32_t rowA = int32_t(cd.row0 + int64_t(td.tj) * k4J);        // x-row view
+        const int32_t rowB = int32_t(2 * (cd.row0 + int64_t(td.ti) * k4I));  // all rows
+        for (int kb = 0; kb < cd.kblocks; ++kb) {
+          if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
+            atomicOr(args.status, kStatusTimeoutProducer);
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(full_bar(stage), k4StageBytes);
+          tma_load_2d(a_addr(stage), &tmA, kb * k4KB, rowA, full_bar(stage));
+          tma_load_2d(b_addr(stage), &tmB, kb * k4KB, rowB, full_bar(stage));
+          tma_load_2d(sfa_addr(stage), &tmSa, kb * 16, rowA, full_bar(stage));
+          tma_load_2d(sfb_addr(stage), &tmSb, kb * 16, rowB, full_bar(stage));
+          ++issued;
+          if (++stage == k4Stages) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+      }
+      if (!ok) {
+        int s = stage;
+        uint32_t ph = phase;
+        for (int q = 0; q < k4Stages && q < issued; ++q) {
+          if (--s < 0) {
+            s = k4Stages - 1;
+            ph ^= 1u;
+          }
+          volatile int never = 0;
+          if (!mbar_wait(full_bar(s), ph, &never)) atomicOr(args.status, kStatusTimeoutOther);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_nvf4(128, 128);
+      int stage = 0, acc = 0;
+      uint32_t phase = 0, acc_phase = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
+        const ChanDesc cd = args.chans[args.tiles[t].ch];
+        if (!mbar_wait(tempty_bar(acc), acc_phase ^ 1u, abort_flag)) {
+          atomicOr(args.status, kStatusTimeoutMma);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + uint32_t(acc * k4AccCols);
+        for (int kb = 0; kb < cd.kblocks; ++kb) {
+          if (!mbar_wait(full_bar(stage), phase, abort_flag) ||
+              !mbar_wait(sf_bar(stage), phase, abort_flag)) {
+            atomicOr(args.status, kStatusTimeoutMma);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sf0 = tmem_base + uint32_t(k4SfCol0 + stage * k4SfColsPerStage);
+#pragma unroll
+          for (int s = 0; s < 4; ++s) {
+            mma_nvf4(d, sdesc_sw128_kmajor(a_addr(stage) + 32 * s),
+                     sdesc_sw128_kmajor(b_addr(stage) + 32 * s), idesc, sf0 + 4 * s,
+                     sf0 + 16 + 4 * s, (kb | s) != 0);
+          }
+          mma_commit(empty_bar(stage));
+          if (++stage == k4Stages) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+        if (!ok) break;
+        mma_commit(tfull_bar(acc));
+        if (++acc == 2) {
+          acc = 0;
+          acc_phase ^= 1u;
+        }
+      }
+      mma_commit(done_bar);
+      volatile int never = 0;
+      if (!mbar_wait(done_bar, 0, &never)) atomicOr(args.status, kStatusTimeoutOther);
+    }
+  } else if (warp >= 6) {
+    // ------------------------------------------------ scale factors -> TMEM
+    // Warp w fills its lane quarter (w % 4) with the replicated layout: lane
+    // l, column c of a k-step holds the 4 block scales of row l + 32c.
+    const int q = warp & 3;
+    const uint32_t lane_base = uint32_t(q * 32) << 16;
+    int stage = 0;
+    uint32_t phase = 0;
+    for (int t = blockIdx.x; t < args.num_tiles; t += gridDim.x) {
+      const ChanDesc cd = args.chans[args.tiles[t].ch];
+      bool ok = true;
+      for (int kb = 0; kb < cd.kblocks; ++kb) {
+        ok = __all_sync(0xffffffffu, mbar_wait(full_bar(stage), phase, abort_flag));
+        if (!ok) break;
+        uint32_t wa[16], wb[16];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const uint4 va = *reinterpret_cast<const uint4*>(smem + (sfa_addr(stage) - smem0) +
+                                                           16 * (lane + 32 * c));
+          const uint4 vb = *reinterpret_cast<const uint4*>(smem + (sfb_addr(stage) - smem0) +
+                                                           16 * (lane + 32 * c));
+          wa[0 * 4 + c] = va.x; wa[1 * 4 + c] = va.y; wa[2 * 4 + c] = va.z; wa[3 * 4 + c] = va.w;
+          wb[0 * 4 + c] = vb.x; wb[1 * 4 + c] = vb.y; wb[2 * 4 + c] = vb.z; wb[3 * 4 + c] = vb.w;
+        }
+        const uint32_t col = tmem_base + lane_base + uint32_t(k4SfCol0 + stage * k4SfColsPerStage);
+        __syncwarp();
+        tmem_st_32x32b_x16(col, wa);
+        tmem_st_32x32b_x16(col + 16, wb);
+        tmem_wait_st();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(sf_bar(stage));
+        if (++stage == k4Stages) {
+          stage = 0;
+          phase ^= 1u;
+        }
+      }
+      if (!ok) {
+        if (lane == 0) atomicOr(args.status, kStatusTimeoutOther);
+        break;
+      }
+    }
+  } else {
+    // ------------------------------------------------ epilogue (warps 2..5)
+    const int q = warp & 3;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    float2* out = static_cast<float2*>(args.out);
+    for (int t = blockIdx.x; t < args.num_tiles; t += gridDim.x) {
+      const TileDesc td = args.tiles[t];
+      const ChanDesc cd = args.chans[td.ch];
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(tfull_bar(acc), acc_phase, abort_flag));
+      if (!ok) {
+        if (lane == 0) atomicOr(args.status, kStatusTimeoutEpilogue);
+        break;
+      }
+      tc_fence_after();
+      const int n = cd.n;
+      const int jw = int(td.tj) * k4J + q * 32;
+      const int j = jw + lane;
+      const int ib = int(td.ti) * k4I;
+      const float sc = args.alpha * (args.chan_scale ? args.chan_scale[td.ch] : 1.f);
+      float2* outc = out + cd.out0;
+      const uint32_t tb = tmem_base + (uint32_t(q * 32) << 16) + uint32_t(acc * k4AccCols);
+#pragma unroll 1
+      for (int c = 0; c < k4AccCols / 32; ++c) {
+        const int i0 = ib + 16 * c;
+        if (i0 + 15 < jw || i0 >= n) continue;
+        uint32_t r[32];
+        __syncwarp();
+        tmem_ld_32x32b_x32(tb + 32u * c, r);
+        tmem_wait_ld();
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+          const int i = i0 + m;
+          if (i < n && j <= i) {
+            float vr = __uint_as_float(r[2 * m]) * sc;
+            float vi = (i == j) ? 0.f : __uint_as_float(r[2 * m + 1]) * sc;
+            float2* p = outc + int64_t(i) * (i + 1) / 2 + j;
+            if (args.beta != 0.f) {
+              const float2 o = *p;
+              vr += args.beta * o.x;
+              vi += args.beta * o.y;
+            }
+            __stcs(p, make_float2(vr, vi));
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tempty_bar(acc));
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1u;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem_base, 512);
+  }
+}
+
+}  // namespace
+
+// Workspace: E2M1 operand rows (2 per input), then their scale bytes.
+size_t nvfp4_workspace_bytes(int64_t rows, int K) {
+  const int64_t pitch = (2 * int64_t(K) + 255) / 256 * 128;  // bytes per operand row
+  return size_t(2 * rows * pitch) + size_t(2 * rows * (pitch / 8)) + 2048;
+}
+
+int nvfp4_kblocks(int K) { return int((2 * int64_t(K) + 255) / 256); }
+
+cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, uint8_t* ws,
+                         float* gscale, float* out_scale, uint32_t* amax_bits,
+                         const TileDesc* tiles, const ChanDesc* chans, int num_tiles, void* C,
+                         float alpha, float beta, uint32_t* status, int sm_count, void* encode_fn,
+                         cudaStream_t s) {
+  auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(encode_fn);
+  if (!encode) return cudaErrorInvalidValue;
+  const int64_t pitch = (2 * int64_t(K) + 255) / 256 * 128;
+  const int64_t sfpitch = pitch / 8;
+  uint8_t* z = ws;
+  uint8_t* sf = ws + ((2 * rows * pitch + 1023) / 1024) * 1024;
+  // channel amax -> global scales -> quantise
+  cudaError_t e = cudaMemsetAsync(amax_bits, 0, sizeof(uint32_t) * size_t(batch), s);
+  if (e != cudaSuccess) return e;
+  e = launch_channel_amax(A, int64_t(n) * K, batch, amax_bits, sm_count, s);
+  if (e != cudaSuccess) return e;
+  fp4_scale_kernel<<<(batch + 127) / 128, 128, 0, s>>>(amax_bits, batch, gscale, out_scale);
+  const int64_t work = rows * (pitch / 8);
+  int64_t blocks = (work + 255) / 256;
+  if (blocks > int64_t(sm_count) * 16) blocks = int64_t(sm_count) * 16;
+  nvfp4_quantize_kernel<<<unsigned(blocks), 256, 0, s>>>(static_cast<const float2*>(A), z, sf,
+                                                          rows, K, int(pitch), int(sfpitch), n,
+                                                          gscale);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+
+  CUtensorMap tmA, tmB, tmSa, tmSb;
+  const cuuint32_t estr[2] = {1, 1};
+  auto enc2 = [&](CUtensorMap* m, void* base, int64_t inner, int64_t nrows, int64_t stride,
+                  uint32_t box0, CUtensorMapSwizzle sw) {
+    const cuuint64_t dims[2] = {cuuint64_t(inner), cuuint64_t(nrows)};
+    const cuuint64_t str[1] = {cuuint64_t(stride)};
+    const cuuint32_t box[2] = {box0, 128};
+    return encode(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, str, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  };
+  if (enc2(&tmA, z, pitch, rows, 2 * pitch, k4KB, CU_TENSOR_MAP_SWIZZLE_128B) != CUDA_SUCCESS ||
+      enc2(&tmB, z, pitch, 2 * rows, pitch, k4KB, CU_TENSOR_MAP_SWIZZLE_128B) != CUDA_SUCCESS ||
+      enc2(&tmSa, sf, sfpitch, rows, 2 * sfpitch, 16, CU_TENSOR_MAP_SWIZZLE_NONE) != CUDA_SUCCESS ||
+      enc2(&tmSb, sf, sfpitch, 2 * rows, sfpitch, 16, CU_TENSOR_MAP_SWIZZLE_NONE) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  Fp4Args args{tiles, chans, num_tiles, C, alpha, beta, out_scale, status};
+  static bool attr = false;
+  if (!attr) {
+    e = cudaFuncSetAttribute(herk_fp4_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(k4Smem));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const int grid = num_tiles < sm_count ? num_tiles : sm_count;
+  herk_fp4_tc_kernel<<<grid, k4Threads, k4Smem, s>>>(tmA, tmB, tmSa, tmSb, args);
+  return cudaGetLastError();
+}
+
+}  // namespace ftdx

@@ -111,6 +111,17 @@ __global__ void __launch_bounds__(256) quantize_kernel(const float2* __restrict_
 
 }  // namespace
 
+cudaError_t launch_channel_amax(const void* a, int64_t per_chan, int batch, uint32_t* amax_bits,
+                                int sm_count, cudaStream_t s) {
+  int bx = int((per_chan + 256 * 8 - 1) / (256 * 8));
+  const int cap = (sm_count * 8 + batch - 1) / batch;
+  if (bx > cap) bx = cap;
+  if (bx < 1) bx = 1;
+  amax_kernel<<<dim3(unsigned(bx), unsigned(batch)), 256, 0, s>>>(static_cast<const float2*>(a),
+                                                                   per_chan, amax_bits);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_float_to_planes(const void* a, uint8_t* z, int64_t rows, int K, int Kp,
                                    int zpitch, int n, int batch, int split, float* qscale,
                                    float* out_scale, uint32_t* amax_bits, int sm_count,

@@ -87,3 +87,37 @@ def test_kahan_accumulation_across_dumps():
     assert np.abs(exact).max() > 2 ** 24          # beyond FP32's exact-integer range
     assert err_k <= 2.0                            # compensated: ~exact
     assert err_n > 4 * max(err_k, 0.5)             # plain FP32 accumulation drifts
+
+
+# ---------------------------------------------------------------- NVFP4
+E2M1 = np.array([0.0, 0.5, 1.0, 1.5, 2.0, 3.0, 4.0, 6.0])
+
+
+def test_nvfp4_exactly_representable_input_is_exact():
+    # Every block of 8 complex samples holds E2M1 values times a per-block power
+    # of two, with one component at 6 x that power: the quantiser's block scales
+    # come out exact (448, 224, 112 in UE4M3) and so does every product, so the
+    # NVFP4 result must equal FP64 rounded to FP32.  Catches any mistake in the
+    # packing, scale-factor layout or tile walk.
+    from ftd_b200._lib import COMPUTE_FP4
+    rng = np.random.default_rng(90)
+    B, N, K = 2, 130, 256
+    e = rng.choice(E2M1, size=(B, N, K, 2)) * rng.choice([-1.0, 1.0], size=(B, N, K, 2))
+    blocks = e.reshape(B, N, K // 8, 16)
+    blocks[..., 0] = 6.0                              # the block maximum
+    pw = 2.0 ** rng.integers(-2, 1, size=(B, N, K // 8, 1))
+    pw[:, 0, 0, 0] = 1.0                              # channel max = 6
+    v = (blocks * pw).reshape(B, N, K, 2)
+    vc = (v[..., 0] + 1j * v[..., 1]).astype(np.complex64)
+    got = run_float(vc, COMPUTE_FP4)
+    ref = oracle.herk_c128(vc.astype(np.complex128), N, K, B).astype(np.float32)
+    assert np.array_equal(got, ref), np.abs(got - ref).max()
+
+
+def test_nvfp4_error(workload):
+    from ftd_b200._lib import COMPUTE_FP4
+    v, ref = workload
+    err = oracle.correlation_errors(run_float(v, COMPUTE_FP4), ref, v.shape[1])
+    print("nvfp4", err)
+    # E2M1 with block-16 scales: ~10% per sample; normalised by sqrt(R_ii R_jj)
+    assert err["rms_norm"] < 1e-2 and err["max_norm"] < 6e-2
