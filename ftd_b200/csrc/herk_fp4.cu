@@ -107,6 +107,23 @@ __global__ void __launch_bounds__(256) nvfp4_quantize_kernel(
   }
 }
 
+// Autocorrelation of every input row, sum_t |v_t|^2, accumulated in FP64
+// (one warp per row).
+__global__ void __launch_bounds__(256) row_power_kernel(const float2* __restrict__ a, int64_t rows,
+                                                        int K, float* __restrict__ power) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < rows;
+       r += (int64_t(gridDim.x) * blockDim.x) >> 5) {
+    double acc = 0.0;
+    for (int t = lane; t < K; t += 32) {
+      const float2 v = __ldg(a + r * K + t);
+      acc += double(v.x) * v.x + double(v.y) * v.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) power[r] = float(acc);
+  }
+}
+
 // Block-scaled instruction descriptor: E2M1 x E2M1, UE4M3 scales, FP32
 // accumulate, K-major A and B, K = 64.
 constexpr uint32_t idesc_nvf4(uint32_t M, uint32_t N) {
@@ -121,6 +138,7 @@ struct Fp4Args {
   float alpha, beta;
   const float* chan_scale;
   uint32_t* status;
+  const float* row_power;  // exact sum_t |v_t|^2 per input row (the autocorrelations)
 };
 
 __global__ void __launch_bounds__(k4Threads, 1)
@@ -340,7 +358,10 @@ __global__ void __launch_bounds__(k4Threads, 1)
         for (int m = 0; m < 16; ++m) {
           const int i = i0 + m;
           if (i < n && j <= i) {
-            float vr = __uint_as_float(r[2 * m]) * sc;
+            // autocorrelations come from the FP32 power pass: their NVFP4
+            // estimate would carry the quantisation-noise power as a bias
+            float vr = (i == j) ? args.row_power[cd.row0 + i] * args.alpha
+                                : __uint_as_float(r[2 * m]) * sc;
             float vi = (i == j) ? 0.f : __uint_as_float(r[2 * m + 1]) * sc;
             float2* p = outc + int64_t(i) * (i + 1) / 2 + j;
             if (args.beta != 0.f) {
@@ -375,7 +396,7 @@ __global__ void __launch_bounds__(k4Threads, 1)
 // Workspace: E2M1 operand rows (2 per input), then their scale bytes.
 size_t nvfp4_workspace_bytes(int64_t rows, int K) {
   const int64_t pitch = (2 * int64_t(K) + 255) / 256 * 128;  // bytes per operand row
-  return size_t(2 * rows * pitch) + size_t(2 * rows * (pitch / 8)) + 2048;
+  return size_t(2 * rows * pitch) + size_t(2 * rows * (pitch / 8)) + size_t(4 * rows) + 4096;
 }
 
 int nvfp4_kblocks(int K) { return int((2 * int64_t(K) + 255) / 256); }
@@ -391,6 +412,7 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
   const int64_t sfpitch = pitch / 8;
   uint8_t* z = ws;
   uint8_t* sf = ws + ((2 * rows * pitch + 1023) / 1024) * 1024;
+  float* power = reinterpret_cast<float*>(sf + ((2 * rows * sfpitch + 1023) / 1024) * 1024);
   // channel amax -> global scales -> quantise
   cudaError_t e = cudaMemsetAsync(amax_bits, 0, sizeof(uint32_t) * size_t(batch), s);
   if (e != cudaSuccess) return e;
@@ -422,7 +444,14 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
       enc2(&tmSa, sf, sfpitch, rows, 2 * sfpitch, 16, CU_TENSOR_MAP_SWIZZLE_NONE) != CUDA_SUCCESS ||
       enc2(&tmSb, sf, sfpitch, 2 * rows, sfpitch, 16, CU_TENSOR_MAP_SWIZZLE_NONE) != CUDA_SUCCESS)
     return cudaErrorInvalidValue;
-  Fp4Args args{tiles, chans, num_tiles, C, alpha, beta, out_scale, status};
+  {
+    int64_t pb = (rows * 32 + 255) / 256;
+    if (pb > int64_t(sm_count) * 16) pb = int64_t(sm_count) * 16;
+    row_power_kernel<<<unsigned(pb), 256, 0, s>>>(static_cast<const float2*>(A), rows, K, power);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  Fp4Args args{tiles, chans, num_tiles, C, alpha, beta, out_scale, status, power};
   static bool attr = false;
   if (!attr) {
     e = cudaFuncSetAttribute(herk_fp4_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -198,7 +198,10 @@ def correlation_errors(got: np.ndarray, ref: np.ndarray, N: int) -> dict:
     norm = np.sqrt(np.maximum(auto[:, i] * auto[:, j], 1e-300))
     e = np.abs(g - r) / norm
     de = np.abs(g[:, diag].real - auto) / np.maximum(auto, 1e-300)
+    off = e[:, i != j]
     return {"max_norm": float(e.max()), "rms_norm": float(np.sqrt(np.mean(e ** 2))),
+            "max_offdiag_norm": float(off.max()) if off.size else 0.0,
+            "rms_offdiag_norm": float(np.sqrt(np.mean(off ** 2))) if off.size else 0.0,
             "max_auto_rel": float(de.max()), "rms_auto_rel": float(np.sqrt(np.mean(de ** 2)))}
 
 

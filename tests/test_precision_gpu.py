@@ -96,9 +96,10 @@ E2M1 = np.array([0.0, 0.5, 1.0, 1.5, 2.0, 3.0, 4.0, 6.0])
 def test_nvfp4_exactly_representable_input_is_exact():
     # Every block of 8 complex samples holds E2M1 values times a per-block power
     # of two, with one component at 6 x that power: the quantiser's block scales
-    # come out exact (448, 224, 112 in UE4M3) and so does every product, so the
-    # NVFP4 result must equal FP64 rounded to FP32.  Catches any mistake in the
-    # packing, scale-factor layout or tile walk.
+    # come out exact (448, 224, 112 in UE4M3) and so does every element, so the
+    # only error left is FP32 rounding (of the accumulation and of the channel
+    # scale g^2, which is not a power of two): rtol 1e-6.  Any mistake in the
+    # packing, scale-factor layout or tile walk shows up as O(1) errors.
     from ftd_b200._lib import COMPUTE_FP4
     rng = np.random.default_rng(90)
     B, N, K = 2, 130, 256
@@ -110,8 +111,10 @@ def test_nvfp4_exactly_representable_input_is_exact():
     v = (blocks * pw).reshape(B, N, K, 2)
     vc = (v[..., 0] + 1j * v[..., 1]).astype(np.complex64)
     got = run_float(vc, COMPUTE_FP4)
-    ref = oracle.herk_c128(vc.astype(np.complex128), N, K, B).astype(np.float32)
-    assert np.array_equal(got, ref), np.abs(got - ref).max()
+    ref = oracle.herk_c128(vc.astype(np.complex128), N, K, B)
+    err = np.abs(got - ref).max() / np.abs(ref).max()
+    print("nvfp4 exact-input max rel err", err)
+    assert err < 1e-6
 
 
 def test_nvfp4_error(workload):
@@ -119,5 +122,7 @@ def test_nvfp4_error(workload):
     v, ref = workload
     err = oracle.correlation_errors(run_float(v, COMPUTE_FP4), ref, v.shape[1])
     print("nvfp4", err)
-    # E2M1 with block-16 scales: ~10% per sample; normalised by sqrt(R_ii R_jj)
-    assert err["rms_norm"] < 1e-2 and err["max_norm"] < 6e-2
+    # E2M1 with block-16 scales: ~17% RMS quantisation noise per sample, i.e.
+    # ~0.17 sqrt(2/K) per normalised cross-correlation; autocorrelations exact
+    assert err["rms_offdiag_norm"] < 1e-2 and err["max_offdiag_norm"] < 5e-2
+    assert err["max_auto_rel"] < 1e-5
