@@ -353,9 +353,11 @@ def run_ours(args, rank, world, dist):
     if not args.no_e2e:
         e2e = run_e2e(torch, args, dev, qc, N, K, B, flops, world, dist)
 
-    batched = None
+    batched = precision = differentiation = None
     if not args.no_extra:
         batched = run_batched_leg(torch, dev)
+        precision = run_precision_leg(torch, dev)
+        differentiation = run_diff_leg(torch, dev)
 
     peak = None
     if not args.no_peak:
@@ -397,6 +399,8 @@ def run_ours(args, rank, world, dist):
         "speedup_vs_plain": (value / world / plain["value"]) if plain else None,
         "e2e": e2e,
         "batched_uneven_flagged": batched,
+        "precision_modes": precision,
+        "adjoint_and_gain_gradient": differentiation,
         "clocks": clk,
     }
     if world == 1 and not args.no_cpu_baseline:
@@ -445,6 +449,116 @@ def run_batched_leg(torch, dev, seed=3, n_chans=96, inputs=4096):
                         f"1536..{inputs} active after flagging, one call (tuned, graph replay)",
             "value": flops / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms,
             "tflop_per_step": flops / 1e12}
+
+
+def _timed(torch, fn, reps=5, warm=2):
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_precision_leg(torch, dev, N=4096, B=64, K=1024, seed=4, n_err=512):
+    """Float complex voltages, 4096 inputs x 64 channels x K=1024: per-channel
+    RMS log-uniform in [0.1, 10]; 1% of time samples carry 20-sigma bursts on
+    5% of the inputs.  Throughput of each compute mode, and its error against
+    an FP64 correlation (torch, on the device) of the first n_err inputs of
+    two channels: |dR_ij| / sqrt(R_ii R_jj), cross- and auto-correlations."""
+    from ftd_b200 import Correlator, tri_size
+    from ftd_b200._lib import (COMPUTE_FP4, COMPUTE_FP8, COMPUTE_FP8_SPLIT, IN_FP32,
+                               OUT_FP32)
+    g = torch.Generator(device=dev).manual_seed(seed)
+    rms = torch.exp(torch.empty(B, device=dev).uniform_(float(__import__("math").log(0.1)),
+                                                         float(__import__("math").log(10.0)),
+                                                         generator=g))
+    V = torch.randn(B, N, K, 2, device=dev, generator=g) * (rms.view(B, 1, 1, 1) / 2 ** 0.5)
+    n_rfi, t_rfi = max(1, N // 20), max(1, K // 100)
+    for b in range(B):
+        ins = torch.randperm(N, device=dev, generator=g)[:n_rfi]
+        ts = torch.randperm(K, device=dev, generator=g)[:t_rfi]
+        ph = torch.rand(n_rfi, t_rfi, device=dev, generator=g) * (2 * 3.141592653589793)
+        amp = 20.0 * rms[b]
+        sub = torch.stack([amp * torch.cos(ph), amp * torch.sin(ph)], -1)
+        V[b, ins[:, None], ts[None, :]] = sub
+    C = torch.empty(B, tri_size(N), 2, device=dev)
+    flops = herk_flops(N, K, B)
+    # FP64 reference of the first n_err inputs of channels 0 and 1
+    Vs = torch.view_as_complex(V[:2, :n_err].double().contiguous())
+    Rref = Vs @ Vs.conj().transpose(1, 2)
+    ii, jj = torch.tril_indices(n_err, n_err, device=dev)
+    order = torch.argsort(ii * n_err + jj)
+    ii, jj = ii[order], jj[order]
+    ref = Rref[:, ii, jj]
+    auto = torch.diagonal(Rref, dim1=1, dim2=2).real
+    norm = torch.sqrt(auto[:, ii] * auto[:, jj])
+    off = ii != jj
+    out = {}
+    with Correlator(device=dev.index) as c:
+        for name, mode in [("fp8_channel_scaled", COMPUTE_FP8), ("fp8_hi_lo_split", COMPUTE_FP8_SPLIT),
+                           ("nvfp4_block16", COMPUTE_FP4)]:
+            def step():
+                c.herk(V, C, N, K, B, input=IN_FP32, compute=mode, output=OUT_FP32, tune=False)
+            ms = _timed(torch, step)
+            if c.device_status() != 0:
+                raise RuntimeError("device wait timed out in the precision leg")
+            got = torch.view_as_complex(C[:2, :tri_size(n_err)].double().contiguous())
+            e = (got - ref).abs() / norm
+            out[name] = {"value": flops / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms,
+                         "max_rel_err_cross": float(e[:, off].max()),
+                         "rms_rel_err_cross": float(e[:, off].pow(2).mean().sqrt()),
+                         "max_rel_err_auto": float(e[:, ~off].max())}
+    del V, C
+    out["workload"] = (f"{N} inputs x {B} channels x K={K}, float complex Gaussian, RMS "
+                       f"log-uniform [0.1, 10], 1% of samples 20-sigma bursts on 5% of inputs; "
+                       f"errors |dR|/sqrt(R_ii R_jj) vs FP64 on the first {n_err} inputs of 2 "
+                       f"channels")
+    return out
+
+
+def run_diff_leg(torch, dev, N=2048, B=32, K=512, seed=5):
+    """Adjoint dV = (G + G^H) V (G random Hermitian complex64, V int4) and the
+    gain-calibration gradient, 2048 inputs x 32 channels x K=512."""
+    from ftd_b200 import Correlator, tri_size
+    from ftd_b200._lib import IN_INT4, OUT_FP32
+    g = torch.Generator(device=dev).manual_seed(seed)
+    qc = make_qc(torch, B, N, K, dev, seed=seed)
+    qm = make_qc(torch, B, N, K, dev, seed=seed + 1)
+    A = torch.view_as_complex(torch.randn(B, N, N, 2, device=dev, generator=g))
+    G = torch.view_as_real(((A + A.conj().transpose(1, 2)) / 2).contiguous()).contiguous()
+    del A
+    dV = torch.empty(B, N, K, 2, device=dev)
+    P = tri_size(N)
+    Ro = torch.empty(B, P, 2, device=dev)
+    Rm = torch.empty_like(Ro)
+    W = torch.rand(B, P, device=dev, generator=g)
+    ph = torch.rand(N, device=dev, generator=g) * 6.283185307179586
+    mag = 1.0 + (torch.rand(N, device=dev, generator=g) - 0.5) * 0.2
+    gains = torch.stack([mag * torch.cos(ph), mag * torch.sin(ph)], -1).contiguous()
+    grad = torch.empty(N, 2, dtype=torch.float64, device=dev)
+    loss = torch.empty(1, dtype=torch.float64, device=dev)
+    with Correlator(device=dev.index) as c:
+        c.herk(qc, Ro, N, K, B, input=IN_INT4, output=OUT_FP32)
+        c.herk(qm, Rm, N, K, B, input=IN_INT4, output=OUT_FP32)
+        ms_adj = _timed(torch, lambda: c.herk_adjoint(G, qc, dV, N, K, B))
+        ms_gg = _timed(torch, lambda: c.gain_gradient(Ro, Rm, W, gains, N, B, grad, loss))
+        if c.device_status() != 0:
+            raise RuntimeError("device wait timed out in the differentiation leg")
+    adj_flops = 8.0 * N * N * K * B
+    gg_bytes = float(B) * P * (8 + 8 + 4)
+    return {"workload": f"{N} inputs x {B} channels x K={K}",
+            "adjoint": {"value": adj_flops / (ms_adj * 1e-3) / 1e12, "unit": UNIT,
+                        "ms_per_step": ms_adj,
+                        "note": "8 N^2 K per channel; executed as bf16 hi + lo (2x that on "
+                                "the tensor cores), plus the G + G^H split pass"},
+            "gain_gradient": {"value": gg_bytes / (ms_gg * 1e-3) / 1e9, "unit": "GB/s",
+                              "ms_per_step": ms_gg, "bytes_per_step": gg_bytes}}
 
 
 def run_e2e(torch, args, dev, qc_dev, N, K, B, flops, world, dist):

@@ -176,6 +176,8 @@ def workload4_voltages(seed: int, batch: int, N: int, K: int, rfi_time_frac: flo
     v = (rng.normal(size=(batch, N, K)) + 1j * rng.normal(size=(batch, N, K))) / np.sqrt(2.0)
     v *= rms[:, None, None]
     for b in range(batch):
+        if rfi_time_frac <= 0 or rfi_input_frac <= 0:
+            break
         ins = rng.choice(N, size=max(1, int(round(rfi_input_frac * N))), replace=False)
         ts = rng.choice(K, size=max(1, int(round(rfi_time_frac * K))), replace=False)
         phase = np.exp(2j * np.pi * rng.uniform(size=(len(ins), len(ts))))

@@ -123,6 +123,18 @@ def test_nvfp4_error(workload):
     err = oracle.correlation_errors(run_float(v, COMPUTE_FP4), ref, v.shape[1])
     print("nvfp4", err)
     # E2M1 with block-16 scales: ~17% RMS quantisation noise per sample, i.e.
-    # ~0.17 sqrt(2/K) per normalised cross-correlation; autocorrelations exact
-    assert err["rms_offdiag_norm"] < 1e-2 and err["max_offdiag_norm"] < 5e-2
+    # ~0.17 sqrt(2/K) per normalised cross-correlation; the largest errors are
+    # between inputs that share 20-sigma bursts (the small component of a
+    # burst sample keeps one mantissa bit).  Autocorrelations are exact.
+    assert err["rms_offdiag_norm"] < 1e-2 and err["max_offdiag_norm"] < 8e-2
     assert err["max_auto_rel"] < 1e-5
+
+
+def test_nvfp4_error_without_rfi():
+    from ftd_b200._lib import COMPUTE_FP4
+    B, N, K = 4, 256, 1024
+    v = oracle.workload4_voltages(406, B, N, K, rfi_time_frac=0.0, rfi_input_frac=0.0)
+    ref = oracle.herk_c128(v.astype(np.complex128), N, K, B)
+    err = oracle.correlation_errors(run_float(v, COMPUTE_FP4), ref, N)
+    print("nvfp4 no-rfi", err)
+    assert err["rms_offdiag_norm"] < 1e-2 and err["max_offdiag_norm"] < 3e-2
