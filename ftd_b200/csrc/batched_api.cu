@@ -209,7 +209,7 @@ extern "C" ftdx_status ftdx_herk_batched_v(ftdx_handle h, const ftdx_channel_des
       TuneEntry best;
       ftdx_status st = tune_sweep(
           h, [&](const Strategy& cand, cudaStream_t ss) { return launch_v(h, call, cand, ss); },
-          default_candidates(h, output == FTDX_OUT_FP32), s, &best);
+          default_candidates(h, output == FTDX_OUT_FP32, false), s, &best);
       if (st != FTDX_OK) return st;
       record_tuned(h, key, best);
       strat = best.st;

@@ -29,7 +29,9 @@ struct Plan {
 
 // Launch strategy of the correlator kernel; chosen by the autotuner.
 struct Strategy {
-  int store_mode = 0;  // 0: direct stores, 1: shared-memory staging + bulk copies
+  // 0: direct stores, 1: shared-memory staging + bulk copies,
+  // 2: CTA-pair kernel (256 x 128 tiles on two SMs, direct stores)
+  int store_mode = 0;
   int grid = 0;        // persistent CTAs (0: one per SM); -1: one CTA per tile (not persistent)
   bool operator==(const Strategy& o) const {
     return store_mode == o.store_mode && grid == o.grid;
@@ -74,6 +76,7 @@ struct GraphEntry {
 struct ftdx_context {
   int device = 0;
   int sm_count = 148;
+  int pair_grid = -1;  // cached pair_grid_limit (-1: not queried yet)
   int verbosity = 0;
   std::string device_name;
   std::string last_error;
@@ -115,10 +118,13 @@ ftdx_status cuda_fail(ftdx_handle h, cudaError_t e, const char* what);
 bool stream_capturing(cudaStream_t s);
 ftdx_status ensure_workspace(ftdx_handle h, size_t bytes, cudaStream_t s);
 ftdx_status ensure_aux(ftdx_handle h, size_t bytes, cudaStream_t s);
+// pair: tiles of the CTA-pair kernel (tj over 256 inputs, ti over 128)
 ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
-                     const Plan** out);
+                     const Plan** out, bool pair = false);
 ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t Kp,
-                              CUtensorMap* tm);
+                              CUtensorMap* tm, int box_rows = kTile);
+// Even number of CTAs of the pair kernel that can be resident at once.
+int pair_grid_limit(ftdx_handle h);
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 void* tensor_map_encoder();  // cuTensorMapEncodeTiled through the runtime
 
@@ -137,7 +143,7 @@ void load_tune_cache(ftdx_handle h);
 
 // Autotuning and graph replay shared by the correlator entry points.
 using LaunchFn = std::function<ftdx_status(const Strategy&, cudaStream_t)>;
-std::vector<Strategy> default_candidates(ftdx_handle h, bool fp32_out);
+std::vector<Strategy> default_candidates(ftdx_handle h, bool fp32_out, bool pair_ok);
 ftdx_status tune_sweep(ftdx_handle h, const LaunchFn& launch, const std::vector<Strategy>& cands,
                        cudaStream_t s, TuneEntry* best);
 void record_tuned(ftdx_handle h, const TuneKey& k, const TuneEntry& e);

@@ -8,6 +8,8 @@
 #include <cstdlib>
 #include <cstring>
 
+#include <algorithm>
+
 #include "context.h"
 
 namespace ftdx {
@@ -108,8 +110,9 @@ ftdx_status ensure_aux(ftdx_handle h, size_t bytes, cudaStream_t s) {
 // Lower-triangle tile list for `batch` channels of N inputs, channel-major so
 // that concurrently running CTAs share a channel's operand in L2.
 ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
-                     const Plan** out) {
-  auto key = std::make_tuple(N, kblocks, batch);
+                     const Plan** out, bool pair) {
+  // kblocks < 2^23 (K <= 2^30), so pair plans never share a key with others
+  auto key = std::make_tuple(N, pair ? kblocks + (1 << 24) : kblocks, batch);
   auto it = h->plans.find(key);
   if (it != h->plans.end()) {
     *out = it->second.get();
@@ -130,7 +133,8 @@ ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t 
     chans[c].out0 = int64_t(c) * (int64_t(N) * (N + 1) / 2);
     chans[c].out_ptr = 0;
     for (int ti = 0; ti < nb; ++ti)
-      for (int tj = 0; tj <= ti; ++tj) tiles.push_back(TileDesc{c, uint16_t(ti), uint16_t(tj)});
+      for (int tj = 0; tj <= (pair ? ti / 2 : ti); ++tj)
+        tiles.push_back(TileDesc{c, uint16_t(ti), uint16_t(tj)});
   }
   auto p = std::make_unique<Plan>();
   p->num_tiles = int(tiles.size());
@@ -149,16 +153,28 @@ ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t 
   return FTDX_OK;
 }
 
+int pair_grid_limit(ftdx_handle h) {
+  if (h->pair_grid < 0) {
+    int clusters = 0;
+    if (herk_fp8_pair_max_clusters(h->sm_count, &clusters) != cudaSuccess) {
+      cudaGetLastError();
+      clusters = 0;
+    }
+    h->pair_grid = 2 * std::min(clusters, h->sm_count / 2);
+  }
+  return h->pair_grid;
+}
+
 // Tensor map over the operand planes Z[2][rows][Kp] (bytes): box of
-// 128 samples x 128 rows x 1 plane, 128-byte swizzle.
+// 128 samples x box_rows rows x 1 plane, 128-byte swizzle.
 ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t Kp,
-                              CUtensorMap* tm) {
+                              CUtensorMap* tm, int box_rows) {
   auto enc = get_encode_fn();
   if (!enc) return fail(h, FTDX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
   const cuuint32_t estr[3] = {1, 1, 1};
   const cuuint64_t dims[3] = {cuuint64_t(Kp), cuuint64_t(rows), 2};
   const cuuint64_t strides[2] = {cuuint64_t(Kp), cuuint64_t(rows * Kp)};
-  const cuuint32_t box[3] = {cuuint32_t(kStageK), cuuint32_t(kTile), 1};
+  const cuuint32_t box[3] = {cuuint32_t(kStageK), cuuint32_t(box_rows), 1};
   CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, z, dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);

@@ -4,6 +4,7 @@
 // tune_herk / strategy_cache::run_autotune (cutlass_gemm_api.cu:1389-1409,
 // strategy_cache.hpp:504-721) and the direct-HERK graph cache
 // (cutlass_gemm_api.cu:200-315, 1738-1807) of the reference.
+#include <algorithm>
 #include <cerrno>
 #include <cstdio>
 #include <cstring>
@@ -123,8 +124,13 @@ ftdx_status launch_fp4(ftdx_handle h, const HerkCall& c, cudaStream_t s) {
   return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "NVFP4 launch");
 }
 
+bool use_pair(ftdx_handle h, const Strategy& strat) {
+  return strat.store_mode == 2 && pair_grid_limit(h) >= 2;
+}
+
 // Workspace and tile plan for a call; allocates, so never while capturing.
-ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan** plan) {
+ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan** plan,
+                    bool pair = false) {
   const int64_t Kp = round_up(c.K, kStageK);
   const int64_t zpitch = is_split(c) ? 2 * Kp : Kp;
   const int64_t rows = int64_t(c.N) * c.batch;
@@ -134,14 +140,15 @@ ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan
     st = ensure_aux(h, size_t(12) * size_t(c.batch) + 256, s);
     if (st != FTDX_OK) return st;
   }
-  return get_plan(h, c.N, int(Kp / kStageK), c.batch, s, plan);
+  return get_plan(h, c.N, int(Kp / kStageK), c.batch, s, plan, pair);
 }
 
 // Promotion kernel + correlator kernel on stream s.
 ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, cudaStream_t s) {
   if (is_fp4(c)) return launch_fp4(h, c, s);
+  const bool pair = use_pair(h, strat);
   const Plan* plan = nullptr;
-  ftdx_status st = prepare(h, c, s, &plan);
+  ftdx_status st = prepare(h, c, s, &plan, pair);
   if (st != FTDX_OK) return st;
   const int64_t Kp = round_up(c.K, kStageK);
   const int64_t zpitch = is_split(c) ? 2 * Kp : Kp;
@@ -161,8 +168,9 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
                                  is_split(c) ? 1 : 0, qscale, out_scale, amax, h->sm_count, s);
   }
   if (e != cudaSuccess) return cuda_fail(h, e, "operand promotion launch");
-  CUtensorMap tmZ;
+  CUtensorMap tmZ, tmB;
   st = encode_planes_map(h, h->z, rows, zpitch, &tmZ);
+  if (st == FTDX_OK && pair) st = encode_planes_map(h, h->z, rows, zpitch, &tmB, kTile / 2);
   if (st != FTDX_OK) return st;
   HerkArgs args = herk_args_default();
   args.tiles = plan->d_tiles;
@@ -186,11 +194,19 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
     args.kahan = 1;
     args.out2 = c.comp;
   }
-  int grid = strat.grid > 0 ? strat.grid : h->sm_count;
-  if (grid > h->sm_count) grid = h->sm_count;  // persistent: at most one CTA per SM
-  if (strat.grid < 0) grid = plan->num_tiles;   // one tile per CTA
-  if (grid > plan->num_tiles) grid = plan->num_tiles;
-  {
+  if (pair) {
+    // persistent pairs, at most as many as can be resident together
+    const int limit = pair_grid_limit(h);
+    int grid = strat.grid > 0 ? std::min(strat.grid, limit) : limit;
+    if (strat.grid < 0) grid = 2 * plan->num_tiles;
+    grid = std::min(grid, 2 * plan->num_tiles) & ~1;
+    ScopedTimer tm(h, s, 0);
+    e = launch_herk_fp8_pair(tmZ, tmB, args, grid, s);
+  } else {
+    int grid = strat.grid > 0 ? strat.grid : h->sm_count;
+    if (grid > h->sm_count) grid = h->sm_count;  // persistent: at most one CTA per SM
+    if (strat.grid < 0) grid = plan->num_tiles;   // one tile per CTA
+    if (grid > plan->num_tiles) grid = plan->num_tiles;
     ScopedTimer tm(h, s, 0);
     e = launch_herk_fp8(tmZ, args, grid, s);
   }
@@ -214,7 +230,7 @@ ftdx_status run_tune(ftdx_handle h, const HerkCall& c, cudaStream_t s, TuneEntry
   TuneEntry best;
   st = tune_sweep(
       h, [&](const Strategy& cand, cudaStream_t ss) { return launch_all(h, c, cand, ss); },
-      default_candidates(h, c.output == FTDX_OUT_FP32), s, &best);
+      default_candidates(h, c.output == FTDX_OUT_FP32, !is_fp4(c)), s, &best);
   if (st != FTDX_OK) return st;
   record_tuned(h, tune_key(h, c), best);
   if (out) *out = best;
@@ -229,20 +245,22 @@ ftdx_status run_graph(ftdx_handle h, const HerkCall& c, const Strategy& strat, c
       h, key,
       [&](cudaStream_t ss) {
         const Plan* plan = nullptr;
-        return ss == h->capture_stream ? launch_all(h, c, strat, ss) : prepare(h, c, ss, &plan);
+        return ss == h->capture_stream ? launch_all(h, c, strat, ss)
+                                       : prepare(h, c, ss, &plan, use_pair(h, strat));
       },
       s);
 }
 
 }  // namespace
 
-std::vector<Strategy> default_candidates(ftdx_handle h, bool fp32_out) {
+std::vector<Strategy> default_candidates(ftdx_handle h, bool fp32_out, bool pair_ok) {
   std::vector<Strategy> v;
   const int grids[2] = {h->sm_count, h->sm_count - h->sm_count / 8};
   for (int g : grids) {
     v.push_back(Strategy{0, g});
     if (fp32_out) v.push_back(Strategy{1, g});
   }
+  if (pair_ok && pair_grid_limit(h) >= 2) v.push_back(Strategy{2, pair_grid_limit(h)});
   return v;
 }
 
@@ -368,7 +386,7 @@ void load_tune_cache(ftdx_handle h) {
     if (!(is >> magic >> ver >> dev >> k.n >> k.kp >> k.batch >> k.input >> k.output >>
           e.st.store_mode >> e.st.grid >> e.ms) ||
         magic != "ftdx-tune" || ver != 1 || (k.n < 1 && k.n != -1) || k.kp < 1 || k.batch < 1 ||
-        e.st.store_mode < 0 || e.st.store_mode > 1 || e.st.grid < 0 || !(e.ms >= 0.f)) {
+        e.st.store_mode < 0 || e.st.store_mode > 2 || e.st.grid < 0 || !(e.ms >= 0.f)) {
       ++h->cache_bad_lines;
       continue;
     }
@@ -554,9 +572,14 @@ ftdx_status ftdx_herk_kahan(ftdx_handle h, const void* A, void* sum, void* comp,
 
 ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid) {
   if (!h) return FTDX_ERR_INVALID_ARG;
-  if (store_mode < 0 || store_mode > 1 || grid < -1)
+  if (store_mode < 0 || store_mode > 2 || grid < -1)
     return fail(h, FTDX_ERR_INVALID_ARG, "set_strategy: store_mode %d / grid %d", store_mode,
                 grid);
+  if (store_mode == 2) {
+    cudaSetDevice(h->device);
+    if (pair_grid_limit(h) < 2)
+      return fail(h, FTDX_ERR_UNSUPPORTED, "set_strategy: no CTA pair fits on this device");
+  }
   h->default_strategy = Strategy{store_mode, grid};
   return FTDX_OK;
 }

@@ -491,6 +491,252 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   }
 }
 
+// ------------------------------------------------------------------ CTA-pair kernel
+// Same computation with one tcgen05 cta_group::2 MMA over a pair of CTAs
+// (a 2-CTA cluster on neighbouring SMs): tile = 256 column inputs j (MMA M,
+// 128 per CTA) x 128 row inputs i (MMA N, each CTA loads 64 of them).  Per
+// stage each CTA loads 48 KB instead of 64 KB for the same MMA work on its
+// SM, 25% fewer L2-to-shared bytes.  The leader CTA (rank 0) owns the full
+// barriers (the partner's loads count their bytes there) and issues the MMAs;
+// each commit is sent to the matching barrier of both CTAs; both CTAs'
+// epilogue warps release an accumulator on the leader's barrier.
+constexpr int kPairAPlane = 128 * kStageK;  // 16 KB: this CTA's 128 j rows
+constexpr int kPairBPlane = 64 * kStageK;   // 8 KB: this CTA's 64 i rows
+constexpr int kPairStageBytes = 2 * kPairAPlane + 2 * kPairBPlane;
+constexpr int kPairStages = 4;
+constexpr size_t kPairSmem = 1024 + size_t(kPairStages) * kPairStageBytes + 256;
+
+template <typename OutT>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
+    herk_fp8_pair_kernel(const __grid_constant__ CUtensorMap tmA,
+                         const __grid_constant__ CUtensorMap tmB, const HerkArgs args) {
+  extern __shared__ uint8_t smem_dyn[];
+  uint8_t* smem = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kPairStages * kPairStageBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kPairStages + 5);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const uint32_t smem0 = smem_u32(smem);
+  const uint32_t bar0 = smem_u32(bars);
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (kPairStages + s); };
+  auto tfull_bar = [&](int b) { return bar0 + 8u * (2 * kPairStages + b); };
+  auto tempty_bar = [&](int b) { return bar0 + 8u * (2 * kPairStages + 2 + b); };
+  const uint32_t done_bar = bar0 + 8u * (2 * kPairStages + 4);
+  // planes of stage s: Re_j, Im_j (128 rows each), Re_i, Im_i (64 rows each)
+  auto a_addr = [&](int s, int p) { return smem0 + uint32_t(s * kPairStageBytes + p * kPairAPlane); };
+  auto b_addr = [&](int s, int p) {
+    return smem0 + uint32_t(s * kPairStageBytes + 2 * kPairAPlane + p * kPairBPlane);
+  };
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+  const int pair = int(blockIdx.x >> 1), npairs = int(gridDim.x >> 1);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kPairStages; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(tfull_bar(b), 1);
+      mbar_init(tempty_bar(b), 2 * kEpiWarps);
+    }
+    mbar_init(done_bar, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    tma_prefetch_desc(&tmA);
+    tma_prefetch_desc(&tmB);
+  }
+  if (warp == 1) {
+    tmem_alloc_pair(smem_u32(tmem_slot), 2 * kAccCols);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // both CTAs' barriers exist before any cross-CTA signal
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------------------------ TMA producer (both CTAs)
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      for (int t = pair; t < args.num_tiles; t += npairs) {
+        const TileDesc td = args.tiles[t];
+        const ChanDesc cd = args.chans[td.ch];
+        const int32_t rowJ = int32_t(cd.row0 + int64_t(td.tj) * 256 + 128 * rank);
+        const int32_t rowI = int32_t(cd.row0 + int64_t(td.ti) * kTile + 64 * rank);
+        const int nkb = cd.kblocks * args.nseg;
+        bool ok = true;
+        for (int kb = 0; kb < nkb; ++kb) {
+          if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
+            atomicOr(args.status, kStatusTimeoutProducer);
+            ok = false;
+            break;
+          }
+          const int seg = kb / cd.kblocks;
+          const int kk = kb - seg * cd.kblocks;
+          const int sa = seg == 0 ? args.seg_a[0] : (seg == 1 ? args.seg_a[1] : args.seg_a[2]);
+          const int sb = seg == 0 ? args.seg_b[0] : (seg == 1 ? args.seg_b[1] : args.seg_b[2]);
+          const int32_t kA = (sa + kk) * kStageK, kB = (sb + kk) * kStageK;
+          if (leader) mbar_arrive_expect_tx(full_bar(stage), 2 * kPairStageBytes);
+          const uint32_t fb = map_shared(full_bar(stage), 0);
+          tma_load_3d_pair(a_addr(stage, 0), &tmA, kA, rowJ, 0, fb);
+          tma_load_3d_pair(a_addr(stage, 1), &tmA, kA, rowJ, 1, fb);
+          tma_load_3d_pair(b_addr(stage, 0), &tmB, kB, rowI, 0, fb);
+          tma_load_3d_pair(b_addr(stage, 1), &tmB, kB, rowI, 1, fb);
+          if (++stage == kPairStages) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+        if (!ok) break;
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------ MMA issuer (leader CTA)
+    if (lane == 0 && leader) {
+      constexpr uint32_t idesc = idesc_f32acc(0, 0, 256, kTile);
+      constexpr uint32_t idesc_neg = idesc_f32acc(0, 0, 256, kTile, 1);
+      int stage = 0, acc = 0;
+      uint32_t phase = 0, acc_phase = 0;
+      bool ok = true;
+      for (int t = pair; t < args.num_tiles && ok; t += npairs) {
+        const ChanDesc cd = args.chans[args.tiles[t].ch];
+        if (!mbar_wait(tempty_bar(acc), acc_phase ^ 1u, abort_flag)) {
+          atomicOr(args.status, kStatusTimeoutMma);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d_re = tmem_base + uint32_t(acc * kAccCols);
+        const uint32_t d_im = d_re + uint32_t(kTile);
+        const int nkb = cd.kblocks * args.nseg;
+        for (int kb = 0; kb < nkb; ++kb) {
+          if (!mbar_wait(full_bar(stage), phase, abort_flag)) {
+            atomicOr(args.status, kStatusTimeoutMma);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll
+          for (int s = 0; s < kStageK / 32; ++s) {
+            const uint64_t dare = sdesc_sw128_kmajor(a_addr(stage, 0) + 32 * s);
+            const uint64_t daim = sdesc_sw128_kmajor(a_addr(stage, 1) + 32 * s);
+            const uint64_t dbre = sdesc_sw128_kmajor(b_addr(stage, 0) + 32 * s);
+            const uint64_t dbim = sdesc_sw128_kmajor(b_addr(stage, 1) + 32 * s);
+            const uint32_t first = (kb | s) != 0;
+            mma_f8f6f4_pair(d_re, dare, dbre, idesc, first);
+            mma_f8f6f4_pair(d_im, dare, dbim, idesc, first);
+            mma_f8f6f4_pair(d_re, daim, dbim, idesc, 1);
+            mma_f8f6f4_pair(d_im, daim, dbre, idesc_neg, 1);
+          }
+          mma_commit_pair(empty_bar(stage));
+          mma_commit_pair(map_shared(empty_bar(stage), 1));
+          if (++stage == kPairStages) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+        if (!ok) break;
+        mma_commit_pair(tfull_bar(acc));
+        mma_commit_pair(map_shared(tfull_bar(acc), 1));
+        if (++acc == 2) {
+          acc = 0;
+          acc_phase ^= 1u;
+        }
+      }
+      mma_commit_pair(done_bar);
+      volatile int never = 0;
+      if (!mbar_wait(done_bar, 0, &never)) atomicOr(args.status, kStatusTimeoutOther);
+    }
+  } else {
+    // ------------------------------------------------ epilogue (both CTAs)
+    using Out2 = typename Complex2<OutT>::type;
+    constexpr int kChunks = kTile / 32 / (kEpiWarps / 4);
+    const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    Out2* out = static_cast<Out2*>(args.out);
+    for (int t = pair; t < args.num_tiles; t += npairs) {
+      const TileDesc td = args.tiles[t];
+      const ChanDesc cd = args.chans[td.ch];
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(tfull_bar(acc), acc_phase, abort_flag));
+      if (!ok) {
+        if (lane == 0) atomicOr(args.status, kStatusTimeoutEpilogue);
+        break;
+      }
+      tc_fence_after();
+      const int n = cd.n;
+      const int jw = int(td.tj) * 256 + 128 * int(rank) + q * 32;
+      const int j = jw + lane;
+      const int ib = int(td.ti) * kTile;
+      Out2* outc = cd.out_ptr ? reinterpret_cast<Out2*>(cd.out_ptr) : out + cd.out0;
+      const uint32_t tb = tmem_base + (uint32_t(q * 32) << 16) + uint32_t(acc * kAccCols);
+      const float sc = args.alpha * (args.chan_scale ? args.chan_scale[td.ch] : 1.f);
+#pragma unroll 1
+      for (int cc = 0; cc < kChunks; ++cc) {
+        const int c = half * kChunks + cc;
+        const int i0 = ib + 32 * c;
+        if (i0 + 31 < jw || i0 >= n) continue;  // warp-uniform: nothing to store
+        uint32_t re[32], im[32];
+        __syncwarp();
+        tmem_ld_32x32b_x32(tb + 32u * c, re);
+        tmem_ld_32x32b_x32(tb + uint32_t(kTile) + 32u * c, im);
+        tmem_wait_ld();
+        Out2* p = outc + int64_t(i0) * (i0 + 1) / 2 + j;
+        float2* pc = args.kahan ? static_cast<float2*>(args.out2) + cd.out0 +
+                                      int64_t(i0) * (i0 + 1) / 2 + j
+                                : nullptr;
+#pragma unroll
+        for (int m = 0; m < 32; ++m) {
+          const int i = i0 + m;
+          if (i < n && j <= i) {
+            float vr = __uint_as_float(re[m]) * sc;
+            float vi = (i == j) ? 0.f : __uint_as_float(im[m]) * sc;
+            if (args.kahan) {
+              const float2 sum = get(p), cmp = *pc;
+              const float yr = __fsub_rn(vr, cmp.x), yi = __fsub_rn(vi, cmp.y);
+              const float tr = __fadd_rn(sum.x, yr), ti = __fadd_rn(sum.y, yi);
+              *pc = make_float2(__fsub_rn(__fsub_rn(tr, sum.x), yr),
+                                __fsub_rn(__fsub_rn(ti, sum.y), yi));
+              vr = tr;
+              vi = ti;
+            } else if (args.beta != 0.f) {
+              const float2 o = get(p);
+              vr += args.beta * o.x;
+              vi += args.beta * o.y;
+            }
+            put(p, vr, vi);
+          }
+          p += i + 1;
+          if (args.kahan) pc += i + 1;
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(map_shared(tempty_bar(acc), 0));
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1u;
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // neither CTA leaves while the other may still signal it
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc_pair(tmem_base, 2 * kAccCols);
+  }
+}
+
 // ------------------------------------------------------------------ launchers
 static int rows_per_block(int chunks) {
   int r = 8192 / (chunks > 0 ? chunks : 1);
@@ -535,6 +781,47 @@ static cudaError_t launch_herk_t(const CUtensorMap& tmZ, const HerkArgs& a, int 
   }
   herk_fp8_tc_kernel<OutT><<<grid, kHerkThreads, kHerkSmem, s>>>(tmZ, a);
   return cudaGetLastError();
+}
+
+template <typename OutT>
+static cudaError_t pair_attributes() {
+  static bool done = false;
+  if (done) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(herk_fp8_pair_kernel<OutT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPairSmem));
+  if (e == cudaSuccess) done = true;
+  return e;
+}
+
+template <typename OutT>
+static cudaError_t launch_pair_t(const CUtensorMap& tmA, const CUtensorMap& tmB, const HerkArgs& a,
+                                 int grid, cudaStream_t s) {
+  cudaError_t e = pair_attributes<OutT>();
+  if (e != cudaSuccess) return e;
+  herk_fp8_pair_kernel<OutT><<<grid, kHerkThreads, kPairSmem, s>>>(tmA, tmB, a);
+  return cudaGetLastError();
+}
+
+cudaError_t herk_fp8_pair_max_clusters(int sm_count, int* clusters) {
+  cudaError_t e = pair_attributes<float>();
+  if (e == cudaSuccess) e = pair_attributes<__half>();
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(sm_count & ~1), 1, 1);
+  cfg.blockDim = dim3(kHerkThreads, 1, 1);
+  cfg.dynamicSmemBytes = kPairSmem;
+  int nf = 0, nh = 0;
+  e = cudaOccupancyMaxActiveClusters(&nf, herk_fp8_pair_kernel<float>, &cfg);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&nh, herk_fp8_pair_kernel<__half>, &cfg);
+  *clusters = nf < nh ? nf : nh;
+  return e;
+}
+
+cudaError_t launch_herk_fp8_pair(const CUtensorMap& tmA, const CUtensorMap& tmB,
+                                 const HerkArgs& a, int grid, cudaStream_t s) {
+  if (grid < 2 || (grid & 1)) return cudaErrorInvalidConfiguration;
+  return a.out_fp16 ? launch_pair_t<__half>(tmA, tmB, a, grid, s)
+                    : launch_pair_t<float>(tmA, tmB, a, grid, s);
 }
 
 cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s) {

@@ -108,6 +108,12 @@ cudaError_t launch_fp16_to_planes(const void* a16, uint8_t* z, int64_t rows, int
 cudaError_t launch_gather_qc_to_planes(const GatherDesc* g, int nch, int max_n, uint8_t* z,
                                        int64_t total_rows, int Kp, cudaStream_t s);
 cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s);
+// CTA-pair variant: tiles of 256 column x 128 row inputs (TileDesc::tj counts
+// 256-input blocks); tmA boxes 128 rows, tmB boxes 64 rows; grid even.
+cudaError_t launch_herk_fp8_pair(const CUtensorMap& tmA, const CUtensorMap& tmB,
+                                 const HerkArgs& a, int grid, cudaStream_t s);
+// Number of 2-CTA clusters of the pair kernel that fit on the device at once.
+cudaError_t herk_fp8_pair_max_clusters(int sm_count, int* clusters);
 // Gain-calibration loss and gradient over packed triangles (gain_grad.cu).
 cudaError_t launch_gain_grad(const float2* robs, const float2* rmod, const float* w,
                              const float2* g, int n, int nchan, double* grad, double* loss,

@@ -181,9 +181,13 @@ FTDX_API ftdx_status ftdx_set_graph_mode(ftdx_handle h, int enable);
 FTDX_API int ftdx_graph_count(ftdx_handle h);
 
 /* Strategy for calls that are not tuned (tune = 0, or no cache entry):
- * store_mode 0 = direct stores, 1 = shared-memory staging + bulk copies;
- * grid > 0 = that many persistent CTAs (capped at one per SM), 0 = one per
- * SM, -1 = one CTA per tile (a plain, non-persistent launch). */
+ * store_mode 0 = direct stores, 1 = shared-memory staging + bulk copies,
+ * 2 = CTA-pair kernel (one tcgen05 cta_group::2 MMA over two SMs per
+ * 256 x 128 tile; uniform ftdx_herk calls only, others use 0);
+ * grid > 0 = that many persistent CTAs (capped at one per SM; even and capped
+ * at the co-resident pairs for store_mode 2), 0 = one per SM, -1 = one CTA
+ * (pair) per tile (a plain, non-persistent launch).  The tuner also times
+ * store_mode 2 for uniform calls. */
 FTDX_API ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid);
 
 /* ---- correlation without any allocation -----------------------------------
