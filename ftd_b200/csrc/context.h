@@ -122,7 +122,7 @@ ftdx_status ensure_aux(ftdx_handle h, size_t bytes, cudaStream_t s);
 ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
                      const Plan** out, bool pair = false);
 ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t Kp,
-                              CUtensorMap* tm, int box_rows = kTile);
+                              CUtensorMap* tm, int box_rows = kTile, int nplanes = 2);
 // Even number of CTAs of the pair kernel that can be resident at once.
 int pair_grid_limit(ftdx_handle h);
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }

@@ -161,18 +161,19 @@ int pair_grid_limit(ftdx_handle h) {
       clusters = 0;
     }
     h->pair_grid = 2 * std::min(clusters, h->sm_count / 2);
+    if (h->verbosity > 0) fprintf(stderr, "ftdx: %d co-resident CTA pairs\n", h->pair_grid / 2);
   }
   return h->pair_grid;
 }
 
-// Tensor map over the operand planes Z[2][rows][Kp] (bytes): box of
+// Tensor map over the operand planes Z[nplanes][rows][Kp] (bytes): box of
 // 128 samples x box_rows rows x 1 plane, 128-byte swizzle.
 ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t Kp,
-                              CUtensorMap* tm, int box_rows) {
+                              CUtensorMap* tm, int box_rows, int nplanes) {
   auto enc = get_encode_fn();
   if (!enc) return fail(h, FTDX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
   const cuuint32_t estr[3] = {1, 1, 1};
-  const cuuint64_t dims[3] = {cuuint64_t(Kp), cuuint64_t(rows), 2};
+  const cuuint64_t dims[3] = {cuuint64_t(Kp), cuuint64_t(rows), cuuint64_t(nplanes)};
   const cuuint64_t strides[2] = {cuuint64_t(Kp), cuuint64_t(rows * Kp)};
   const cuuint32_t box[3] = {cuuint32_t(kStageK), cuuint32_t(box_rows), 1};
   CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, z, dims, strides, box, estr,

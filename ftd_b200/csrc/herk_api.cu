@@ -134,7 +134,8 @@ ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan
   const int64_t Kp = round_up(c.K, kStageK);
   const int64_t zpitch = is_split(c) ? 2 * Kp : Kp;
   const int64_t rows = int64_t(c.N) * c.batch;
-  ftdx_status st = ensure_workspace(h, size_t(2 * rows * zpitch), s);
+  // the pair kernel reads a third plane, -Re
+  ftdx_status st = ensure_workspace(h, size_t((pair ? 3 : 2) * rows * zpitch), s);
   if (st != FTDX_OK) return st;
   if (c.input == FTDX_IN_FP32) {
     st = ensure_aux(h, size_t(12) * size_t(c.batch) + 256, s);
@@ -159,18 +160,21 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   cudaError_t e;
   {
     ScopedTimer tm(h, s, 1);
-    if (c.input == FTDX_IN_INT4)
-      e = launch_qc_to_planes(static_cast<const uint8_t*>(c.A), h->z, rows, c.K, int(Kp), s);
-    else if (c.input == FTDX_IN_FP16)
-      e = launch_fp16_to_planes(c.A, h->z, rows, c.K, int(Kp), s);
-    else
-      e = launch_float_to_planes(c.A, h->z, rows, c.K, int(Kp), int(zpitch), c.N, c.batch,
-                                 is_split(c) ? 1 : 0, qscale, out_scale, amax, h->sm_count, s);
+    if (c.input == FTDX_IN_INT4) {
+      e = launch_qc_to_planes(static_cast<const uint8_t*>(c.A), h->z, rows, c.K, int(Kp), s,
+                              pair);
+    } else {
+      if (c.input == FTDX_IN_FP16)
+        e = launch_fp16_to_planes(c.A, h->z, rows, c.K, int(Kp), s);
+      else
+        e = launch_float_to_planes(c.A, h->z, rows, c.K, int(Kp), int(zpitch), c.N, c.batch,
+                                   is_split(c) ? 1 : 0, qscale, out_scale, amax, h->sm_count, s);
+      if (e == cudaSuccess && pair) e = launch_negate_plane(h->z, rows * zpitch, h->sm_count, s);
+    }
   }
   if (e != cudaSuccess) return cuda_fail(h, e, "operand promotion launch");
-  CUtensorMap tmZ, tmB;
-  st = encode_planes_map(h, h->z, rows, zpitch, &tmZ);
-  if (st == FTDX_OK && pair) st = encode_planes_map(h, h->z, rows, zpitch, &tmB, kTile / 2);
+  CUtensorMap tmZ;
+  st = encode_planes_map(h, h->z, rows, zpitch, &tmZ, kTile, pair ? 3 : 2);
   if (st != FTDX_OK) return st;
   HerkArgs args = herk_args_default();
   args.tiles = plan->d_tiles;
@@ -201,7 +205,7 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
     if (strat.grid < 0) grid = 2 * plan->num_tiles;
     grid = std::min(grid, 2 * plan->num_tiles) & ~1;
     ScopedTimer tm(h, s, 0);
-    e = launch_herk_fp8_pair(tmZ, tmB, args, grid, s);
+    e = launch_herk_fp8_pair(tmZ, args, grid, s);
   } else {
     int grid = strat.grid > 0 ? strat.grid : h->sm_count;
     if (grid > h->sm_count) grid = h->sm_count;  // persistent: at most one CTA per SM
@@ -436,7 +440,7 @@ ftdx_status ftdx_init_herk(ftdx_handle h, int N, int K, int batch, void* stream)
   const HerkCall c{reinterpret_cast<const void*>(16), reinterpret_cast<void*>(16), N, K, batch,
                    FTDX_IN_INT4, FTDX_OUT_FP32, 1.f, 0.f};
   const Plan* p = nullptr;
-  return prepare(h, c, static_cast<cudaStream_t>(stream), &p);
+  return prepare(h, c, static_cast<cudaStream_t>(stream), &p, use_pair(h, h->default_strategy));
 }
 
 ftdx_status ftdx_end_herk(ftdx_handle h) {

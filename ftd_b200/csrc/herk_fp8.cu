@@ -43,9 +43,12 @@ __device__ __forceinline__ void qc4_to_e4m3(uint32_t w, uint32_t& re, uint32_t& 
 
 // One thread converts 16 samples of one antenna row.  Each block owns
 // `rows_per_block` consecutive rows so that all index math is 32-bit.
+// With neg_plane set a third plane receives -Re (sign bit flipped), the B
+// operand of the CTA-pair kernel's partner CTA.
 __global__ void __launch_bounds__(256) qc_to_planes_kernel(const uint8_t* __restrict__ qc,
                                                            uint8_t* __restrict__ z, int64_t rows,
-                                                           int K, int Kp, int rows_per_block) {
+                                                           int K, int Kp, int rows_per_block,
+                                                           int neg_plane) {
   const int chunks = Kp >> 4;
   const int64_t r0 = int64_t(blockIdx.x) * rows_per_block;
   const int64_t nrows64 = rows - r0 < rows_per_block ? rows - r0 : rows_per_block;
@@ -80,6 +83,22 @@ __global__ void __launch_bounds__(256) qc_to_planes_kernel(const uint8_t* __rest
     uint8_t* dst = z + r * Kp + t0;
     *reinterpret_cast<uint4*>(dst) = make_uint4(re[0], re[1], re[2], re[3]);
     *reinterpret_cast<uint4*>(dst + plane) = make_uint4(im[0], im[1], im[2], im[3]);
+    if (neg_plane) {
+      constexpr uint32_t kS = 0x80808080u;
+      *reinterpret_cast<uint4*>(dst + 2 * plane) =
+          make_uint4(re[0] ^ kS, re[1] ^ kS, re[2] ^ kS, re[3] ^ kS);
+    }
+  }
+}
+
+// Plane 2 = plane 0 with every E4M3 sign flipped (-Re), for inputs whose
+// promotion kernel writes two planes.  n16 = plane bytes / 16.
+__global__ void __launch_bounds__(256) negate_plane_kernel(uint4* __restrict__ z, int64_t n16) {
+  constexpr uint32_t kS = 0x80808080u;
+  for (int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < n16;
+       x += int64_t(gridDim.x) * blockDim.x) {
+    const uint4 v = z[x];
+    z[x + 2 * n16] = make_uint4(v.x ^ kS, v.y ^ kS, v.z ^ kS, v.w ^ kS);
   }
 }
 
@@ -492,24 +511,28 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
 }
 
 // ------------------------------------------------------------------ CTA-pair kernel
-// Same computation with one tcgen05 cta_group::2 MMA over a pair of CTAs
-// (a 2-CTA cluster on neighbouring SMs): tile = 256 column inputs j (MMA M,
-// 128 per CTA) x 128 row inputs i (MMA N, each CTA loads 64 of them).  Per
-// stage each CTA loads 48 KB instead of 64 KB for the same MMA work on its
-// SM, 25% fewer L2-to-shared bytes.  The leader CTA (rank 0) owns the full
-// barriers (the partner's loads count their bytes there) and issues the MMAs;
-// each commit is sent to the matching barrier of both CTAs; both CTAs'
-// epilogue warps release an accumulator on the leader's barrier.
-constexpr int kPairAPlane = 128 * kStageK;  // 16 KB: this CTA's 128 j rows
-constexpr int kPairBPlane = 64 * kStageK;   // 8 KB: this CTA's 64 i rows
-constexpr int kPairStageBytes = 2 * kPairAPlane + 2 * kPairBPlane;
-constexpr int kPairStages = 4;
+// Same computation with tcgen05 cta_group::2 MMAs of M = 256, N = 256 over a
+// pair of CTAs (a 2-CTA cluster): tile = 256 column inputs j (128 per CTA,
+// TMEM lane = j) x 128 row inputs i.  The N = 256 columns of one MMA are the
+// Re and Im halves of the accumulator; the B operand's first 128 rows come
+// from the leader CTA's shared memory and the last 128 from the partner's:
+//   MMA 1: A = Re_j, B = [Re_i | Im_i]   -> Re += Re_j Re_i, Im += Re_j Im_i
+//   MMA 2: A = Im_j, B = [Im_i | -Re_i]  -> Re += Im_j Im_i, Im -= Im_j Re_i
+// so the leader loads (Re_i, Im_i) and the partner (Im_i, -Re_i), the third
+// operand plane holding -Re.  Two MMAs per 32 samples instead of four of
+// N = 128: each MMA reads half as many operand bytes per multiply-add from
+// shared memory, which bounds the single-CTA kernel.  The leader CTA (rank 0)
+// owns the full barriers (the partner's loads count their bytes there) and
+// issues the MMAs; each commit is sent to the matching barrier of both CTAs;
+// both CTAs' epilogue warps release an accumulator on the leader's barrier.
+constexpr int kPairPlane = 128 * kStageK;  // 16 KB: 128 rows of 128 samples
+constexpr int kPairStageBytes = 4 * kPairPlane;
+constexpr int kPairStages = 3;
 constexpr size_t kPairSmem = 1024 + size_t(kPairStages) * kPairStageBytes + 256;
 
 template <typename OutT>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
-    herk_fp8_pair_kernel(const __grid_constant__ CUtensorMap tmA,
-                         const __grid_constant__ CUtensorMap tmB, const HerkArgs args) {
+    herk_fp8_pair_kernel(const __grid_constant__ CUtensorMap tmZ, const HerkArgs args) {
   extern __shared__ uint8_t smem_dyn[];
   uint8_t* smem = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kPairStages * kPairStageBytes);
@@ -522,11 +545,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
   auto tfull_bar = [&](int b) { return bar0 + 8u * (2 * kPairStages + b); };
   auto tempty_bar = [&](int b) { return bar0 + 8u * (2 * kPairStages + 2 + b); };
   const uint32_t done_bar = bar0 + 8u * (2 * kPairStages + 4);
-  // planes of stage s: Re_j, Im_j (128 rows each), Re_i, Im_i (64 rows each)
-  auto a_addr = [&](int s, int p) { return smem0 + uint32_t(s * kPairStageBytes + p * kPairAPlane); };
-  auto b_addr = [&](int s, int p) {
-    return smem0 + uint32_t(s * kPairStageBytes + 2 * kPairAPlane + p * kPairBPlane);
-  };
+  // planes of stage s: Re_j, Im_j, then the B halves X (MMA 1) and Y (MMA 2)
+  auto plane = [&](int s, int p) { return smem0 + uint32_t(s * kPairStageBytes + p * kPairPlane); };
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t rank = cluster_rank();
@@ -547,8 +567,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
     fence_mbar_init();
   }
   if (warp == 0 && lane == 0) {
-    tma_prefetch_desc(&tmA);
-    tma_prefetch_desc(&tmB);
+    tma_prefetch_desc(&tmZ);
   }
   if (warp == 1) {
     tmem_alloc_pair(smem_u32(tmem_slot), 2 * kAccCols);
@@ -569,7 +588,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
         const TileDesc td = args.tiles[t];
         const ChanDesc cd = args.chans[td.ch];
         const int32_t rowJ = int32_t(cd.row0 + int64_t(td.tj) * 256 + 128 * rank);
-        const int32_t rowI = int32_t(cd.row0 + int64_t(td.ti) * kTile + 64 * rank);
+        const int32_t rowI = int32_t(cd.row0 + int64_t(td.ti) * kTile);
+        const int32_t pX = int32_t(rank), pY = int32_t(rank) + 1;  // leader: Re, Im; partner: Im, -Re
         const int nkb = cd.kblocks * args.nseg;
         bool ok = true;
         for (int kb = 0; kb < nkb; ++kb) {
@@ -585,10 +605,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
           const int32_t kA = (sa + kk) * kStageK, kB = (sb + kk) * kStageK;
           if (leader) mbar_arrive_expect_tx(full_bar(stage), 2 * kPairStageBytes);
           const uint32_t fb = map_shared(full_bar(stage), 0);
-          tma_load_3d_pair(a_addr(stage, 0), &tmA, kA, rowJ, 0, fb);
-          tma_load_3d_pair(a_addr(stage, 1), &tmA, kA, rowJ, 1, fb);
-          tma_load_3d_pair(b_addr(stage, 0), &tmB, kB, rowI, 0, fb);
-          tma_load_3d_pair(b_addr(stage, 1), &tmB, kB, rowI, 1, fb);
+          tma_load_3d_pair(plane(stage, 0), &tmZ, kA, rowJ, 0, fb);
+          tma_load_3d_pair(plane(stage, 1), &tmZ, kA, rowJ, 1, fb);
+          tma_load_3d_pair(plane(stage, 2), &tmZ, kB, rowI, pX, fb);
+          tma_load_3d_pair(plane(stage, 3), &tmZ, kB, rowI, pY, fb);
           if (++stage == kPairStages) {
             stage = 0;
             phase ^= 1u;
@@ -600,8 +620,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
   } else if (warp == 1) {
     // ------------------------------------------------ MMA issuer (leader CTA)
     if (lane == 0 && leader) {
-      constexpr uint32_t idesc = idesc_f32acc(0, 0, 256, kTile);
-      constexpr uint32_t idesc_neg = idesc_f32acc(0, 0, 256, kTile, 1);
+      constexpr uint32_t idesc = idesc_f32acc(0, 0, 256, 2 * kTile);
       int stage = 0, acc = 0;
       uint32_t phase = 0, acc_phase = 0;
       bool ok = true;
@@ -612,8 +631,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
           break;
         }
         tc_fence_after();
-        const uint32_t d_re = tmem_base + uint32_t(acc * kAccCols);
-        const uint32_t d_im = d_re + uint32_t(kTile);
+        const uint32_t d = tmem_base + uint32_t(acc * kAccCols);  // Re | Im columns
         const int nkb = cd.kblocks * args.nseg;
         for (int kb = 0; kb < nkb; ++kb) {
           if (!mbar_wait(full_bar(stage), phase, abort_flag)) {
@@ -624,15 +642,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
           tc_fence_after();
 #pragma unroll
           for (int s = 0; s < kStageK / 32; ++s) {
-            const uint64_t dare = sdesc_sw128_kmajor(a_addr(stage, 0) + 32 * s);
-            const uint64_t daim = sdesc_sw128_kmajor(a_addr(stage, 1) + 32 * s);
-            const uint64_t dbre = sdesc_sw128_kmajor(b_addr(stage, 0) + 32 * s);
-            const uint64_t dbim = sdesc_sw128_kmajor(b_addr(stage, 1) + 32 * s);
-            const uint32_t first = (kb | s) != 0;
-            mma_f8f6f4_pair(d_re, dare, dbre, idesc, first);
-            mma_f8f6f4_pair(d_im, dare, dbim, idesc, first);
-            mma_f8f6f4_pair(d_re, daim, dbim, idesc, 1);
-            mma_f8f6f4_pair(d_im, daim, dbre, idesc_neg, 1);
+            const uint64_t dare = sdesc_sw128_kmajor(plane(stage, 0) + 32 * s);
+            const uint64_t daim = sdesc_sw128_kmajor(plane(stage, 1) + 32 * s);
+            const uint64_t dbx = sdesc_sw128_kmajor(plane(stage, 2) + 32 * s);
+            const uint64_t dby = sdesc_sw128_kmajor(plane(stage, 3) + 32 * s);
+            mma_f8f6f4_pair(d, dare, dbx, idesc, (kb | s) != 0);
+            mma_f8f6f4_pair(d, daim, dby, idesc, 1);
           }
           mma_commit_pair(empty_bar(stage));
           mma_commit_pair(map_shared(empty_bar(stage), 1));
@@ -744,10 +759,19 @@ static int rows_per_block(int chunks) {
 }
 
 cudaError_t launch_qc_to_planes(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
-                                cudaStream_t s) {
+                                cudaStream_t s, bool neg_plane) {
   const int rpb = rows_per_block(Kp >> 4);
   const int64_t blocks = (rows + rpb - 1) / rpb;
-  qc_to_planes_kernel<<<unsigned(blocks), 256, 0, s>>>(qc, z, rows, K, Kp, rpb);
+  qc_to_planes_kernel<<<unsigned(blocks), 256, 0, s>>>(qc, z, rows, K, Kp, rpb, neg_plane ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_negate_plane(uint8_t* z, int64_t plane_bytes, int sm_count, cudaStream_t s) {
+  const int64_t n16 = plane_bytes / 16;
+  int64_t blocks = (n16 + 255) / 256;
+  if (blocks > int64_t(sm_count) * 8) blocks = int64_t(sm_count) * 8;
+  if (blocks < 1) blocks = 1;
+  negate_plane_kernel<<<unsigned(blocks), 256, 0, s>>>(reinterpret_cast<uint4*>(z), n16);
   return cudaGetLastError();
 }
 
@@ -794,11 +818,11 @@ static cudaError_t pair_attributes() {
 }
 
 template <typename OutT>
-static cudaError_t launch_pair_t(const CUtensorMap& tmA, const CUtensorMap& tmB, const HerkArgs& a,
-                                 int grid, cudaStream_t s) {
+static cudaError_t launch_pair_t(const CUtensorMap& tmZ, const HerkArgs& a, int grid,
+                                 cudaStream_t s) {
   cudaError_t e = pair_attributes<OutT>();
   if (e != cudaSuccess) return e;
-  herk_fp8_pair_kernel<OutT><<<grid, kHerkThreads, kPairSmem, s>>>(tmA, tmB, a);
+  herk_fp8_pair_kernel<OutT><<<grid, kHerkThreads, kPairSmem, s>>>(tmZ, a);
   return cudaGetLastError();
 }
 
@@ -817,11 +841,10 @@ cudaError_t herk_fp8_pair_max_clusters(int sm_count, int* clusters) {
   return e;
 }
 
-cudaError_t launch_herk_fp8_pair(const CUtensorMap& tmA, const CUtensorMap& tmB,
-                                 const HerkArgs& a, int grid, cudaStream_t s) {
+cudaError_t launch_herk_fp8_pair(const CUtensorMap& tmZ, const HerkArgs& a, int grid,
+                                 cudaStream_t s) {
   if (grid < 2 || (grid & 1)) return cudaErrorInvalidConfiguration;
-  return a.out_fp16 ? launch_pair_t<__half>(tmA, tmB, a, grid, s)
-                    : launch_pair_t<float>(tmA, tmB, a, grid, s);
+  return a.out_fp16 ? launch_pair_t<__half>(tmZ, a, grid, s) : launch_pair_t<float>(tmZ, a, grid, s);
 }
 
 cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s) {

@@ -98,8 +98,11 @@ inline HerkArgs herk_args_default() {
 }
 
 // Host-side launchers (herk_fp8.cu).
+// neg_plane: also write plane 2 = -Re (CTA-pair kernel operand)
 cudaError_t launch_qc_to_planes(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
-                                cudaStream_t s);
+                                cudaStream_t s, bool neg_plane = false);
+// Plane 2 = -(plane 0), planes of plane_bytes each (a multiple of 16).
+cudaError_t launch_negate_plane(uint8_t* z, int64_t plane_bytes, int sm_count, cudaStream_t s);
 cudaError_t launch_fp16_to_planes(const void* a16, uint8_t* z, int64_t rows, int K, int Kp,
                                   cudaStream_t s);
 // Gathered promotion for `nch` channels with a common plane pitch Kp
@@ -109,9 +112,10 @@ cudaError_t launch_gather_qc_to_planes(const GatherDesc* g, int nch, int max_n, 
                                        int64_t total_rows, int Kp, cudaStream_t s);
 cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s);
 // CTA-pair variant: tiles of 256 column x 128 row inputs (TileDesc::tj counts
-// 256-input blocks); tmA boxes 128 rows, tmB boxes 64 rows; grid even.
-cudaError_t launch_herk_fp8_pair(const CUtensorMap& tmA, const CUtensorMap& tmB,
-                                 const HerkArgs& a, int grid, cudaStream_t s);
+// 256-input blocks); tmZ covers three planes (Re, Im, -Re), boxes of 128
+// rows; grid even.
+cudaError_t launch_herk_fp8_pair(const CUtensorMap& tmZ, const HerkArgs& a, int grid,
+                                 cudaStream_t s);
 // Number of 2-CTA clusters of the pair kernel that fit on the device at once.
 cudaError_t herk_fp8_pair_max_clusters(int sm_count, int* clusters);
 // Gain-calibration loss and gradient over packed triangles (gain_grad.cu).
