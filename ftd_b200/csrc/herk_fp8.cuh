@@ -37,6 +37,11 @@ constexpr int kStgRows = 8;
 constexpr int kStgRowBytes = kTile * 8 + 16;
 constexpr int kStgBytes = 2 /*halves*/ * 2 /*buffers*/ * kStgRows * kStgRowBytes;
 constexpr size_t kHerkSmem = 1024 + size_t(kStages) * kStageBytes + kStgBytes + 256;
+// Shared sectors of the sector-aligned epilogue: per half, two buffers of
+// 32 rows x 3 warp boundaries x 4 complex64 elements (reuses the staging area).
+constexpr int kSecBufBytes = 32 * 3 * 4 * 8;
+constexpr int kSecBytes = 2 /*halves*/ * 2 /*buffers*/ * kSecBufBytes;
+static_assert(kSecBytes <= kStgBytes, "sector buffers live in the staging area");
 
 // One lower-triangle tile: channel, row block ti (i), column block tj (j), tj <= ti.
 struct TileDesc {

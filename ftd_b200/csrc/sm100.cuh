@@ -147,6 +147,13 @@ __device__ __forceinline__ void st_shared_v2(uint32_t addr, uint32_t a, uint32_t
   asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(addr), "r"(a), "r"(b) : "memory");
 }
 
+// 32-byte streaming store (one whole L2 sector) from one thread.
+__device__ __forceinline__ void st_global_cs_v8(void* p, float4 a, float4 b) {
+  asm volatile("st.global.cs.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(a.x),
+               "f"(a.y), "f"(a.z), "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w)
+               : "memory");
+}
+
 // ---------------------------------------------------------------- CTA pairs
 // (a cluster of two CTAs running one tcgen05 cta_group::2 MMA together)
 __device__ __forceinline__ uint32_t cluster_rank() {
@@ -160,10 +167,19 @@ __device__ __forceinline__ uint32_t map_shared(uint32_t addr, uint32_t rank) {
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
   return r;
 }
-// Arrive on an mbarrier given by its shared::cluster address (any CTA of the pair).
-__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
-  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
+// Relaxed arrive (no memory ordering, synchronisation only) on an mbarrier
+// given by its shared::cluster address (any CTA of the pair).  For handing
+// TMEM back to the MMA issuer: the tcgen05.ld reads are complete
+// (tcgen05.wait::ld) and ordered by tcgen05.fence::before_thread_sync, and
+// the issuer reads no memory the arriving threads wrote, so a release (which
+// would wait for their global stores) is not needed.
+__device__ __forceinline__ void mbar_arrive_cluster_relaxed(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.relaxed.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
                : "memory");
+}
+// Same for an mbarrier of this CTA.
+__device__ __forceinline__ void mbar_arrive_relaxed(uint32_t bar) {
+  asm volatile("mbarrier.arrive.relaxed.cta.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ void cluster_sync_all() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" :::
