@@ -23,6 +23,7 @@ IN_FP16, IN_INT4, IN_FP32 = 0, 1, 2
 COMPUTE_FP8, COMPUTE_FP6, COMPUTE_FP4, COMPUTE_FP8_SPLIT = 0, 1, 2, 3
 OUT_FP16, OUT_FP32 = 0, 1
 FORMAT_PACKED_TRIANGLE = 0
+LAYOUT_TIME_ANT_CHAN_POL, LAYOUT_CHAN_POL_ANT_TIME = 0, 1
 
 
 class FtdxError(RuntimeError):
@@ -39,6 +40,12 @@ class ChannelDesc(ctypes.Structure):
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("verbosity", ctypes.c_int),
                 ("tune_cache", ctypes.c_char_p), ("reserved", ctypes.c_int * 8)]
+
+
+class FtdDesc(ctypes.Structure):
+    _fields_ = [("n_ant", ctypes.c_int), ("n_chan", ctypes.c_int), ("n_pol", ctypes.c_int),
+                ("n_time", ctypes.c_int), ("n_time_inner", ctypes.c_int), ("layout", ctypes.c_int),
+                ("pol_sum", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
 
 
 _vp = ctypes.c_void_p
@@ -58,6 +65,7 @@ PROTOTYPES = {
     "ftdx_gain_gradient": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp]),
     "ftdx_herk_kahan": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
     "ftdx_herk_batched_v": (_i, [_vp, ctypes.c_void_p, _i, _i, _f, _f, _vp, _i]),
+    "ftdx_herk_ftd": (_i, [_vp, _vp, _vp, ctypes.POINTER(FtdDesc), _i, _f, _f, _vp]),
     "ftdx_end_herk": (_i, [_vp]),
     "ftdx_device_status": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32)]),
     "ftdx_set_profiling": (_i, [_vp, _i]),

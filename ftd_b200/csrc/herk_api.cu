@@ -26,6 +26,7 @@ struct HerkCall {
   float alpha, beta;
   ftdx_compute compute = FTDX_COMPUTE_FP8;
   void* comp = nullptr;  // Kahan compensation buffer (ftdx_herk_kahan)
+  const ftdx_ftd_desc* ftd = nullptr;  // raw packet-ordered input (ftdx_herk_ftd)
 };
 
 bool is_split(const HerkCall& c) { return c.compute == FTDX_COMPUTE_FP8_SPLIT; }
@@ -160,7 +161,19 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   cudaError_t e;
   {
     ScopedTimer tm(h, s, 1);
-    if (c.input == FTDX_IN_INT4) {
+    if (c.ftd) {
+      const ftdx_ftd_desc& d = *c.ftd;
+      FtdGeom g;
+      g.n_ant = d.n_ant, g.n_chan = d.n_chan, g.n_pol = d.n_pol, g.n_ti = d.n_time_inner;
+      g.K = d.n_time / d.n_time_inner;
+      g.n_time = d.n_time;
+      g.pol_sum = d.pol_sum;
+      g.Kp = int(Kp);
+      g.rows = rows;
+      g.neg_plane = pair ? 1 : 0;
+      e = launch_ftd_to_planes(static_cast<const uint8_t*>(c.A), h->z, g, int(d.layout),
+                               h->sm_count, s);
+    } else if (c.input == FTDX_IN_INT4) {
       e = launch_qc_to_planes(static_cast<const uint8_t*>(c.A), h->z, rows, c.K, int(Kp), s,
                               pair);
     } else {
@@ -551,6 +564,43 @@ ftdx_status ftdx_gain_gradient(ftdx_handle h, const void* R_obs, const void* R_m
                          static_cast<const float2*>(g), N, n_chans, grad, loss,
                          static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "gain gradient launch");
+}
+
+ftdx_status ftdx_herk_ftd(ftdx_handle h, const void* raw, void* C, const ftdx_ftd_desc* d,
+                          ftdx_output output, float alpha, float beta, void* stream) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  if (!d) return fail(h, FTDX_ERR_INVALID_ARG, "herk_ftd: null descriptor");
+  if (d->n_ant < 1 || d->n_chan < 1 || d->n_pol < 1 || d->n_time_inner < 1 || d->n_time < 1 ||
+      d->n_time % d->n_time_inner != 0)
+    return fail(h, FTDX_ERR_INVALID_ARG,
+                "herk_ftd: bad geometry (n_ant %d, n_chan %d, n_pol %d, n_time %d, n_time_inner %d)",
+                d->n_ant, d->n_chan, d->n_pol, d->n_time, d->n_time_inner);
+  if (d->layout != FTDX_LAYOUT_TIME_ANT_CHAN_POL && d->layout != FTDX_LAYOUT_CHAN_POL_ANT_TIME)
+    return fail(h, FTDX_ERR_INVALID_ARG, "herk_ftd: bad layout %d", int(d->layout));
+  if (d->pol_sum != 0 && d->pol_sum != 1)
+    return fail(h, FTDX_ERR_INVALID_ARG, "herk_ftd: pol_sum must be 0 or 1");
+  const int K = d->n_time / d->n_time_inner;
+  const int64_t keff = d->pol_sum ? int64_t(d->n_pol) * K : int64_t(K);
+  const int64_t batch = int64_t(d->n_chan) * d->n_time_inner * (d->pol_sum ? 1 : d->n_pol);
+  if (keff > (int64_t(1) << 30) || batch > (int64_t(1) << 30) ||
+      int64_t(d->n_time) * d->n_ant * d->n_chan * d->n_pol > (int64_t(1) << 40))
+    return fail(h, FTDX_ERR_INVALID_ARG, "herk_ftd: problem too large");
+  HerkCall c{raw, C, d->n_ant, int(keff), int(batch), FTDX_IN_INT4, output, alpha, beta};
+  c.ftd = d;
+  ftdx_status st = validate(h, c, FTDX_COMPUTE_FP8, FTDX_FORMAT_PACKED_TRIANGLE);
+  if (st != FTDX_OK) return st;
+  if (d->layout == FTDX_LAYOUT_TIME_ANT_CHAN_POL &&
+      (round_up(keff, kStageK) > 64 * 65535 || d->n_time_inner > 65535))
+    return fail(h, FTDX_ERR_INVALID_ARG, "herk_ftd: K or n_time_inner too large for this layout");
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+  // strategy of the equivalent batch-first call (tuned entry if one exists)
+  Strategy strat = h->default_strategy;
+  HerkCall plain = c;
+  plain.ftd = nullptr;
+  auto it = h->tuned.find(tune_key(h, plain));
+  if (it != h->tuned.end()) strat = it->second.st;
+  return launch_all(h, c, strat, static_cast<cudaStream_t>(stream));
 }
 
 ftdx_status ftdx_herk_kahan(ftdx_handle h, const void* A, void* sum, void* comp, int N, int K,

@@ -106,6 +106,19 @@ inline HerkArgs herk_args_default() {
 // neg_plane: also write plane 2 = -Re (CTA-pair kernel operand)
 cudaError_t launch_qc_to_planes(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
                                 cudaStream_t s, bool neg_plane = false);
+// Raw packet-ordered QC input (corner_turn.cu): geometry of the promotion.
+struct FtdGeom {
+  int n_ant, n_chan, n_pol, n_ti;  // antennas, channels, polarisations, time_inner
+  int K;                           // samples per (chan, pol, ti) and antenna
+  int n_time;                      // K * n_ti
+  int pol_sum;                     // rows hold all pols back to back (n_pol*K columns)
+  int Kp;                          // padded row length (multiple of kStageK)
+  int64_t rows;                    // plane rows = n_ant * batches
+  int neg_plane;                   // also write plane 2 = -Re
+};
+// layout 0: [t][ant][chan][pol], t = k*n_ti + ti; 1: [chan][pol][ant][t], t = ti*K + k.
+cudaError_t launch_ftd_to_planes(const uint8_t* raw, uint8_t* z, const FtdGeom& g, int layout,
+                                 int sm_count, cudaStream_t s);
 // Plane 2 = -(plane 0), planes of plane_bytes each (a multiple of 16).
 cudaError_t launch_negate_plane(uint8_t* z, int64_t plane_bytes, int sm_count, cudaStream_t s);
 cudaError_t launch_fp16_to_planes(const void* a16, uint8_t* z, int64_t rows, int K, int Kp,

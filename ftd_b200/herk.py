@@ -118,6 +118,18 @@ class Correlator:
                                          int(bool(tune)))
         check(self._h, st, "ftdx_herk_batched_v")
 
+    def herk_ftd(self, raw, C, n_ant: int, n_chan: int, n_pol: int, n_time: int,
+                 n_time_inner: int = 1, layout: int = _lib.LAYOUT_TIME_ANT_CHAN_POL,
+                 pol_sum: bool = False, output: int = OUT_FP32, alpha: float = 1.0,
+                 beta: float = 0.0, stream=None) -> None:
+        """Correlate raw packet-ordered QC voltages with the corner turn fused
+        into the promotion pass.  Output batch b = (chan*n_pol + pol)*n_time_inner
+        + ti (pol_sum: chan*n_time_inner + ti, pols summed); see ftdx_herk_ftd."""
+        d = _lib.FtdDesc(n_ant, n_chan, n_pol, n_time, n_time_inner, layout, int(bool(pol_sum)))
+        st = self._L.ftdx_herk_ftd(self._h, _ptr(raw), _ptr(C), ctypes.byref(d), output,
+                                   float(alpha), float(beta), _stream(stream))
+        check(self._h, st, "ftdx_herk_ftd")
+
     def herk_kahan(self, A, S, comp, N: int, K: int, batch: int, input: int = IN_INT4,
                    compute: int = COMPUTE_FP8, stream=None) -> None:
         """S += A A^H with Kahan compensation kept in `comp` (both packed complex64)."""

@@ -128,6 +128,38 @@ FTDX_API ftdx_status ftdx_herk_batched_v(ftdx_handle h, const ftdx_channel_desc*
                                          int n_chans, ftdx_output output, float alpha,
                                          float beta, void* stream, int tune);
 
+/* Correlation straight from raw packet-ordered QC voltages: the corner turn
+ * into per-(channel, pol, time_inner) antenna rows is fused into the operand
+ * promotion pass, so the raw buffer is read once and no batch-first copy is
+ * made.  Two source layouts of the reference are accepted:
+ *   FTDX_LAYOUT_TIME_ANT_CHAN_POL: byte [t][ant][chan][pol], t = k*n_time_inner
+ *     + ti (the FTD packet order of tests/visibility_pipeline_test.cpp:55-96,
+ *     cpu_herk_ftd);
+ *   FTDX_LAYOUT_CHAN_POL_ANT_TIME: byte [chan][pol][ant][t], t = ti*K + k (the
+ *     order qc_pol_gather_transpose_kernel reads, lib/bench_pipeline.cu:306-331).
+ * K = n_time / n_time_inner (n_time must be a multiple of n_time_inner).
+ * Output: one packed lower triangle (N = n_ant) per batch b = (chan*n_pol +
+ * pol)*n_time_inner + ti, the batch order of cpu_herk_ftd.  With pol_sum = 1
+ * the polarisations are summed, R = sum_pol V_pol V_pol^H, one triangle per
+ * b = chan*n_time_inner + ti (what the reference's two HERKs with beta = 1 on
+ * pol-separated buffers produce, lib/bench_pipeline.cu:1366-1378); it runs as
+ * one HERK over n_pol*K samples.  QC int4 input, FP8 compute. */
+typedef enum {
+  FTDX_LAYOUT_TIME_ANT_CHAN_POL = 0,
+  FTDX_LAYOUT_CHAN_POL_ANT_TIME = 1
+} ftdx_layout;
+
+typedef struct ftdx_ftd_desc {
+  int n_ant, n_chan, n_pol, n_time, n_time_inner;
+  ftdx_layout layout;
+  int pol_sum;
+  int reserved[4];
+} ftdx_ftd_desc;
+
+FTDX_API ftdx_status ftdx_herk_ftd(ftdx_handle h, const void* raw, void* C,
+                                   const ftdx_ftd_desc* desc, ftdx_output output, float alpha,
+                                   float beta, void* stream);
+
 /* Kahan-compensated accumulation across integration dumps (no counterpart
  * in the reference): sum += A A^H with the FP32 rounding error of every
  * addition carried in `comp` (same packed layout and size as `sum`, complex64,

@@ -29,8 +29,9 @@ extract() {  # file name
   extract "$T1" cpu_herk
   extract "$T2" decode_qc_byte
   extract "$T2" cpu_herk_batch_first
+  extract "$T2" cpu_herk_ftd
 } > "$OUT/ref_extract.inc"
-for f in encode_int4 cpu_herk decode_qc_byte cpu_herk_batch_first; do
+for f in encode_int4 cpu_herk decode_qc_byte cpu_herk_batch_first cpu_herk_ftd; do
   grep -q "$f(" "$OUT/ref_extract.inc" || { echo "build_ref: $f not found" >&2; exit 3; }
 done
 /usr/bin/g++ -O3 -fopenmp -march=x86-64-v3 -std=c++17 -fPIC -shared -I"$OUT" \

@@ -8,9 +8,13 @@ baseline; the product (``ftd_b200``) never does.
   host correlator ``cpu_herk`` (cutlass_interface/test_herk_int4.cu:51-70)
   with exact int64 accumulation for QC int4 input and FP64 for float input.
 * ``_ref/libref_herk.so`` (``build_ref.sh`` + ``ref_harness.cpp``): the
-  reference's own ``cpu_herk``, ``encode_int4``, ``decode_qc_byte`` and
-  ``cpu_herk_batch_first`` compiled from the reference tree, used to pin the
-  restatement and as the timed CPU baseline.
+  reference's own ``cpu_herk``, ``encode_int4``, ``decode_qc_byte``,
+  ``cpu_herk_batch_first`` and ``cpu_herk_ftd`` compiled from the reference
+  tree, used to pin the restatement and as the timed CPU baseline.
+* ``ftd_to_batch_first``: the corner turn of raw packet-ordered QC input
+  into per-(channel, pol, time_inner) antenna rows, restating the index maps
+  of cpu_herk_ftd (tests/visibility_pipeline_test.cpp:55-96) and of
+  qc_pol_gather_transpose_kernel (lib/bench_pipeline.cu:306-331).
 * Seeded input generators for the workloads the correlator is measured on.
 """
 from __future__ import annotations
@@ -81,6 +85,9 @@ def ref_lib():
         L.ref_encode.argtypes = [_i32p, _i32p, ctypes.c_int64, _u8p]
         L.ref_cpu_herk.argtypes = [_u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f64p]
         L.ref_cpu_herk_batch_first.argtypes = [_u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p]
+        if hasattr(L, "ref_cpu_herk_ftd"):
+            L.ref_cpu_herk_ftd.argtypes = [_u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p]
         L.ref_num_threads.restype = ctypes.c_int
         _ref = L
     return _ref
@@ -144,6 +151,51 @@ def ref_cpu_herk(qc: np.ndarray, N: int, K: int, batch: int) -> np.ndarray:
     out = np.empty((batch, tri_size(N), 2), dtype=np.float64)
     L.ref_cpu_herk(_p(qc, _u8p), N, K, batch, _p(out, _f64p))
     return out
+
+
+def ref_cpu_herk_ftd(raw: np.ndarray, batch_idx: int, n_ant: int, n_chan: int, n_pol: int,
+                     n_time_inner: int, n_time: int) -> np.ndarray:
+    """The reference's cpu_herk_ftd for one batch -> float32 [P, 2]."""
+    L = ref_lib()
+    if L is None or not hasattr(L, "ref_cpu_herk_ftd"):
+        raise RuntimeError("reference host correlator not built (oracle/build_ref.sh)")
+    raw = np.ascontiguousarray(raw, dtype=np.uint8).reshape(-1)
+    out = np.empty((tri_size(n_ant), 2), dtype=np.float32)
+    L.ref_cpu_herk_ftd(_p(raw, _u8p), batch_idx, n_ant, n_chan, n_pol, n_time_inner, n_time,
+                       _p(out, _f32p))
+    return out
+
+
+# layouts of raw packet-ordered input
+LAYOUT_TIME_ANT_CHAN_POL, LAYOUT_CHAN_POL_ANT_TIME = 0, 1
+
+
+def ftd_to_batch_first(raw: np.ndarray, n_ant: int, n_chan: int, n_pol: int, n_time: int,
+                       n_time_inner: int, layout: int, pol_sum: bool = False) -> np.ndarray:
+    """Raw QC bytes -> batch-first [batch, n_ant, K'] rows.
+
+    layout 0, [t][ant][chan][pol] with t = k*n_time_inner + ti
+      (cpu_herk_ftd, tests/visibility_pipeline_test.cpp:65-75);
+    layout 1, [chan][pol][ant][t] with t = ti*K + k
+      (qc_pol_gather_transpose_kernel, lib/bench_pipeline.cu:321-330).
+    batch b = (chan*n_pol + pol)*n_time_inner + ti, K' = K; with pol_sum the
+    pols are concatenated along the sample axis (column pol*K + k), b =
+    chan*n_time_inner + ti and K' = n_pol*K.
+    """
+    K = n_time // n_time_inner
+    raw = np.ascontiguousarray(raw, dtype=np.uint8).reshape(-1)
+    if layout == LAYOUT_TIME_ANT_CHAN_POL:
+        a = raw.reshape(K, n_time_inner, n_ant, n_chan, n_pol)   # [k, ti, ant, chan, pol]
+        a = a.transpose(3, 4, 1, 2, 0)                            # [chan, pol, ti, ant, k]
+    elif layout == LAYOUT_CHAN_POL_ANT_TIME:
+        a = raw.reshape(n_chan, n_pol, n_ant, n_time_inner, K)   # [chan, pol, ant, ti, k]
+        a = a.transpose(0, 1, 3, 2, 4)                            # [chan, pol, ti, ant, k]
+    else:
+        raise ValueError(layout)
+    if pol_sum:
+        a = a.transpose(0, 2, 3, 1, 4)                            # [chan, ti, ant, pol, k]
+        return np.ascontiguousarray(a).reshape(n_chan * n_time_inner, n_ant, n_pol * K)
+    return np.ascontiguousarray(a).reshape(n_chan * n_pol * n_time_inner, n_ant, K)
 
 
 def num_threads() -> int:

@@ -8,6 +8,7 @@
 //   cpu_herk              cutlass_interface/test_herk_int4.cu:51-70
 //   decode_qc_byte        tests/visibility_pipeline_test.cpp:42-53
 //   cpu_herk_batch_first  tests/visibility_pipeline_test.cpp:136-168
+//   cpu_herk_ftd          tests/visibility_pipeline_test.cpp:55-96
 // Test infrastructure only; the product never links it.
 #include <complex>
 #include <cstdint>
@@ -62,6 +63,12 @@ void ref_cpu_herk(const uint8_t* qc, int N, int K, int batch, double* out) {
 void ref_cpu_herk_batch_first(const uint8_t* qc, int N, int K, int batch, float* out) {
   const int64_t P = int64_t(N) * (N + 1) / 2;
   for (int b = 0; b < batch; ++b) cpu_herk_batch_first(qc, b, N, K, out + 2 * P * b);
+}
+
+// The reference's FTD-layout correlator for one batch; out = [P][2] float.
+void ref_cpu_herk_ftd(const uint8_t* qc, int batch_idx, int n_ant, int n_chan, int n_pol,
+                      int n_time_inner, int n_time, float* out) {
+  cpu_herk_ftd(qc, batch_idx, n_ant, n_chan, n_pol, n_time_inner, n_time, out);
 }
 
 int ref_num_threads(void) {

@@ -15,6 +15,10 @@ reference's packed lower triangles ``tri`` [batch, N(N+1)/2, 2]:
   CutlassHerkCorrectnessTest shape (:1188-1262).
 * herk_edge_*: ragged shapes (N, K not multiples of the tile sizes, N = 1,
   K = 1) and the all-(+-7) adversarial input, from cpu_herk.
+* ftd/ftd_tacp_*.npz: raw packet-ordered QC bytes [t][ant][chan][pol] and the
+  per-batch triangles of the reference's cpu_herk_ftd
+  (tests/visibility_pipeline_test.cpp:55-96), batch b = (chan*n_pol + pol)
+  *n_time_inner + ti.
 
 Run from the repository root: ``python tests/golden/make_golden.py``.
 """
@@ -66,6 +70,22 @@ def main():
         re, im = oracle.gaussian_int4(rng, (batch, N, K))
         qc = oracle.encode_qc(re, im)
         save(f"herk_edge_n{N}_k{K}_b{batch}", qc, N, K, batch, oracle.ref_cpu_herk(qc, N, K, batch))
+
+    # raw packet-ordered input through the reference's cpu_herk_ftd
+    os.makedirs(os.path.join(OUT, "ftd"), exist_ok=True)
+    for (n_ant, n_chan, n_pol, n_ti, K) in [(24, 3, 2, 2, 48), (37, 2, 2, 1, 70)]:
+        n_time = K * n_ti
+        raw = np.random.default_rng(n_ant * 100 + K).integers(
+            0, 256, size=n_time * n_ant * n_chan * n_pol, dtype=np.uint8)
+        nb = n_chan * n_pol * n_ti
+        tri = np.stack([oracle.ref_cpu_herk_ftd(raw, b, n_ant, n_chan, n_pol, n_ti, n_time)
+                        for b in range(nb)])
+        name = f"ftd_tacp_a{n_ant}_c{n_chan}_p{n_pol}_ti{n_ti}_k{K}"
+        assert np.all(tri == np.rint(tri)), name
+        np.savez_compressed(os.path.join(OUT, "ftd", name + ".npz"), raw=raw,
+                            tri=tri.astype(np.int32), n_ant=n_ant, n_chan=n_chan, n_pol=n_pol,
+                            n_time_inner=n_ti, n_time=n_time)
+        print(name, raw.size, "bytes in,", tri.shape)
 
     # adversarial: every sample +-7 in both parts (largest sums, all sign mixes)
     N, K, batch = 160, 256, 1

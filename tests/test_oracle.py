@@ -76,3 +76,68 @@ def test_oracle_matches_reference_cpu_herk_fresh_inputs():
         qc = rng.integers(0, 256, size=B * N * K, dtype=np.uint8)
         ref = oracle.ref_cpu_herk(qc, N, K, B)
         assert np.array_equal(oracle.herk_qc(qc, N, K, B).astype(np.float64), ref)
+
+
+# ------------------------------------------------ raw packet-ordered input
+def _ftd_golden(golden_dir):
+    return sorted(glob.glob(os.path.join(golden_dir, "ftd", "*.npz")))
+
+
+def test_ftd_corner_turn_matches_golden(golden_dir):
+    # the oracle's corner turn + int64 HERK against cpu_herk_ftd's triangles
+    files = _ftd_golden(golden_dir)
+    assert len(files) >= 2
+    for f in files:
+        z = np.load(f)
+        a, c, p = int(z["n_ant"]), int(z["n_chan"]), int(z["n_pol"])
+        ti, t = int(z["n_time_inner"]), int(z["n_time"])
+        bf = oracle.ftd_to_batch_first(z["raw"], a, c, p, t, ti, oracle.LAYOUT_TIME_ANT_CHAN_POL)
+        got = oracle.herk_qc(bf, a, t // ti, bf.shape[0])
+        assert np.array_equal(got, z["tri"].astype(np.int64)), os.path.basename(f)
+
+
+def test_ftd_corner_turn_matches_reference_fresh_inputs():
+    if oracle.ref_lib() is None or not hasattr(oracle.ref_lib(), "ref_cpu_herk_ftd"):
+        pytest.skip("reference host correlator not built")
+    rng = np.random.default_rng(77)
+    for (a, c, p, ti, K) in [(9, 4, 2, 3, 17), (16, 1, 1, 1, 64), (5, 2, 3, 2, 5)]:
+        t = K * ti
+        raw = rng.integers(0, 256, size=t * a * c * p, dtype=np.uint8)
+        bf = oracle.ftd_to_batch_first(raw, a, c, p, t, ti, oracle.LAYOUT_TIME_ANT_CHAN_POL)
+        R = oracle.herk_qc(bf, a, K, bf.shape[0]).astype(np.float32)
+        for b in range(bf.shape[0]):
+            assert np.array_equal(R[b], oracle.ref_cpu_herk_ftd(raw, b, a, c, p, ti, t)), (a, b)
+
+
+def test_ftd_chan_pol_ant_time_index_map():
+    # [chan][pol][ant][t], t = ti*K + k: restates the index arithmetic of
+    # qc_pol_gather_transpose_kernel (lib/bench_pipeline.cu:321-330), which
+    # writes pol p of (ch, t_inner, ant, k) from
+    # qc[ch*2*n_ant*n_time + p*n_ant*n_time + ant*n_time + t_inner*K + k]
+    a, c, p, ti, K = 6, 3, 2, 2, 9
+    t = ti * K
+    raw = np.random.default_rng(3).integers(0, 256, size=c * p * a * t, dtype=np.uint8)
+    bf = oracle.ftd_to_batch_first(raw, a, c, p, t, ti, oracle.LAYOUT_CHAN_POL_ANT_TIME)
+    for ch in range(c):
+        for pol in range(p):
+            for tin in range(ti):
+                for ant in range(a):
+                    for k in range(K):
+                        src = ch * p * a * t + pol * a * t + ant * t + tin * K + k
+                        b = (ch * p + pol) * ti + tin
+                        assert bf[b, ant, k] == raw[src]
+
+
+def test_ftd_pol_sum_is_sum_over_pols():
+    # pol_sum concatenates the pols along the sample axis: its HERK equals the
+    # sum of the per-pol HERKs (the reference adds pol 1 with beta = 1)
+    a, c, p, ti, K = 11, 2, 2, 2, 20
+    t = ti * K
+    rng = np.random.default_rng(4)
+    for layout in (oracle.LAYOUT_TIME_ANT_CHAN_POL, oracle.LAYOUT_CHAN_POL_ANT_TIME):
+        raw = rng.integers(0, 256, size=c * p * a * t, dtype=np.uint8)
+        per = oracle.ftd_to_batch_first(raw, a, c, p, t, ti, layout)
+        summed = oracle.ftd_to_batch_first(raw, a, c, p, t, ti, layout, pol_sum=True)
+        Rp = oracle.herk_qc(per, a, K, per.shape[0]).reshape(c, p, ti, -1, 2)
+        Rs = oracle.herk_qc(summed, a, p * K, summed.shape[0]).reshape(c, ti, -1, 2)
+        assert np.array_equal(Rs, Rp.sum(axis=1))
