@@ -362,9 +362,10 @@ def run_ours(args, rank, world, dist):
     if not args.no_e2e:
         e2e = run_e2e(torch, args, dev, qc, N, K, B, flops, world, dist)
 
-    batched = precision = differentiation = None
+    batched = precision = differentiation = raw_layout = None
     if not args.no_extra:
         batched = run_batched_leg(torch, dev)
+        raw_layout = run_ftd_leg(torch, dev)
         precision = run_precision_leg(torch, dev)
         differentiation = run_diff_leg(torch, dev)
 
@@ -410,6 +411,7 @@ def run_ours(args, rank, world, dist):
         "speedup_vs_plain": (value / world / plain["value"]) if plain else None,
         "e2e": e2e,
         "batched_uneven_flagged": batched,
+        "raw_layout_fused_corner_turn": raw_layout,
         "precision_modes": precision,
         "adjoint_and_gain_gradient": differentiation,
         "clocks": clk,
@@ -460,6 +462,37 @@ def run_batched_leg(torch, dev, seed=3, n_chans=96, inputs=4096):
                         f"1536..{inputs} active after flagging, one call (tuned, graph replay)",
             "value": flops / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms,
             "tflop_per_step": flops / 1e12}
+
+
+def run_ftd_leg(torch, dev, n_ant=2048, n_chan=64, n_pol=2, K=1024, seed=6):
+    """Raw packet-ordered input [t][ant][chan][pol] (2048 antennas x 64
+    channels x 2 pols x 1024 samples, 268 MB of QC bytes): the fused corner
+    turn + correlator (ftdx_herk_ftd, one triangle per (channel, pol)) against
+    the same correlation after a separate batch-first reorder pass."""
+    from ftd_b200 import Correlator, tri_size
+    from ftd_b200._lib import IN_INT4, LAYOUT_TIME_ANT_CHAN_POL, OUT_FP32
+    nb = n_chan * n_pol
+    raw = make_qc(torch, 1, K, n_ant * n_chan * n_pol, dev, seed=seed).reshape(-1)
+    C = torch.empty(nb, tri_size(n_ant), 2, device=dev)
+    flops = herk_flops(n_ant, K, nb)
+    with Correlator(device=dev.index) as c:
+        c.init_herk(n_ant, K, nb)
+        fused = _timed(torch, lambda: c.herk_ftd(raw, C, n_ant, n_chan, n_pol, K, 1,
+                                                  layout=LAYOUT_TIME_ANT_CHAN_POL), reps=10)
+        bf = torch.empty(nb, n_ant, K, dtype=torch.uint8, device=dev)
+
+        def separate():
+            bf.view(n_chan, n_pol, n_ant, K).copy_(raw.view(K, n_ant, n_chan, n_pol)
+                                                   .permute(2, 3, 1, 0))
+            c.herk(bf, C, n_ant, K, nb, input=IN_INT4, output=OUT_FP32, tune=False)
+        sep = _timed(torch, separate, reps=10)
+        if c.device_status() != 0:
+            raise RuntimeError("device wait timed out in the raw-layout leg")
+    return {"workload": f"raw [t][ant][chan][pol] QC: {n_ant} antennas x {n_chan} channels x "
+                        f"{n_pol} pols x K={K} -> {nb} triangles",
+            "value": flops / (fused * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": fused,
+            "separate_reorder_then_herk": {"value": flops / (sep * 1e-3) / 1e12,
+                                           "ms_per_step": sep}}
 
 
 def _timed(torch, fn, reps=5, warm=2):
