@@ -6,7 +6,8 @@ C ABI in ``include/ftdx.h``).  Importing this package does not need a GPU;
 calling into the library does, and fails loudly without one.
 """
 from ._lib import FtdxError, LIB_PATH, load  # noqa: F401
-from .herk import (Correlator, herk_batched_cutlass_fp16, herk_batched_cutlass_qc,  # noqa: F401
-                   herk_batched_cutlass_qc_fp16, init_cutlass_api, tri_size)
+from .herk import (Correlator, Pipeline, herk_batched_cutlass_fp16,  # noqa: F401
+                   herk_batched_cutlass_qc, herk_batched_cutlass_qc_fp16, init_cutlass_api,
+                   tri_size)
 
 __version__ = "0.1.0"

@@ -48,6 +48,12 @@ class FtdDesc(ctypes.Structure):
                 ("pol_sum", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
 
 
+class PipelineConfig(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int), ("K", ctypes.c_int), ("batch", ctypes.c_int),
+                ("output", ctypes.c_int), ("ftd", ctypes.POINTER(FtdDesc)),
+                ("host_threads", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
+
+
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
 _f = ctypes.c_float
@@ -66,6 +72,11 @@ PROTOTYPES = {
     "ftdx_herk_kahan": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
     "ftdx_herk_batched_v": (_i, [_vp, ctypes.c_void_p, _i, _i, _f, _f, _vp, _i]),
     "ftdx_herk_ftd": (_i, [_vp, _vp, _vp, ctypes.POINTER(FtdDesc), _i, _f, _f, _vp]),
+    "ftdx_pipeline_create": (_i, [_vp, ctypes.POINTER(PipelineConfig), ctypes.POINTER(_vp)]),
+    "ftdx_pipeline_correlate": (_i, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _i]),
+    "ftdx_pipeline_destroy": (_i, [_vp]),
+    "ftdx_pipeline_sizes": (_i, [_vp, ctypes.POINTER(ctypes.c_size_t),
+                                 ctypes.POINTER(ctypes.c_size_t)]),
     "ftdx_end_herk": (_i, [_vp]),
     "ftdx_device_status": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32)]),
     "ftdx_set_profiling": (_i, [_vp, _i]),

@@ -221,6 +221,80 @@ _api: Correlator | None = None
 _tune_enabled = False
 
 
+def _host_ptr(x) -> int:
+    """Address of a host buffer: a CPU torch tensor (pinned or not) or a
+    C-contiguous numpy array."""
+    if hasattr(x, "data_ptr"):
+        if getattr(x, "is_cuda", False):
+            raise FtdxError(1, "pipeline buffers are host memory")
+        if not x.is_contiguous():
+            raise FtdxError(1, "pipeline buffer is not contiguous")
+        return x.data_ptr()
+    if hasattr(x, "ctypes"):
+        if not x.flags["C_CONTIGUOUS"]:
+            raise FtdxError(1, "pipeline buffer is not C-contiguous")
+        return x.ctypes.data
+    raise TypeError(f"cannot take a host pointer of {type(x)!r}")
+
+
+class Pipeline:
+    """Host-to-host correlation of a stream of payloads (ftdx_pipeline_*):
+    H2D, correlation and D2H overlapped across payloads.  Replaces
+    VisibilityPipeline::correlate / correlate_pipelined (CUTLASS branch)."""
+
+    def __init__(self, corr: Correlator, N: int = 0, K: int = 0, batch: int = 0,
+                 output: int = OUT_FP32, ftd: dict | None = None, host_threads: int = 0):
+        self._corr = corr
+        self._L = corr._L
+        self._ftd = None
+        if ftd is not None:
+            self._ftd = _lib.FtdDesc(ftd["n_ant"], ftd["n_chan"], ftd["n_pol"], ftd["n_time"],
+                                     ftd.get("n_time_inner", 1),
+                                     ftd.get("layout", _lib.LAYOUT_TIME_ANT_CHAN_POL),
+                                     int(bool(ftd.get("pol_sum", False))))
+        cfg = _lib.PipelineConfig(N, K, batch, output,
+                                  ctypes.pointer(self._ftd) if self._ftd is not None else None,
+                                  host_threads)
+        h = ctypes.c_void_p()
+        check(corr._h, self._L.ftdx_pipeline_create(corr._h, ctypes.byref(cfg), ctypes.byref(h)),
+              "ftdx_pipeline_create")
+        self._p = h
+
+    @property
+    def sizes(self) -> tuple[int, int]:
+        a, b = ctypes.c_size_t(), ctypes.c_size_t()
+        check(self._corr._h, self._L.ftdx_pipeline_sizes(self._p, ctypes.byref(a), ctypes.byref(b)),
+              "ftdx_pipeline_sizes")
+        return a.value, b.value
+
+    def correlate(self, vis_outputs, raw_inputs) -> None:
+        """Correlate every payload; returns when all outputs are in host memory."""
+        n = len(raw_inputs)
+        if len(vis_outputs) != n:
+            raise FtdxError(1, "as many outputs as inputs are needed")
+        outs = (ctypes.c_void_p * max(n, 1))(*[_host_ptr(v) for v in vis_outputs])
+        ins = (ctypes.c_void_p * max(n, 1))(*[_host_ptr(r) for r in raw_inputs])
+        check(self._corr._h, self._L.ftdx_pipeline_correlate(self._p, outs, ins, n),
+              "ftdx_pipeline_correlate")
+
+    def close(self):
+        if self._p:
+            self._L.ftdx_pipeline_destroy(self._p)
+            self._p = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def _get_api() -> Correlator:
     global _api
     if _api is None:

@@ -160,6 +160,36 @@ FTDX_API ftdx_status ftdx_herk_ftd(ftdx_handle h, const void* raw, void* C,
                                    const ftdx_ftd_desc* desc, ftdx_output output, float alpha,
                                    float beta, void* stream);
 
+/* Host-to-host correlation pipeline: replaces the CUTLASS branch of
+ * ggp::VisibilityPipeline::correlate and ::correlate_pipelined
+ * (lib/visibility_pipeline.cu:253-308, 483-549).  For every payload: H2D of
+ * the raw QC bytes, correlation, D2H of the packed triangles (split over two
+ * streams, i.e. two copy engines) with two device buffer sets, so that
+ * payload p's D2H overlaps payload p+1's H2D and correlation.  Host buffers may be pinned (DMA
+ * directly) or pageable (staged through pinned buffers, copied by
+ * host_threads threads).  A payload is batch-first QC [batch][N][K] bytes, or,
+ * when ftd is set, raw packet-ordered bytes described by *ftd (see
+ * ftdx_herk_ftd).  ftdx_pipeline_correlate returns when every output is in
+ * host memory.  The pipeline uses the handle's correlator (its workspace,
+ * tuning cache and strategy); one pipeline per handle at a time. */
+typedef struct ftdx_pipeline* ftdx_pipeline_t;
+
+typedef struct ftdx_pipeline_config {
+  int N, K, batch;          /* batch-first payload geometry (ignored when ftd is set) */
+  ftdx_output output;
+  const ftdx_ftd_desc* ftd; /* raw packet-ordered payloads instead (copied at create) */
+  int host_threads;         /* threads for pageable staging copies (0: up to 8) */
+  int reserved[7];
+} ftdx_pipeline_config;
+
+FTDX_API ftdx_status ftdx_pipeline_create(ftdx_handle h, const ftdx_pipeline_config* cfg,
+                                          ftdx_pipeline_t* out);
+FTDX_API ftdx_status ftdx_pipeline_correlate(ftdx_pipeline_t p, void* const* vis_outputs,
+                                             const void* const* raw_inputs, int n_payloads);
+FTDX_API ftdx_status ftdx_pipeline_destroy(ftdx_pipeline_t p);
+/* Bytes of one payload's input and output. */
+FTDX_API ftdx_status ftdx_pipeline_sizes(ftdx_pipeline_t p, size_t* in_bytes, size_t* out_bytes);
+
 /* Kahan-compensated accumulation across integration dumps (no counterpart
  * in the reference): sum += A A^H with the FP32 rounding error of every
  * addition carried in `comp` (same packed layout and size as `sum`, complex64,
