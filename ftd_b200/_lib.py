@@ -72,6 +72,8 @@ PROTOTYPES = {
     "ftdx_herk_kahan": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
     "ftdx_herk_batched_v": (_i, [_vp, ctypes.c_void_p, _i, _i, _f, _f, _vp, _i]),
     "ftdx_herk_ftd": (_i, [_vp, _vp, _vp, ctypes.POINTER(FtdDesc), _i, _f, _f, _vp]),
+    "ftdx_strided_batch_gemm": (ctypes.c_longlong, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _i,
+                                                    _i, _vp]),
     "ftdx_pipeline_create": (_i, [_vp, ctypes.POINTER(PipelineConfig), ctypes.POINTER(_vp)]),
     "ftdx_pipeline_correlate": (_i, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _i]),
     "ftdx_pipeline_destroy": (_i, [_vp]),

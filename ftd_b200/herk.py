@@ -130,6 +130,13 @@ class Correlator:
                                    float(alpha), float(beta), _stream(stream))
         check(self._h, st, "ftdx_herk_ftd")
 
+    def strided_batch_gemm(self, A, B, C, m: int, n: int, k: int, trans_a: int, trans_b: int,
+                           batch: int, data_type: int, stream=None) -> int:
+        """quda::stridedBatchGEMMCutlass's HERK branch: flop count, or -1."""
+        return int(self._L.ftdx_strided_batch_gemm(self._h, _ptr(A), _ptr(B), _ptr(C), m, n, k,
+                                                   trans_a, trans_b, batch, data_type,
+                                                   _stream(stream)))
+
     def herk_kahan(self, A, S, comp, N: int, K: int, batch: int, input: int = IN_INT4,
                    compute: int = COMPUTE_FP8, stream=None) -> None:
         """S += A A^H with Kahan compensation kept in `comp` (both packed complex64)."""

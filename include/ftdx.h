@@ -190,6 +190,19 @@ FTDX_API ftdx_status ftdx_pipeline_destroy(ftdx_pipeline_t p);
 /* Bytes of one payload's input and output. */
 FTDX_API ftdx_status ftdx_pipeline_sizes(ftdx_pipeline_t p, size_t* in_bytes, size_t* out_bytes);
 
+/* The HERK branch of quda::stridedBatchGEMMCutlass (lib/cutlass_interface.cu:316-381),
+ * the XEngine's BLAS entry: when A == B, trans_a is the conjugate transpose
+ * (QUDA_BLAS_OP_C = 2), trans_b none (QUDA_BLAS_OP_N = 0), m == n and data_type
+ * is single complex (QUDA_BLAS_DATATYPE_C = 2), C = A A^H is computed for the
+ * [batch][n][k] interleaved complex64 A into the packed lower triangle
+ * (complex64) at C, and the reference's flop count 8*m*n*k*batch is returned
+ * after the stream is synchronised.  Any other pattern returns -1 with the last
+ * error set (the reference reports it through errorQuda).  FP8 with a
+ * per-channel scale where the reference narrows to unscaled FP16 -> FP8. */
+FTDX_API long long ftdx_strided_batch_gemm(ftdx_handle h, const void* A, const void* B, void* C,
+                                           int m, int n, int k, int trans_a, int trans_b,
+                                           int batch, int data_type, void* stream);
+
 /* Kahan-compensated accumulation across integration dumps (no counterpart
  * in the reference): sum += A A^H with the FP32 rounding error of every
  * addition carried in `comp` (same packed layout and size as `sum`, complex64,
