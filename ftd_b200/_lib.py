@@ -48,6 +48,15 @@ class FtdDesc(ctypes.Structure):
                 ("pol_sum", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
 
 
+class ImagingConfig(ctypes.Structure):
+    _fields_ = [("n_ant", ctypes.c_int), ("n_chan", ctypes.c_int), ("n_pol", ctypes.c_int),
+                ("n_grid", ctypes.c_int), ("n_beam", ctypes.c_int), ("chan_tile", ctypes.c_int),
+                ("cell_size_rad", ctypes.c_float), ("baseline_uv_m", ctypes.c_void_p),
+                ("freq_hz", ctypes.c_void_p), ("taper", ctypes.c_void_p),
+                ("beam_pixels", ctypes.c_void_p), ("output_stage", ctypes.c_int),
+                ("reserved", ctypes.c_int * 7)]
+
+
 class PipelineConfig(ctypes.Structure):
     _fields_ = [("N", ctypes.c_int), ("K", ctypes.c_int), ("batch", ctypes.c_int),
                 ("output", ctypes.c_int), ("ftd", ctypes.POINTER(FtdDesc)),
@@ -74,6 +83,7 @@ PROTOTYPES = {
     "ftdx_herk_ftd": (_i, [_vp, _vp, _vp, ctypes.POINTER(FtdDesc), _i, _f, _f, _vp]),
     "ftdx_strided_batch_gemm": (ctypes.c_longlong, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _i,
                                                     _i, _vp]),
+    "ftdx_image_beams": (_i, [_vp, ctypes.POINTER(ImagingConfig), _vp, _vp, _vp, _vp]),
     "ftdx_pipeline_create": (_i, [_vp, ctypes.POINTER(PipelineConfig), ctypes.POINTER(_vp)]),
     "ftdx_pipeline_correlate": (_i, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _i]),
     "ftdx_pipeline_destroy": (_i, [_vp]),

@@ -72,7 +72,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         _run(cmd)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    _run([NVCC, *ARCH, "-shared", "-o", tmp, *objs])
+    _run([NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcufft", "-Xlinker",
+          "-rpath=/usr/local/cuda/lib64"])
     os.replace(tmp, LIB)
     return LIB
 

@@ -107,6 +107,8 @@ struct ftdx_context {
   };
   std::vector<Timed> timed;
   std::vector<cudaEvent_t> event_pool;
+  // imaging workspace and FFT plans (imaging.cu), created on first use
+  std::shared_ptr<void> imaging;
 };
 
 namespace ftdx {

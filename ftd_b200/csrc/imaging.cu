@@ -1,0 +1,204 @@
+// imaging.cu -- UV gridding of the packed triangles with fused polarisation
+// reduction and taper, inverse 2-D FFT (cuFFT), beam extraction
+// (ftdx_image_beams).  Replaces the FP32 paths of
+// imaging_pipeline::ImagingPipeline::grid_and_image (lib/imaging_pipeline.cu)
+// and stages 2-5 of VisibilityBeamformer::compute (lib/visibility_bf.cpp:305-380);
+// cell arithmetic as uv_cell / pillbox_grid_scatter_fp32_fp32grid_kernel
+// (include/kernels/imaging_kernels.cuh:37-47, 219-268).
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <memory>
+
+#include "context.h"
+
+namespace ftdx {
+
+struct ImagingState {
+  float2* grid = nullptr;
+  size_t grid_bytes = 0;
+  std::map<std::pair<int, int>, cufftHandle> plans;  // (Ng, channels) -> plan
+  ~ImagingState() {
+    for (auto& p : plans) cufftDestroy(p.second);
+    if (grid) cudaFree(grid);
+  }
+};
+
+namespace {
+
+constexpr double kLightSpeed = 299792458.0;
+
+// Row i and column j of packed lower-triangle index k = i(i+1)/2 + j (exact
+// for every k of a 32-bit row count).
+__device__ __forceinline__ void tri_row_col(int64_t k, int& i, int& j) {
+  int64_t r = int64_t((sqrt(8.0 * double(k) + 1.0) - 1.0) * 0.5);
+  while (r * (r + 1) / 2 > k) --r;
+  while ((r + 1) * (r + 2) / 2 <= k) ++r;
+  i = int(r);
+  j = int(k - r * (r + 1) / 2);
+}
+
+// One thread per (channel of the tile, baseline): sum the n_pol visibilities,
+// then add them (times the taper weight of the cell) at the baseline's cell
+// and, for a cross-correlation, the conjugate at the mirrored cell.
+__global__ void __launch_bounds__(256) grid_scatter_kernel(
+    const float2* __restrict__ vis, const float2* __restrict__ uv, const double* __restrict__ freq,
+    const float* __restrict__ taper, float2* __restrict__ grid, int64_t n_bl, int n_pol, int Ng,
+    int f0, int nf, float cell) {
+  const int64_t total = int64_t(nf) * n_bl;
+  const int64_t plane = int64_t(Ng) * Ng;
+  const float half = 0.5f * float(Ng);
+  for (int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < total;
+       x += int64_t(gridDim.x) * blockDim.x) {
+    const int fl = int(x / n_bl);
+    const int64_t k = x - int64_t(fl) * n_bl;
+    const int f = f0 + fl;
+    const float2* vp = vis + int64_t(f) * n_pol * n_bl + k;
+    float2 v = __ldg(vp);
+    for (int p = 1; p < n_pol; ++p) {
+      const float2 w = __ldg(vp + int64_t(p) * n_bl);
+      v.x += w.x;
+      v.y += w.y;
+    }
+    const float2 b = __ldg(uv + k);
+    const double lambda = kLightSpeed / __ldg(freq + f);
+    const float ul = float(double(b.x) / lambda), vl = float(double(b.y) / lambda);
+    float2* g = grid + int64_t(fl) * plane;
+    const int iu = int(roundf(ul / cell + half)), iv = int(roundf(vl / cell + half));
+    if (iu >= 0 && iu < Ng && iv >= 0 && iv < Ng) {
+      const int64_t c = int64_t(iv) * Ng + iu;
+      const float wt = taper ? __ldg(taper + c) : 1.f;
+      atomicAdd(g + c, make_float2(v.x * wt, v.y * wt));
+    }
+    int i, j;
+    tri_row_col(k, i, j);
+    if (i != j) {
+      const int iuc = int(roundf(-ul / cell + half)), ivc = int(roundf(-vl / cell + half));
+      if (iuc >= 0 && iuc < Ng && ivc >= 0 && ivc < Ng) {
+        const int64_t c = int64_t(ivc) * Ng + iuc;
+        const float wt = taper ? __ldg(taper + c) : 1.f;
+        atomicAdd(g + c, make_float2(v.x * wt, -v.y * wt));
+      }
+    }
+  }
+}
+
+__global__ void beam_extract_kernel(const float2* __restrict__ img, const int* __restrict__ pix,
+                                    float* __restrict__ beams, int Ng, int n_beam, int nf,
+                                    float norm) {
+  const int total = nf * n_beam;
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < total; x += gridDim.x * blockDim.x) {
+    const int fl = x / n_beam, b = x - fl * n_beam;
+    const int r = __ldg(pix + 2 * b), c = __ldg(pix + 2 * b + 1);
+    float out = 0.f;
+    if (r >= 0 && r < Ng && c >= 0 && c < Ng) {
+      const float2 z = img[int64_t(fl) * Ng * Ng + int64_t(r) * Ng + c];
+      out = (z.x * z.x + z.y * z.y) * norm;
+    }
+    beams[x] = out;
+  }
+}
+
+}  // namespace
+}  // namespace ftdx
+
+using namespace ftdx;
+
+extern "C" ftdx_status ftdx_image_beams(ftdx_handle h, const ftdx_imaging_config* cfg,
+                                        const void* vis, float* beams, void* grid_out,
+                                        void* stream) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  if (!cfg || !vis) return fail(h, FTDX_ERR_INVALID_ARG, "image_beams: null config or vis");
+  const ftdx_imaging_config& c = *cfg;
+  if (c.n_ant < 1 || c.n_chan < 1 || c.n_pol < 1 || c.n_grid < 2 || c.n_beam < 0 ||
+      c.chan_tile < 0 || !(c.cell_size_rad > 0.f) || !c.baseline_uv_m || !c.freq_hz ||
+      c.output_stage < 0 || c.output_stage > 2 || c.n_grid > 32768)
+    return fail(h, FTDX_ERR_INVALID_ARG, "image_beams: bad configuration");
+  if (c.output_stage == 0 && c.n_beam > 0 && (!beams || !c.beam_pixels))
+    return fail(h, FTDX_ERR_INVALID_ARG, "image_beams: beams need beam_pixels and an output");
+  if (c.output_stage > 0 && !grid_out)
+    return fail(h, FTDX_ERR_INVALID_ARG, "image_beams: output_stage %d needs grid_out",
+                c.output_stage);
+  if (((reinterpret_cast<uintptr_t>(vis) | reinterpret_cast<uintptr_t>(c.baseline_uv_m)) & 7) != 0)
+    return fail(h, FTDX_ERR_INVALID_ARG, "image_beams: vis and baseline_uv_m must be 8-byte aligned");
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int Ng = c.n_grid;
+  const int64_t plane = int64_t(Ng) * Ng;
+  const int64_t n_bl = int64_t(c.n_ant) * (c.n_ant + 1) / 2;
+  int tile = c.chan_tile;
+  if (tile == 0) tile = int(std::max<int64_t>(1, (int64_t(64) << 20) / (plane * 8)));
+  tile = std::min(tile, c.n_chan);
+  if (!h->imaging) h->imaging = std::make_shared<ImagingState>();
+  auto* st = static_cast<ImagingState*>(h->imaging.get());
+  const size_t need = size_t(tile) * size_t(plane) * sizeof(float2);
+  if (st->grid_bytes < need) {
+    if (stream_capturing(s))
+      return fail(h, FTDX_ERR_CAPACITY, "image_beams: grid workspace needed while capturing");
+    cudaStreamSynchronize(s);
+    if (st->grid) cudaFree(st->grid);
+    st->grid = nullptr;
+    st->grid_bytes = 0;
+    e = cudaMalloc(&st->grid, need);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(h, FTDX_ERR_ALLOC, "image_beams: grid workspace of %zu bytes", need);
+    }
+    st->grid_bytes = need;
+  }
+  const float norm = 1.f / (float(Ng) * float(Ng));
+  for (int f0 = 0; f0 < c.n_chan; f0 += tile) {
+    const int nf = std::min(tile, c.n_chan - f0);
+    e = cudaMemsetAsync(st->grid, 0, size_t(nf) * size_t(plane) * sizeof(float2), s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "grid clear");
+    {
+      const int64_t total = int64_t(nf) * n_bl;
+      const int64_t blocks = std::min<int64_t>((total + 255) / 256, int64_t(h->sm_count) * 32);
+      grid_scatter_kernel<<<unsigned(std::max<int64_t>(blocks, 1)), 256, 0, s>>>(
+          static_cast<const float2*>(vis), reinterpret_cast<const float2*>(c.baseline_uv_m),
+          c.freq_hz, c.taper, st->grid, n_bl, c.n_pol, Ng, f0, nf, c.cell_size_rad);
+      e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return cuda_fail(h, e, "grid scatter launch");
+    if (c.output_stage == 1) {
+      e = cudaMemcpyAsync(static_cast<float2*>(grid_out) + int64_t(f0) * plane, st->grid,
+                          size_t(nf) * size_t(plane) * sizeof(float2), cudaMemcpyDeviceToDevice, s);
+      if (e != cudaSuccess) return cuda_fail(h, e, "grid copy");
+      continue;
+    }
+    const auto key = std::make_pair(Ng, nf);
+    auto it = st->plans.find(key);
+    if (it == st->plans.end()) {
+      if (stream_capturing(s))
+        return fail(h, FTDX_ERR_CAPACITY, "image_beams: FFT plan needed while capturing");
+      cufftHandle plan = 0;
+      int n[2] = {Ng, Ng};
+      if (cufftPlanMany(&plan, 2, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, nf) !=
+          CUFFT_SUCCESS)
+        return fail(h, FTDX_ERR_CUDA, "image_beams: cufftPlanMany(%d x %d, %d) failed", Ng, Ng,
+                    nf);
+      it = st->plans.emplace(key, plan).first;
+    }
+    if (cufftSetStream(it->second, s) != CUFFT_SUCCESS ||
+        cufftExecC2C(it->second, reinterpret_cast<cufftComplex*>(st->grid),
+                     reinterpret_cast<cufftComplex*>(st->grid), CUFFT_INVERSE) != CUFFT_SUCCESS)
+      return fail(h, FTDX_ERR_CUDA, "image_beams: inverse FFT failed");
+    if (c.output_stage == 2) {
+      e = cudaMemcpyAsync(static_cast<float2*>(grid_out) + int64_t(f0) * plane, st->grid,
+                          size_t(nf) * size_t(plane) * sizeof(float2), cudaMemcpyDeviceToDevice, s);
+      if (e != cudaSuccess) return cuda_fail(h, e, "image copy");
+      continue;
+    }
+    if (c.n_beam > 0) {
+      const int total = nf * c.n_beam;
+      beam_extract_kernel<<<unsigned(std::min((total + 255) / 256, h->sm_count * 8)), 256, 0, s>>>(
+          st->grid, c.beam_pixels, beams + int64_t(f0) * c.n_beam, Ng, c.n_beam, nf, norm);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(h, e, "beam extraction launch");
+    }
+  }
+  return FTDX_OK;
+}

@@ -130,6 +130,20 @@ class Correlator:
                                    float(alpha), float(beta), _stream(stream))
         check(self._h, st, "ftdx_herk_ftd")
 
+    def image_beams(self, vis, beams, n_ant: int, n_chan: int, n_pol: int, n_grid: int,
+                    cell_size_rad: float, baseline_uv_m, freq_hz, taper=None, beam_pixels=None,
+                    n_beam: int = 0, chan_tile: int = 0, output_stage: int = 0, grid_out=None,
+                    stream=None) -> None:
+        """Grid the packed triangles (pols summed, taper fused), inverse FFT and
+        extract beam intensities (ftdx_image_beams).  output_stage 1 / 2 write
+        the UV grid / image of every channel to grid_out instead."""
+        cfg = _lib.ImagingConfig(n_ant, n_chan, n_pol, n_grid, n_beam, chan_tile,
+                                 float(cell_size_rad), _ptr(baseline_uv_m), _ptr(freq_hz),
+                                 _ptr(taper), _ptr(beam_pixels), output_stage)
+        st = self._L.ftdx_image_beams(self._h, ctypes.byref(cfg), _ptr(vis), _ptr(beams),
+                                      _ptr(grid_out), _stream(stream))
+        check(self._h, st, "ftdx_image_beams")
+
     def strided_batch_gemm(self, A, B, C, m: int, n: int, k: int, trans_a: int, trans_b: int,
                            batch: int, data_type: int, stream=None) -> int:
         """quda::stridedBatchGEMMCutlass's HERK branch: flop count, or -1."""

@@ -190,6 +190,40 @@ FTDX_API ftdx_status ftdx_pipeline_destroy(ftdx_pipeline_t p);
 /* Bytes of one payload's input and output. */
 FTDX_API ftdx_status ftdx_pipeline_sizes(ftdx_pipeline_t p, size_t* in_bytes, size_t* out_bytes);
 
+/* ---- imaging from the packed triangles -----------------------------------
+ * Replaces imaging_pipeline::ImagingPipeline::grid_and_image
+ * (include/imaging_pipeline.h, lib/imaging_pipeline.cu) and stages 2-5 of
+ * VisibilityBeamformer::compute (lib/visibility_bf.cpp:305-380) for FP32
+ * visibilities and an FP32 FFT.  Per channel f: every baseline k of the packed
+ * lower triangle (n_bl = n_ant(n_ant+1)/2, row i, column j <= i) is summed over
+ * the n_pol polarisation triangles (fused pol reduction), pillbox-gridded at
+ *   (iu, iv) = round((u_k, v_k) / lambda_f / cell + Ng/2)
+ * and, when i != j, its conjugate at round((-u, -v) / lambda_f / cell + Ng/2)
+ * (cells outside [0, Ng) dropped), each contribution multiplied by the taper
+ * weight of its cell (the taper fused into the scatter); then an unnormalised
+ * inverse 2-D FFT (cuFFT C2C), and beam b of channel f = |image(row_b, col_b)|^2
+ * * norm, norm = 1/Ng^2 (0 for pixels outside the image).
+ * vis: device FP32 [n_chan][n_pol][n_bl][2]; beams: device FP32 [n_chan][n_beam].
+ * output_stage: 0 = beams; 1 = the tapered UV grid and 2 = the image, both
+ * [n_chan][Ng][Ng] complex64 written to grid_out (for checking; beams then
+ * untouched).  The grid workspace holds chan_tile channels (0: as many as
+ * fit in 64 MiB, so that the atomics stay in L2). */
+typedef struct ftdx_imaging_config {
+  int n_ant, n_chan, n_pol, n_grid, n_beam;
+  int chan_tile;
+  float cell_size_rad;
+  const float* baseline_uv_m;  /* device [n_bl][2] (u, v) in metres */
+  const double* freq_hz;       /* device [n_chan] */
+  const float* taper;          /* device [n_grid * n_grid], or NULL */
+  const int* beam_pixels;      /* device [n_beam][2] (row, col), or NULL if n_beam == 0 */
+  int output_stage;
+  int reserved[7];
+} ftdx_imaging_config;
+
+FTDX_API ftdx_status ftdx_image_beams(ftdx_handle h, const ftdx_imaging_config* cfg,
+                                      const void* vis, float* beams, void* grid_out,
+                                      void* stream);
+
 /* The HERK branch of quda::stridedBatchGEMMCutlass (lib/cutlass_interface.cu:316-381),
  * the XEngine's BLAS entry: when A == B, trans_a is the conjugate transpose
  * (QUDA_BLAS_OP_C = 2), trans_b none (QUDA_BLAS_OP_N = 0), m == n and data_type

@@ -297,3 +297,77 @@ def gain_loss_grad(robs: np.ndarray, rmod: np.ndarray, w: np.ndarray, g: np.ndar
         L += float(np.sum(W * np.abs(E) ** 2))
         grad += -4.0 * (W * E * np.conj(Rm)) @ g
     return L, grad
+
+
+# ----------------------------------------------------------------- imaging
+C_LIGHT = 299792458.0
+
+
+def _roundf(x: np.ndarray) -> np.ndarray:
+    """C roundf (halves away from zero) of float32 values, evaluated exactly."""
+    x = x.astype(np.float64)
+    return (np.sign(x) * np.floor(np.abs(x) + 0.5)).astype(np.int64)
+
+
+def tri_rows_cols(n: int):
+    """Row i and column j of every packed lower-triangle index, in order."""
+    i = np.repeat(np.arange(n), np.arange(1, n + 1))
+    j = np.arange(n * (n + 1) // 2) - i * (i + 1) // 2
+    return i, j
+
+
+def uv_cells(uv_m: np.ndarray, freq_hz: float, cell: float, ng: int):
+    """Cell of each baseline and of its mirror, with the float32 arithmetic of
+    uv_cell (include/kernels/imaging_kernels.cuh:37-47): u_lam = float(u / lambda),
+    iu = roundf(u_lam / cell + Ng/2); mirror roundf(-u_lam / cell + Ng/2)."""
+    lam = C_LIGHT / float(freq_hz)
+    ul = (uv_m[:, 0].astype(np.float64) / lam).astype(np.float32)
+    vl = (uv_m[:, 1].astype(np.float64) / lam).astype(np.float32)
+    c, h = np.float32(cell), np.float32(0.5 * ng)
+    iu = _roundf((ul / c).astype(np.float32) + h)
+    iv = _roundf((vl / c).astype(np.float32) + h)
+    iuc = _roundf((-ul / c).astype(np.float32) + h)
+    ivc = _roundf((-vl / c).astype(np.float32) + h)
+    return iu, iv, iuc, ivc
+
+
+def image_grid(vis: np.ndarray, uv_m: np.ndarray, freq_hz: np.ndarray, n_ant: int, ng: int,
+               cell: float, taper: np.ndarray | None = None) -> np.ndarray:
+    """Pillbox gridding (pillbox_grid_scatter_fp32_fp32grid_kernel,
+    include/kernels/imaging_kernels.cuh:219-268) of vis [n_chan, n_pol, n_bl, 2]
+    float32, the pols summed first (in pol order, float32) and each
+    contribution weighted by the taper at its cell; auto-correlations (i == j)
+    are not mirrored.  Returns complex128 [n_chan, Ng, Ng] (exact sums)."""
+    n_chan, n_pol = vis.shape[0], vis.shape[1]
+    v = vis[:, 0].astype(np.float32).copy()
+    for p in range(1, n_pol):
+        v = (v + vis[:, p]).astype(np.float32)
+    vc = v[..., 0].astype(np.float64) + 1j * v[..., 1].astype(np.float64)
+    i, j = tri_rows_cols(n_ant)
+    cross = i != j
+    w = np.ones((ng, ng)) if taper is None else taper.astype(np.float64).reshape(ng, ng)
+    grid = np.zeros((n_chan, ng, ng), dtype=np.complex128)
+    for f in range(n_chan):
+        iu, iv, iuc, ivc = uv_cells(uv_m, freq_hz[f], cell, ng)
+        ok = (iu >= 0) & (iu < ng) & (iv >= 0) & (iv < ng)
+        np.add.at(grid[f], (iv[ok], iu[ok]), vc[f][ok] * w[iv[ok], iu[ok]])
+        okc = cross & (iuc >= 0) & (iuc < ng) & (ivc >= 0) & (ivc < ng)
+        np.add.at(grid[f], (ivc[okc], iuc[okc]), np.conj(vc[f][okc]) * w[ivc[okc], iuc[okc]])
+    return grid
+
+
+def image_from_grid(grid: np.ndarray) -> np.ndarray:
+    """Unnormalised inverse 2-D DFT over the last two axes (cuFFT CUFFT_INVERSE)."""
+    ng = grid.shape[-1]
+    return np.fft.ifft2(grid, axes=(-2, -1)) * (ng * ng)
+
+
+def beam_intensity(image: np.ndarray, pixels: np.ndarray) -> np.ndarray:
+    """|image(row, col)|^2 / Ng^2 per beam, 0 outside the image
+    (extract_beam_intensity_kernel, include/kernels/imaging_kernels.cuh:332-361)."""
+    ng = image.shape[-1]
+    out = np.zeros((image.shape[0], len(pixels)))
+    for b, (r, c) in enumerate(pixels):
+        if 0 <= r < ng and 0 <= c < ng:
+            out[:, b] = np.abs(image[:, r, c]) ** 2 / (ng * ng)
+    return out

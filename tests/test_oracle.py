@@ -141,3 +141,61 @@ def test_ftd_pol_sum_is_sum_over_pols():
         Rp = oracle.herk_qc(per, a, K, per.shape[0]).reshape(c, p, ti, -1, 2)
         Rs = oracle.herk_qc(summed, a, p * K, summed.shape[0]).reshape(c, ti, -1, 2)
         assert np.array_equal(Rs, Rp.sum(axis=1))
+
+
+# ------------------------------------------------ imaging
+def _tri(i, j):
+    return i * (i + 1) // 2 + j
+
+
+def test_imaging_point_and_mirror():
+    # test_gridding_scatter_fp32_grid (lib/test_imaging.cu:109-160): baseline
+    # (1, 0) at u = 2 lambda, v = 3 lambda, cell 1, vis (1, 0.5) lands at
+    # (Ng/2 + 2, Ng/2 + 3) and its conjugate at (Ng/2 - 2, Ng/2 - 3)
+    n, ng, f = 4, 32, 1.0e9
+    lam = oracle.C_LIGHT / f
+    uv = np.zeros((n * (n + 1) // 2, 2), dtype=np.float32)
+    uv[_tri(1, 0)] = [2.0 * lam, 3.0 * lam]
+    vis = np.zeros((1, 1, n * (n + 1) // 2, 2), dtype=np.float32)
+    vis[0, 0, _tri(1, 0)] = [1.0, 0.5]
+    g = oracle.image_grid(vis, uv, np.array([f]), n, ng, 1.0)
+    h = ng // 2
+    assert g[0, h + 3, h + 2] == 1.0 + 0.5j and g[0, h - 3, h - 2] == 1.0 - 0.5j
+    assert np.count_nonzero(g) == 2  # the other baselines carry zero visibility
+
+
+def test_imaging_auto_not_mirrored_and_pol_sum():
+    # test_conjugate_symmetry (lib/test_imaging.cu:163-217): an auto-correlation
+    # at u = 5 appears once, a cross-correlation at u = 3 at +-3 (conjugated)
+    n, ng, f = 3, 32, 1.0e9
+    lam = oracle.C_LIGHT / f
+    uv = np.zeros((6, 2), dtype=np.float32)
+    uv[_tri(1, 1), 0] = 5.0 * lam
+    uv[_tri(2, 0), 0] = 3.0 * lam
+    vis = np.zeros((1, 2, 6, 2), dtype=np.float32)
+    vis[0, 0, _tri(1, 1)] = [2.0, 1.0]
+    vis[0, 0, _tri(2, 0)] = [4.0, 2.0]
+    vis[0, 1, _tri(2, 0)] = [1.0, 1.0]      # second pol adds before gridding
+    g = oracle.image_grid(vis, uv, np.array([f]), n, ng, 1.0)
+    h = ng // 2
+    assert g[0, h, h + 5] == 2.0 + 1.0j and g[0, h, h - 5] == 0
+    assert g[0, h, h + 3] == 5.0 + 3.0j and g[0, h, h - 3] == 5.0 - 3.0j
+
+
+def test_imaging_beams_and_fft_definition():
+    # test_beam_extraction_fp32 (lib/test_imaging.cu:624-660): |3+4i|^2 / Ng^2 etc.
+    ng = 16
+    img = np.zeros((1, ng, ng), dtype=np.complex128)
+    img[0, 4, 5], img[0, 7, 8], img[0, 0, 0] = 3 + 4j, 1, 2j
+    b = oracle.beam_intensity(img, [(4, 5), (7, 8), (0, 0), (-1, 3)])
+    assert np.allclose(b[0], [25 / ng**2, 1 / ng**2, 4 / ng**2, 0])
+    # a unit point at the grid centre transforms to |image| = 1 everywhere
+    # (test_fft_roundtrip_fp32, lib/test_imaging.cu:287-323)
+    g = np.zeros((1, 32, 32), dtype=np.complex128)
+    g[0, 16, 16] = 1
+    assert np.allclose(np.abs(oracle.image_from_grid(g)), 1.0)
+
+
+def test_imaging_roundf_halves_away_from_zero():
+    x = np.array([0.5, 1.5, 2.5, -0.5, -1.5, 0.49999997], dtype=np.float32)
+    assert list(oracle._roundf(x)) == [1, 2, 3, -1, -2, 0]
