@@ -362,10 +362,11 @@ def run_ours(args, rank, world, dist):
     if not args.no_e2e:
         e2e = run_e2e(torch, args, dev, qc, N, K, B, flops, world, dist)
 
-    batched = precision = differentiation = raw_layout = None
+    batched = precision = differentiation = raw_layout = imaging = None
     if not args.no_extra:
         batched = run_batched_leg(torch, dev)
         raw_layout = run_ftd_leg(torch, dev)
+        imaging = run_imaging_leg(torch, dev)
         precision = run_precision_leg(torch, dev)
         differentiation = run_diff_leg(torch, dev)
 
@@ -412,6 +413,7 @@ def run_ours(args, rank, world, dist):
         "e2e": e2e,
         "batched_uneven_flagged": batched,
         "raw_layout_fused_corner_turn": raw_layout,
+        "imaging_from_triangles": imaging,
         "precision_modes": precision,
         "adjoint_and_gain_gradient": differentiation,
         "clocks": clk,
@@ -493,6 +495,36 @@ def run_ftd_leg(torch, dev, n_ant=2048, n_chan=64, n_pol=2, K=1024, seed=6):
             "value": flops / (fused * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": fused,
             "separate_reorder_then_herk": {"value": flops / (sep * 1e-3) / 1e12,
                                            "ms_per_step": sep}}
+
+
+def run_imaging_leg(torch, dev, n_ant=2048, n_chan=64, n_pol=2, ng=2048, n_beam=4096, seed=8):
+    """Imaging from the packed triangles of 2048 antennas x 64 channels x 2
+    pols (FP32, 2.15 GB): pillbox gridding with the pols summed and a taper
+    fused, 2048^2 inverse FFTs (cuFFT), 4096 beam pixels per channel."""
+    from ftd_b200 import Correlator, tri_size
+    g = torch.Generator(device=dev).manual_seed(seed)
+    n_bl = tri_size(n_ant)
+    vis = torch.randn(n_chan, n_pol, n_bl, 2, device=dev, generator=g)
+    freq = 1.0e9 + 1.0e6 * torch.arange(n_chan, device=dev, dtype=torch.float64)
+    lam = 299792458.0 / 1.0e9
+    uv = ((torch.rand(n_bl, 2, device=dev, generator=g) - 0.5) * ng * lam).contiguous()
+    taper = torch.rand(ng, ng, device=dev, generator=g) * 0.8 + 0.2
+    pix = torch.randint(0, ng, (n_beam, 2), device=dev, generator=g, dtype=torch.int32)
+    beams = torch.empty(n_chan, n_beam, device=dev)
+    with Correlator(device=dev.index) as c:
+        def call():
+            c.image_beams(vis, beams, n_ant, n_chan, n_pol, ng, 1.0, uv, freq, taper=taper,
+                          beam_pixels=pix, n_beam=n_beam)
+        ms = _timed(torch, call, reps=5)
+        if c.device_status() != 0:
+            raise RuntimeError("device status after the imaging leg")
+    vis_bytes = n_chan * n_pol * n_bl * 8
+    return {"workload": f"imaging: {n_ant} antennas x {n_chan} channels x {n_pol} pols packed "
+                        f"triangles (FP32) -> {ng}^2 grids -> {n_beam} beams",
+            "ms_per_step": ms, "visibility_bytes": vis_bytes,
+            "visibility_read_gbs": vis_bytes / (ms * 1e-3) / 1e9,
+            "note": "gridding (pols summed, taper fused, FP32 atomics in L2) + cuFFT C2C "
+                    "inverse + beam extraction, per grid tile of the channels that fit in 64 MiB"}
 
 
 def _timed(torch, fn, reps=5, warm=2):

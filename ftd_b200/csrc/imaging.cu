@@ -30,56 +30,62 @@ namespace {
 
 constexpr double kLightSpeed = 299792458.0;
 
-// Row i and column j of packed lower-triangle index k = i(i+1)/2 + j (exact
-// for every k of a 32-bit row count).
+// Row i and column j of packed lower-triangle index k = i(i+1)/2 + j: a float
+// square-root estimate, corrected in integers (exact for every k).
 __device__ __forceinline__ void tri_row_col(int64_t k, int& i, int& j) {
-  int64_t r = int64_t((sqrt(8.0 * double(k) + 1.0) - 1.0) * 0.5);
+  int64_t r = int64_t((sqrtf(8.f * float(k) + 1.f) - 1.f) * 0.5f);
   while (r * (r + 1) / 2 > k) --r;
   while ((r + 1) * (r + 2) / 2 <= k) ++r;
   i = int(r);
   j = int(k - r * (r + 1) / 2);
 }
 
-// One thread per (channel of the tile, baseline): sum the n_pol visibilities,
-// then add them (times the taper weight of the cell) at the baseline's cell
-// and, for a cross-correlation, the conjugate at the mirrored cell.
+constexpr int kMaxTileChans = 64;  // channels of one grid tile (wavelengths in shared memory)
+
+// One thread per baseline, looping over the tile's channels: sum the n_pol
+// visibilities, then add them (times the taper weight of the cell) at the
+// baseline's cell and, for a cross-correlation, the conjugate at the
+// mirrored cell.  The baseline's (u, v) and its row / column are read and
+// decoded once per tile; the wavelengths sit in shared memory.
 __global__ void __launch_bounds__(256) grid_scatter_kernel(
     const float2* __restrict__ vis, const float2* __restrict__ uv, const double* __restrict__ freq,
     const float* __restrict__ taper, float2* __restrict__ grid, int64_t n_bl, int n_pol, int Ng,
     int f0, int nf, float cell) {
-  const int64_t total = int64_t(nf) * n_bl;
+  __shared__ double lambda[kMaxTileChans];
+  for (int f = threadIdx.x; f < nf; f += blockDim.x) lambda[f] = kLightSpeed / freq[f0 + f];
+  __syncthreads();
   const int64_t plane = int64_t(Ng) * Ng;
   const float half = 0.5f * float(Ng);
-  for (int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < total;
-       x += int64_t(gridDim.x) * blockDim.x) {
-    const int fl = int(x / n_bl);
-    const int64_t k = x - int64_t(fl) * n_bl;
-    const int f = f0 + fl;
-    const float2* vp = vis + int64_t(f) * n_pol * n_bl + k;
-    float2 v = __ldg(vp);
-    for (int p = 1; p < n_pol; ++p) {
-      const float2 w = __ldg(vp + int64_t(p) * n_bl);
-      v.x += w.x;
-      v.y += w.y;
-    }
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n_bl;
+       k += int64_t(gridDim.x) * blockDim.x) {
     const float2 b = __ldg(uv + k);
-    const double lambda = kLightSpeed / __ldg(freq + f);
-    const float ul = float(double(b.x) / lambda), vl = float(double(b.y) / lambda);
-    float2* g = grid + int64_t(fl) * plane;
-    const int iu = int(roundf(ul / cell + half)), iv = int(roundf(vl / cell + half));
-    if (iu >= 0 && iu < Ng && iv >= 0 && iv < Ng) {
-      const int64_t c = int64_t(iv) * Ng + iu;
-      const float wt = taper ? __ldg(taper + c) : 1.f;
-      atomicAdd(g + c, make_float2(v.x * wt, v.y * wt));
-    }
     int i, j;
     tri_row_col(k, i, j);
-    if (i != j) {
-      const int iuc = int(roundf(-ul / cell + half)), ivc = int(roundf(-vl / cell + half));
-      if (iuc >= 0 && iuc < Ng && ivc >= 0 && ivc < Ng) {
-        const int64_t c = int64_t(ivc) * Ng + iuc;
+    const bool cross = i != j;
+    for (int fl = 0; fl < nf; ++fl) {
+      const float2* vp = vis + int64_t(f0 + fl) * n_pol * n_bl + k;
+      float2 v = __ldg(vp);
+      for (int p = 1; p < n_pol; ++p) {
+        const float2 w = __ldg(vp + int64_t(p) * n_bl);
+        v.x += w.x;
+        v.y += w.y;
+      }
+      const double lam = lambda[fl];
+      const float ul = float(double(b.x) / lam), vl = float(double(b.y) / lam);
+      float2* g = grid + int64_t(fl) * plane;
+      const int iu = int(roundf(ul / cell + half)), iv = int(roundf(vl / cell + half));
+      if (iu >= 0 && iu < Ng && iv >= 0 && iv < Ng) {
+        const int64_t c = int64_t(iv) * Ng + iu;
         const float wt = taper ? __ldg(taper + c) : 1.f;
-        atomicAdd(g + c, make_float2(v.x * wt, -v.y * wt));
+        atomicAdd(g + c, make_float2(v.x * wt, v.y * wt));
+      }
+      if (cross) {
+        const int iuc = int(roundf(-ul / cell + half)), ivc = int(roundf(-vl / cell + half));
+        if (iuc >= 0 && iuc < Ng && ivc >= 0 && ivc < Ng) {
+          const int64_t c = int64_t(ivc) * Ng + iuc;
+          const float wt = taper ? __ldg(taper + c) : 1.f;
+          atomicAdd(g + c, make_float2(v.x * wt, -v.y * wt));
+        }
       }
     }
   }
@@ -131,7 +137,7 @@ extern "C" ftdx_status ftdx_image_beams(ftdx_handle h, const ftdx_imaging_config
   const int64_t n_bl = int64_t(c.n_ant) * (c.n_ant + 1) / 2;
   int tile = c.chan_tile;
   if (tile == 0) tile = int(std::max<int64_t>(1, (int64_t(64) << 20) / (plane * 8)));
-  tile = std::min(tile, c.n_chan);
+  tile = std::min(std::min(tile, c.n_chan), kMaxTileChans);
   if (!h->imaging) h->imaging = std::make_shared<ImagingState>();
   auto* st = static_cast<ImagingState*>(h->imaging.get());
   const size_t need = size_t(tile) * size_t(plane) * sizeof(float2);
@@ -155,8 +161,7 @@ extern "C" ftdx_status ftdx_image_beams(ftdx_handle h, const ftdx_imaging_config
     e = cudaMemsetAsync(st->grid, 0, size_t(nf) * size_t(plane) * sizeof(float2), s);
     if (e != cudaSuccess) return cuda_fail(h, e, "grid clear");
     {
-      const int64_t total = int64_t(nf) * n_bl;
-      const int64_t blocks = std::min<int64_t>((total + 255) / 256, int64_t(h->sm_count) * 32);
+      const int64_t blocks = std::min<int64_t>((n_bl + 255) / 256, int64_t(h->sm_count) * 32);
       grid_scatter_kernel<<<unsigned(std::max<int64_t>(blocks, 1)), 256, 0, s>>>(
           static_cast<const float2*>(vis), reinterpret_cast<const float2*>(c.baseline_uv_m),
           c.freq_hz, c.taper, st->grid, n_bl, c.n_pol, Ng, f0, nf, c.cell_size_rad);

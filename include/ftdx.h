@@ -206,7 +206,7 @@ FTDX_API ftdx_status ftdx_pipeline_sizes(ftdx_pipeline_t p, size_t* in_bytes, si
  * vis: device FP32 [n_chan][n_pol][n_bl][2]; beams: device FP32 [n_chan][n_beam].
  * output_stage: 0 = beams; 1 = the tapered UV grid and 2 = the image, both
  * [n_chan][Ng][Ng] complex64 written to grid_out (for checking; beams then
- * untouched).  The grid workspace holds chan_tile channels (0: as many as
+ * untouched).  The grid workspace holds chan_tile channels (at most 64; 0: as many as
  * fit in 64 MiB, so that the atomics stay in L2). */
 typedef struct ftdx_imaging_config {
   int n_ant, n_chan, n_pol, n_grid, n_beam;
