@@ -362,11 +362,12 @@ def run_ours(args, rank, world, dist):
     if not args.no_e2e:
         e2e = run_e2e(torch, args, dev, qc, N, K, B, flops, world, dist)
 
-    batched = precision = differentiation = raw_layout = imaging = None
+    batched = precision = differentiation = raw_layout = imaging = xengine = None
     if not args.no_extra:
         batched = run_batched_leg(torch, dev)
         raw_layout = run_ftd_leg(torch, dev)
         imaging = run_imaging_leg(torch, dev)
+        xengine = run_xengine_leg(torch, dev)
         precision = run_precision_leg(torch, dev)
         differentiation = run_diff_leg(torch, dev)
 
@@ -414,6 +415,7 @@ def run_ours(args, rank, world, dist):
         "batched_uneven_flagged": batched,
         "raw_layout_fused_corner_turn": raw_layout,
         "imaging_from_triangles": imaging,
+        "xengine_upper_triangle": xengine,
         "precision_modes": precision,
         "adjoint_and_gain_gradient": differentiation,
         "clocks": clk,
@@ -525,6 +527,24 @@ def run_imaging_leg(torch, dev, n_ant=2048, n_chan=64, n_pol=2, ng=2048, n_beam=
             "visibility_read_gbs": vis_bytes / (ms * 1e-3) / 1e9,
             "note": "gridding (pols summed, taper fused, FP32 atomics in L2) + cuFFT C2C "
                     "inverse + beam extraction, per grid tile of the channels that fit in 64 MiB"}
+
+
+def run_xengine_leg(torch, dev, n_ant=2048, K=1024, batch=128, seed=9):
+    """XEngine-compatible path: [batch][K][n_ant] two's-complement (4,4)b
+    blocks (2048 antennas x K=1024 x 128 = 268 MB) -> packed upper triangles
+    of C = M^H M (the XEngine's triangular format)."""
+    from ftd_b200 import Correlator, tri_size
+    g = torch.Generator(device=dev).manual_seed(seed)
+    p = torch.randint(0, 256, (batch * K * n_ant,), device=dev, dtype=torch.uint8, generator=g)
+    C = torch.empty(batch, tri_size(n_ant), 2, device=dev)
+    with Correlator(device=dev.index) as c:
+        ms = _timed(torch, lambda: c.xengine(p, C, n_ant, K, batch, mat_format=1), reps=10)
+        if c.device_status() != 0:
+            raise RuntimeError("device status after the XEngine leg")
+    return {"workload": f"XEngine: {batch} blocks of [K={K}][{n_ant}] two's-complement (4,4)b "
+                        f"-> packed upper triangles (FP32)",
+            "value": herk_flops(n_ant, K, batch) / (ms * 1e-3) / 1e12, "unit": UNIT,
+            "ms_per_step": ms}
 
 
 def _timed(torch, fn, reps=5, warm=2):

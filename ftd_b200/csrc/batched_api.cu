@@ -148,7 +148,7 @@ ftdx_status launch_v(ftdx_handle h, const VCall& c, const Strategy& strat, cudaS
   args.num_tiles = p->num_tiles;
   args.out_fp16 = (c.output == FTDX_OUT_FP16) ? 1 : 0;
   args.bulk_store = strat.store_mode == 1 ? 1 : 0;
-  args.reserved = 0;
+  args.out_format = 0;
   args.out = nullptr;
   args.alpha = c.alpha;
   args.beta = c.beta;

@@ -66,7 +66,8 @@ __global__ void __launch_bounds__(256) ftd_tacp_to_planes_kernel(const uint8_t* 
       const int64_t s = s0 + 4 * sg;
       uint32_t v = 0;
       if (k < g.K) {
-        const uint8_t* src = raw + (int64_t(k) * g.n_ti + ti) * S + s;
+        const uint8_t* src = raw + (g.t_stride ? int64_t(k) * g.t_stride + ti * g.z_stride
+                                               : (int64_t(k) * g.n_ti + ti) * S) + s;
         if (wide && s + 4 <= S) {
           v = __ldg(reinterpret_cast<const uint32_t*>(src));
         } else {
@@ -115,8 +116,13 @@ __global__ void __launch_bounds__(256) ftd_tacp_to_planes_kernel(const uint8_t* 
 #pragma unroll
   for (int x = 0; x < 8; ++x) q[x] = *reinterpret_cast<const uint32_t*>(src + 4 * x);
   uint32_t re[8], im[8];
+  if (g.twos) {
 #pragma unroll
-  for (int x = 0; x < 8; ++x) qc4_to_e4m3(q[x], re[x], im[x]);
+    for (int x = 0; x < 8; ++x) tc4_to_e4m3(q[x], re[x], im[x]);
+  } else {
+#pragma unroll
+    for (int x = 0; x < 8; ++x) qc4_to_e4m3(q[x], re[x], im[x]);
+  }
   const int64_t plane = g.rows * int64_t(g.Kp);
   uint8_t* dst = z + row * g.Kp + col0 + kb;
   put32(dst, re, nbytes);

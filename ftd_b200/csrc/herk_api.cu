@@ -27,6 +27,8 @@ struct HerkCall {
   ftdx_compute compute = FTDX_COMPUTE_FP8;
   void* comp = nullptr;  // Kahan compensation buffer (ftdx_herk_kahan)
   const ftdx_ftd_desc* ftd = nullptr;  // raw packet-ordered input (ftdx_herk_ftd)
+  bool xeng = false;   // XEngine payload: [batch][K][N] (4,4)b two's complement (ftdx_xengine)
+  int out_format = 0;  // HerkArgs::out_format
 };
 
 bool is_split(const HerkCall& c) { return c.compute == FTDX_COMPUTE_FP8_SPLIT; }
@@ -161,9 +163,16 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   cudaError_t e;
   {
     ScopedTimer tm(h, s, 1);
-    if (c.ftd) {
+    if (c.xeng) {
+      FtdGeom g{};
+      g.n_ant = c.N, g.n_chan = 1, g.n_pol = 1, g.n_ti = c.batch;
+      g.K = c.K, g.n_time = c.K, g.pol_sum = 0, g.Kp = int(Kp), g.rows = rows;
+      g.neg_plane = pair ? 1 : 0;
+      g.t_stride = c.N, g.z_stride = int64_t(c.K) * c.N, g.twos = 1;
+      e = launch_ftd_to_planes(static_cast<const uint8_t*>(c.A), h->z, g, 0, h->sm_count, s);
+    } else if (c.ftd) {
       const ftdx_ftd_desc& d = *c.ftd;
-      FtdGeom g;
+      FtdGeom g{};
       g.n_ant = d.n_ant, g.n_chan = d.n_chan, g.n_pol = d.n_pol, g.n_ti = d.n_time_inner;
       g.K = d.n_time / d.n_time_inner;
       g.n_time = d.n_time;
@@ -195,7 +204,7 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   args.num_tiles = plan->num_tiles;
   args.out_fp16 = (c.output == FTDX_OUT_FP16) ? 1 : 0;
   args.bulk_store = strat.store_mode == 1 ? 1 : 0;
-  args.reserved = 0;
+  args.out_format = c.out_format;
   args.out = c.C;
   args.alpha = c.alpha;
   args.beta = c.beta;
@@ -622,6 +631,28 @@ long long ftdx_strided_batch_gemm(ftdx_handle h, const void* A, const void* B, v
   uint32_t bits = 0;
   if (ftdx_device_status(h, stream, &bits) != FTDX_OK) return -1;
   return 8LL * m * n * k * batch;
+}
+
+ftdx_status ftdx_xengine(ftdx_handle h, const void* payload, void* out, int n_ant, int K,
+                         int batch, int mat_format, ftdx_output output, void* stream) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  if (mat_format != 0 && mat_format != 1)
+    return fail(h, FTDX_ERR_INVALID_ARG, "xengine: mat_format must be 0 (full) or 1 (packed upper)");
+  if (batch > 65535)
+    return fail(h, FTDX_ERR_INVALID_ARG, "xengine: at most 65535 matrices per call");
+  HerkCall c{payload, out, n_ant, K, batch, FTDX_IN_INT4, output, 1.f, 0.f};
+  c.xeng = true;
+  c.out_format = mat_format == 1 ? 1 : 2;
+  ftdx_status st = validate(h, c, FTDX_COMPUTE_FP8, FTDX_FORMAT_PACKED_TRIANGLE);
+  if (st != FTDX_OK) return st;
+  if (round_up(K, kStageK) > 64 * 65535)
+    return fail(h, FTDX_ERR_INVALID_ARG, "xengine: K too large");
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+  // the XEngine formats are written by the single-CTA kernel's direct stores
+  Strategy strat = h->default_strategy;
+  strat.store_mode = 0;
+  return launch_all(h, c, strat, static_cast<cudaStream_t>(stream));
 }
 
 ftdx_status ftdx_herk_kahan(ftdx_handle h, const void* A, void* sum, void* comp, int N, int K,

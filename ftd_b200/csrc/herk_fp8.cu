@@ -197,6 +197,30 @@ template <> struct Complex2<__half> { using type = __half2; };
 // needs a bounds check or the Im(diagonal) = 0 rule.  The fast paths cover
 // the plain (C = A A^H) and scaled (alpha, per-channel scale) stores; beta and
 // Kahan read the old value first.
+// XEngine output formats (HerkArgs::out_format 1 / 2): element (i, j <= i)
+// of R = sum_t v_i conj(v_j) is C(j, i) of C = sum_t conj(v_r) v_c, stored in
+// the packed upper triangle (format 1) or the full matrix with its mirror
+// C(i, j) = conj(R_ij) (format 2).  ob: this channel's output.
+template <typename Out2>
+__device__ __forceinline__ void store_chunk_xengine(Out2* ob, int i0, int j, int n, float sc,
+                                                    int format, const uint32_t (&re)[32],
+                                                    const uint32_t (&im)[32]) {
+#pragma unroll 4
+  for (int m = 0; m < 32; ++m) {
+    const int i = i0 + m;
+    if (i < n && j <= i) {
+      const float vr = __uint_as_float(re[m]) * sc;
+      const float vi = (i == j) ? 0.f : __uint_as_float(im[m]) * sc;
+      if (format == 1) {
+        put(ob + (int64_t(j) * n - int64_t(j) * (j - 1) / 2 + (i - j)), vr, vi);
+      } else {
+        put(ob + int64_t(j) * n + i, vr, vi);
+        if (i != j) put(ob + int64_t(i) * n + j, vr, -vi);
+      }
+    }
+  }
+}
+
 // Sector-aligned variant of the fast store for FP32 output, used when a whole
 // 32-row x 128-column block of the tile (the four warps of one epilogue half)
 // lies below n and strictly below the diagonal.  A row segment of 32
@@ -352,8 +376,10 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
         const TileDesc td = args.tiles[t];
         const ChanDesc cd = args.chans[td.ch];
-        const int32_t rowJ = int32_t(cd.row0 + int64_t(td.tj) * kTile);
-        const int32_t rowI = int32_t(cd.row0 + int64_t(td.ti) * kTile);
+        // the packed-upper output format swaps the blocks: TMEM lane = larger index
+        const bool swap = args.out_format == 1;
+        const int32_t rowJ = int32_t(cd.row0 + int64_t(swap ? td.ti : td.tj) * kTile);
+        const int32_t rowI = int32_t(cd.row0 + int64_t(swap ? td.tj : td.ti) * kTile);
         const bool diag = td.ti == td.tj;  // i block == j block: load it once
         const int nkb = cd.kblocks * args.nseg;
         for (int kb = 0; kb < nkb; ++kb) {
@@ -537,6 +563,46 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
           }
           named_bar_sync(bar_id, 128);
         }
+      } else if (args.out_format == 1) {
+        // Packed upper triangle, row-major (the XEngine's format): the producer
+        // swapped the blocks, so TMEM lane = column c (the i block) and TMEM
+        // column = row r (the j block), and the accumulator holds
+        // sum_t v_r conj(v_c) = conj(C(r, c)).  A warp stores 32 consecutive
+        // c of one row r.
+        const float sc = args.alpha * (args.chan_scale ? args.chan_scale[td.ch] : 1.f);
+        const int cw = ib + q * 32;  // this warp's first column
+        const int c = cw + lane;
+#pragma unroll 1
+        for (int cc = 0; cc < kChunks; ++cc) {
+          const int ch = half * kChunks + cc;
+          const int r0 = j0 + 32 * ch;
+          if (r0 > cw + 31 || cw >= n) continue;  // warp-uniform: nothing to store
+          uint32_t re[32], im[32];
+          __syncwarp();
+          tmem_ld_32x32b_x32(tb + 32u * ch, re);
+          tmem_ld_32x32b_x32(tb + uint32_t(kTile) + 32u * ch, im);
+          tmem_wait_ld();
+          if (r0 + 31 < cw && cw + 31 < n) {
+            // every element strictly above the diagonal and inside n: row
+            // r + 1 starts n - r - 1 elements after element (r, c)'s row start
+            Out2* p = outc + (int64_t(r0) * n - int64_t(r0) * (r0 - 1) / 2 + (c - r0));
+#pragma unroll
+            for (int m = 0; m < 32; ++m) {
+              put(p, __uint_as_float(re[m]) * sc, -__uint_as_float(im[m]) * sc);
+              p += n - (r0 + m) - 1;
+            }
+            continue;
+          }
+#pragma unroll 4
+          for (int m = 0; m < 32; ++m) {
+            const int r = r0 + m;
+            if (c < n && r <= c) {
+              const float vr = __uint_as_float(re[m]) * sc;
+              const float vi = (r == c) ? 0.f : -__uint_as_float(im[m]) * sc;
+              put(outc + (int64_t(r) * n - int64_t(r) * (r - 1) / 2 + (c - r)), vr, vi);
+            }
+          }
+        }
       } else {
         const float sc = args.alpha * (args.chan_scale ? args.chan_scale[td.ch] : 1.f);
 #pragma unroll 1
@@ -549,6 +615,11 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
           tmem_ld_32x32b_x32(tb + 32u * c, re);
           tmem_ld_32x32b_x32(tb + uint32_t(kTile) + 32u * c, im);
           tmem_wait_ld();
+          if (args.out_format != 0) {
+            Out2* ob = args.out_format == 2 ? out + int64_t(td.ch) * n * n : outc;
+            store_chunk_xengine(ob, i0, j, n, sc, args.out_format, re, im);
+            continue;
+          }
           // element (i, j) lives at i(i+1)/2 + j; row i+1 starts i+1 later
           const int64_t e0 = int64_t(i0) * (i0 + 1) / 2 + j;
           if constexpr (sizeof(Out2) == 8) {

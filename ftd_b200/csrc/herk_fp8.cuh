@@ -78,7 +78,13 @@ struct HerkArgs {
   int32_t num_tiles;
   int32_t out_fp16;
   int32_t bulk_store;  // 1: interior tiles leave through shared memory + bulk copies
-  int32_t reserved;
+  // 0: packed lower triangle (element (i, j <= i) at i(i+1)/2 + j);
+  // 1: packed upper triangle, row-major (element (r, c >= r) at
+  //    r*n - r(r-1)/2 + c - r, holding sum_t conj(v_r) v_c: the XEngine's
+  //    triangular format); 2: full n x n matrix of sum_t conj(v_r) v_c (the
+  //    XEngine's Hermitian format).  Formats 1 and 2: single-CTA kernel,
+  //    direct stores, beta = 0, no Kahan.
+  int32_t out_format;
   void* out;
   float alpha;
   float beta;
@@ -115,6 +121,10 @@ struct FtdGeom {
   int Kp;                          // padded row length (multiple of kStageK)
   int64_t rows;                    // plane rows = n_ant * batches
   int neg_plane;                   // also write plane 2 = -Re
+  // layout 0 source offset of (sample k, block z, slice byte s) =
+  //   k*t_stride + z*z_stride + s  (0, 0: the [t][ant][chan][pol] strides)
+  int64_t t_stride, z_stride;
+  int twos;                        // (4,4)b two's complement bytes, low nibble Re
 };
 // layout 0: [t][ant][chan][pol], t = k*n_ti + ti; 1: [chan][pol][ant][t], t = ti*K + k.
 cudaError_t launch_ftd_to_planes(const uint8_t* raw, uint8_t* z, const FtdGeom& g, int layout,

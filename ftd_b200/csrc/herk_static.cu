@@ -153,7 +153,7 @@ extern "C" ftdx_status ftdx_herk_static(const void* A, void* C, int N, int K, in
   args.num_tiles = int(ntiles);
   args.out_fp16 = 0;
   args.bulk_store = 0;
-  args.reserved = 0;
+  args.out_format = 0;
   args.out = C;
   args.alpha = 1.f;
   args.beta = 0.f;

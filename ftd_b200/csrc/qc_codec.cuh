@@ -21,4 +21,23 @@ __device__ __forceinline__ void qc4_to_e4m3(uint32_t w, uint32_t& re, uint32_t& 
   im = __byte_perm(kLo, kHi, si) | ((w << 4) & 0x80808080u);
 }
 
+// Four (4,4)b two's-complement bytes (low nibble Re, high nibble Im, each in
+// [-8, 7]: the XEngine's packet format, promote_data.cuh:66-67) -> E4M3 bytes
+// of the Re and of the Im parts.  Nibbles 0..7 are 0..7; 8..15 are -8..-1,
+// E4M3 codes D0 CE CC CA C8 C4 C0 B8.
+__device__ __forceinline__ uint32_t tc_nibbles_to_e4m3(uint32_t nib) {  // 4 bytes of 0..15
+  constexpr uint32_t kP0 = 0x44403800u, kP1 = 0x4E4C4A48u;
+  constexpr uint32_t kN0 = 0xCACCCED0u, kN1 = 0xB8C0C4C8u;
+  const uint32_t m = nib & 0x07070707u;
+  uint32_t sel = m | (m >> 4);
+  sel = (sel & 0xFFu) | ((sel >> 8) & 0xFF00u);
+  const uint32_t pos = __byte_perm(kP0, kP1, sel), neg = __byte_perm(kN0, kN1, sel);
+  const uint32_t mask = ((nib >> 3) & 0x01010101u) * 0xFFu;
+  return (pos & ~mask) | (neg & mask);
+}
+__device__ __forceinline__ void tc4_to_e4m3(uint32_t w, uint32_t& re, uint32_t& im) {
+  re = tc_nibbles_to_e4m3(w & 0x0F0F0F0Fu);
+  im = tc_nibbles_to_e4m3((w >> 4) & 0x0F0F0F0Fu);
+}
+
 }  // namespace ftdx

@@ -144,6 +144,15 @@ class Correlator:
                                       _ptr(grid_out), _stream(stream))
         check(self._h, st, "ftdx_image_beams")
 
+    def xengine(self, payload, out, n_ant: int, K: int, batch: int, mat_format: int = 1,
+                output: int = OUT_FP32, stream=None) -> None:
+        """XEngine correlation of [batch][K][n_ant] two's-complement (4,4)b
+        payload blocks: packed upper triangles (mat_format 1) or full matrices
+        (0) of C = M^H M (ftdx_xengine)."""
+        st = self._L.ftdx_xengine(self._h, _ptr(payload), _ptr(out), n_ant, K, batch, mat_format,
+                                  output, _stream(stream))
+        check(self._h, st, "ftdx_xengine")
+
     def strided_batch_gemm(self, A, B, C, m: int, n: int, k: int, trans_a: int, trans_b: int,
                            batch: int, data_type: int, stream=None) -> int:
         """quda::stridedBatchGEMMCutlass's HERK branch: flop count, or -1."""

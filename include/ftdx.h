@@ -224,6 +224,19 @@ FTDX_API ftdx_status ftdx_image_beams(ftdx_handle h, const ftdx_imaging_config* 
                                       const void* vis, float* beams, void* grid_out,
                                       void* stream);
 
+/* The XEngine's correlation (ggp::XEngine::compute, lib/xengine.cpp:108-178:
+ * promoteData, the strided-batch GEMM C = M^H M, triangulateFromHerm), with the
+ * conventions its test checks (tests/xengine_test.cpp:213-321): each of the
+ * batch payload blocks is M [K][n_ant] of (4,4)b two's-complement bytes (low
+ * nibble Re, high nibble Im, each in [-8, 7]; promote_data.cuh:66-67), and
+ * C(r, c) = sum_t conj(M(t, r)) M(t, c) is written per block as
+ *   mat_format 1 (QUDA_XENGINE_MAT_TRI): the packed upper triangle, row-major
+ *     (element (r, c >= r) at r*n - r(r-1)/2 + c - r);
+ *   mat_format 0 (QUDA_XENGINE_MAT_HERM): the full n_ant x n_ant matrix.
+ * Exact (integer sums) like the rest; FP32 or FP16 output. */
+FTDX_API ftdx_status ftdx_xengine(ftdx_handle h, const void* payload, void* out, int n_ant, int K,
+                                  int batch, int mat_format, ftdx_output output, void* stream);
+
 /* The HERK branch of quda::stridedBatchGEMMCutlass (lib/cutlass_interface.cu:316-381),
  * the XEngine's BLAS entry: when A == B, trans_a is the conjugate transpose
  * (QUDA_BLAS_OP_C = 2), trans_b none (QUDA_BLAS_OP_N = 0), m == n and data_type

@@ -371,3 +371,26 @@ def beam_intensity(image: np.ndarray, pixels: np.ndarray) -> np.ndarray:
         if 0 <= r < ng and 0 <= c < ng:
             out[:, b] = np.abs(image[:, r, c]) ** 2 / (ng * ng)
     return out
+
+
+# ----------------------------------------------------------------- XEngine
+def decode_twos(b: np.ndarray):
+    """(4,4)b two's complement bytes -> (re, im) int: low nibble Re, high nibble
+    Im, each sign-extended (promote_to_float, tests/xengine_test.cpp:162-167)."""
+    b = np.asarray(b, dtype=np.uint8)
+    re = ((b & 0x0F).astype(np.int16) << 12).astype(np.int16) >> 12
+    im = (b.astype(np.int16) << 8).astype(np.int16) >> 12
+    return re.astype(np.int64), im.astype(np.int64)
+
+
+def xengine(payload: np.ndarray, n_ant: int, K: int, batch: int, mat_format: int) -> np.ndarray:
+    """verifyXEngine's reference (tests/xengine_test.cpp:242-310): per block
+    M [K][n_ant], C = M^H M; mat_format 1 = upper triangle packed row-major,
+    0 = full matrix.  Exact (float64 of integer sums)."""
+    re, im = decode_twos(np.asarray(payload).reshape(batch, K, n_ant))
+    M = re.astype(np.float64) + 1j * im.astype(np.float64)
+    C = np.einsum("btr,btc->brc", np.conj(M), M)
+    if mat_format == 0:
+        return C
+    r, c = np.triu_indices(n_ant)
+    return C[:, r, c]

@@ -199,3 +199,29 @@ def test_imaging_beams_and_fft_definition():
 def test_imaging_roundf_halves_away_from_zero():
     x = np.array([0.5, 1.5, 2.5, -0.5, -1.5, 0.49999997], dtype=np.float32)
     assert list(oracle._roundf(x)) == [1, 2, 3, -1, -2, 0]
+
+
+# ------------------------------------------------ XEngine conventions
+def test_xengine_twos_complement_decode():
+    # promote_to_float (tests/xengine_test.cpp:162-167): low nibble Re, high
+    # nibble Im, each a sign-extended 4-bit two's complement value
+    b = np.arange(256, dtype=np.uint8)
+    re, im = oracle.decode_twos(b)
+    for x in range(256):
+        lo, hi = x & 15, x >> 4
+        assert re[x] == (lo - 16 if lo >= 8 else lo) and im[x] == (hi - 16 if hi >= 8 else hi)
+
+
+def test_xengine_upper_packing_and_hermitian():
+    rng = np.random.default_rng(2)
+    n, K, B = 5, 7, 2
+    p = rng.integers(0, 256, size=B * K * n, dtype=np.uint8)
+    full = oracle.xengine(p, n, K, B, 0)
+    tri = oracle.xengine(p, n, K, B, 1)
+    assert np.allclose(full, np.conj(np.transpose(full, (0, 2, 1))))
+    k = 0
+    for r in range(n):          # row-major upper: (r, c >= r) at r*n - r(r-1)/2 + c - r
+        for c in range(r, n):
+            assert k == r * n - r * (r - 1) // 2 + c - r
+            assert tri[0, k] == full[0, r, c]
+            k += 1
