@@ -55,6 +55,9 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-peak", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the extra workload legs")
+    p.add_argument("--leg", default=None, choices=["nvfp4", "raw", "imaging", "xengine"],
+                   help="run one extra workload alone and print its JSON (profiling cases); "
+                        "nvfp4 uses --inputs/--channels/--k")
     p.add_argument("--strategy", default=None,
                    help="STORE_MODE,GRID: fix the correlator strategy instead of autotuning "
                         "(0 direct stores, 1 bulk stores, 2 CTA-pair kernel)")
@@ -689,8 +692,44 @@ def run_e2e(torch, args, dev, qc_dev, N, K, B, flops, world, dist):
                     "host wall time"}
 
 
+def run_nvfp4_case(torch, dev, N, K, B, reps=5, seed=1):
+    """NVFP4 correlation of seeded Gaussian FP32 complex voltages [B][N][K]:
+    reps calls, the whole FP4 path (amax, quantisation, row power, correlator)
+    timed with CUDA events."""
+    from ftd_b200 import Correlator, tri_size
+    from ftd_b200._lib import COMPUTE_FP4, IN_FP32, OUT_FP32
+    g = torch.Generator(device=dev).manual_seed(seed)
+    A = torch.randn(B, N, K, 2, device=dev, generator=g)
+    C = torch.empty(B, tri_size(N), 2, device=dev)
+    with Correlator(device=dev.index) as c:
+        ms = _timed(torch, lambda: c.herk(A, C, N, K, B, input=IN_FP32, compute=COMPUTE_FP4,
+                                          output=OUT_FP32, tune=False), reps=reps)
+        if c.device_status() != 0:
+            raise RuntimeError("device status after the NVFP4 case")
+    return {"workload": f"NVFP4: {N} inputs x {B} channels x K={K}, Gaussian FP32 complex",
+            "value": herk_flops(N, K, B) / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms}
+
+
+def run_leg(args):
+    import torch
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    if args.leg == "nvfp4":
+        out = run_nvfp4_case(torch, dev, args.inputs, args.k, args.channels)
+    elif args.leg == "raw":
+        out = run_ftd_leg(torch, dev)
+    elif args.leg == "imaging":
+        out = run_imaging_leg(torch, dev)
+    else:
+        out = run_xengine_leg(torch, dev)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.leg:
+        return run_leg(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
