@@ -259,6 +259,7 @@ def run_ours(args, rank, world, dist):
     import torch
     from ftd_b200 import Correlator, tri_size
     from ftd_b200._lib import IN_INT4, OUT_FP32
+    from ftd_b200.shard import max_over_ranks
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -326,11 +327,7 @@ def run_ours(args, rank, world, dist):
     if corr.device_status() != 0:
         raise RuntimeError("device wait timed out in the timed region")
 
-    ms_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, dist, dev)  # the slowest rank sets the step time
     value = flops * world / (ms_max * 1e-3) / 1e12
 
     # --- plain per-channel path: the same kernels launched per channel, one
@@ -668,6 +665,7 @@ def run_e2e(torch, args, dev, qc_dev, N, K, B, flops, world, dist):
     D2H overlaps payload p+1's H2D and correlation.  Host wall time of the
     blocking call, divided by the payloads it carried."""
     from ftd_b200 import Correlator, Pipeline, tri_size
+    from ftd_b200.shard import max_over_ranks
     P = tri_size(N)
     h_in = torch.empty(B * N * K, dtype=torch.uint8, pin_memory=True)
     h_in.copy_(qc_dev.reshape(-1).cpu())
@@ -680,10 +678,7 @@ def run_e2e(torch, args, dev, qc_dev, N, K, B, flops, world, dist):
         t0 = time.perf_counter()
         pipe.correlate([h_out[i % 2] for i in range(steps)], [h_in] * steps)
         ms = (time.perf_counter() - t0) * 1e3 / steps
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, dev)
     return {"value": flops * world / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms,
             "h2d_bytes_per_step": int(B * N * K), "d2h_bytes_per_step": int(B * P * 8),
             "steps": steps,
