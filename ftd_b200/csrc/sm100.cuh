@@ -65,22 +65,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity.  Returns false on
-// timeout or when *abort_flag (shared memory) becomes non-zero.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
-                                          volatile int* abort_flag) {
+// Bounded wait for the phase with the given parity.  Returns false after
+// limit_ns nanoseconds or when *abort_flag (shared memory) becomes non-zero.
+__device__ __forceinline__ bool mbar_wait_limit(uint32_t bar, uint32_t parity,
+                                                volatile int* abort_flag, uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
   for (uint32_t it = 1;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((it & 63u) == 0) {
       if (*abort_flag) return false;
-      if (globaltimer_ns() - t0 > FTDX_WAIT_NS) {
+      if (globaltimer_ns() - t0 > limit_ns) {
         *abort_flag = 1;
         return false;
       }
     }
   }
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
+                                          volatile int* abort_flag) {
+  return mbar_wait_limit(bar, parity, abort_flag, FTDX_WAIT_NS);
 }
 
 // ---------------------------------------------------------------- TMA

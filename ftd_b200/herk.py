@@ -144,6 +144,12 @@ class Correlator:
                                       _ptr(grid_out), _stream(stream))
         check(self._h, st, "ftdx_image_beams")
 
+    def wait_selftest(self, timeout_ms: int = 50, stream=None) -> None:
+        """Make one bounded device wait run out (ftdx_wait_selftest); the next
+        device_status() reports the timeout."""
+        check(self._h, self._L.ftdx_wait_selftest(self._h, timeout_ms, _stream(stream)),
+              "ftdx_wait_selftest")
+
     def xengine(self, payload, out, n_ant: int, K: int, batch: int, mat_format: int = 1,
                 output: int = OUT_FP32, stream=None) -> None:
         """XEngine correlation of [batch][K][n_ant] two's-complement (4,4)b

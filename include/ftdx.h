@@ -224,6 +224,13 @@ FTDX_API ftdx_status ftdx_image_beams(ftdx_handle h, const ftdx_imaging_config* 
                                       const void* vis, float* beams, void* grid_out,
                                       void* stream);
 
+/* Failure-path self-test of the bounded device waits (no counterpart in the
+ * reference): one kernel waits, for timeout_ms (1..2000), on an mbarrier that
+ * nothing arrives on, gives up and records the timeout in the status word;
+ * ftdx_device_status then returns FTDX_ERR_TIMEOUT and the handle stays
+ * usable.  Nothing traps or faults. */
+FTDX_API ftdx_status ftdx_wait_selftest(ftdx_handle h, int timeout_ms, void* stream);
+
 /* The XEngine's correlation (ggp::XEngine::compute, lib/xengine.cpp:108-178:
  * promoteData, the strided-batch GEMM C = M^H M, triangulateFromHerm), with the
  * conventions its test checks (tests/xengine_test.cpp:213-321): each of the
