@@ -102,6 +102,8 @@ PROTOTYPES = {
     "ftdx_set_graph_mode": (_i, [_vp, _i]),
     "ftdx_graph_count": (_i, [_vp]),
     "ftdx_set_strategy": (_i, [_vp, _i, _i]),
+    "ftdx_set_split_k": (_i, [_vp, _i]),
+    "ftdx_tuned_split_k": (_i, [_vp, _i, _i, _i, _i, _i]),
     "ftdx_herk_static": (_i, [_vp, _vp, _i, _i, _i, _vp, ctypes.POINTER(ctypes.c_uint32),
                               ctypes.POINTER(ctypes.c_size_t)]),
     "ftdx_profile_read": (_i, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i),

@@ -217,7 +217,8 @@ extern "C" ftdx_status ftdx_herk_batched_v(ftdx_handle h, const ftdx_channel_des
   }
   if (h->graph_mode && !capturing) {
     const GraphKey gk{reinterpret_cast<const void*>(call.fp), nullptr, -1, kp, n_chans,
-                      int(FTDX_IN_INT4), int(output), alpha, beta, strat.store_mode, strat.grid};
+                      int(FTDX_IN_INT4), int(output), alpha, beta, strat.store_mode, strat.grid,
+                      1};
     return graph_launch(
         h, gk,
         [&](cudaStream_t ss) {

@@ -33,8 +33,9 @@ struct Strategy {
   // 2: CTA-pair kernel (256 x 128 tiles on two SMs, direct stores)
   int store_mode = 0;
   int grid = 0;        // persistent CTAs (0: one per SM); -1: one CTA per tile (not persistent)
+  int splits = 1;      // split-K: K is cut into this many ranges, partials summed afterwards
   bool operator==(const Strategy& o) const {
-    return store_mode == o.store_mode && grid == o.grid;
+    return store_mode == o.store_mode && grid == o.grid && splits == o.splits;
   }
 };
 
@@ -58,11 +59,11 @@ struct GraphKey {
   void* c;
   int n, k, batch, input, output;
   float alpha, beta;
-  int store_mode, grid;
+  int store_mode, grid, splits;
   bool operator==(const GraphKey& o) const {
     return a == o.a && c == o.c && n == o.n && k == o.k && batch == o.batch &&
            input == o.input && output == o.output && alpha == o.alpha && beta == o.beta &&
-           store_mode == o.store_mode && grid == o.grid;
+           store_mode == o.store_mode && grid == o.grid && splits == o.splits;
   }
 };
 struct GraphEntry {
@@ -87,6 +88,9 @@ struct ftdx_context {
   uint8_t* aux = nullptr;
   size_t aux_cap = 0;
   uint32_t* d_status = nullptr;
+  // split-K partial triangles (grown on demand)
+  uint8_t* split_ws = nullptr;
+  size_t split_ws_cap = 0;
   std::map<std::tuple<int, int, int>, std::unique_ptr<ftdx::Plan>> plans;  // (N, kblocks, batch)
   std::map<uint64_t, std::shared_ptr<void>> vplans;  // batched-call plans by fingerprint
   // strategy of untuned calls (ftdx_set_strategy)
@@ -122,7 +126,8 @@ ftdx_status ensure_workspace(ftdx_handle h, size_t bytes, cudaStream_t s);
 ftdx_status ensure_aux(ftdx_handle h, size_t bytes, cudaStream_t s);
 // pair: tiles of the CTA-pair kernel (tj over 256 inputs, ti over 128)
 ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
-                     const Plan** out, bool pair = false);
+                     const Plan** out, bool pair = false, int splits = 1);
+ftdx_status ensure_split_ws(ftdx_handle h, size_t bytes, cudaStream_t s);
 ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t Kp,
                               CUtensorMap* tm, int box_rows = kTile, int nplanes = 2);
 // Even number of CTAs of the pair kernel that can be resident at once.

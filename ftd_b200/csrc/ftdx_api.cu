@@ -86,6 +86,27 @@ ftdx_status ensure_workspace(ftdx_handle h, size_t bytes, cudaStream_t s) {
   return FTDX_OK;
 }
 
+ftdx_status ensure_split_ws(ftdx_handle h, size_t bytes, cudaStream_t s) {
+  if (bytes <= h->split_ws_cap) return FTDX_OK;
+  if (stream_capturing(s))
+    return fail(h, FTDX_ERR_CAPACITY, "split-K workspace needed while capturing; call once first");
+  if (h->split_ws) {
+    cudaDeviceSynchronize();
+    cudaFree(h->split_ws);
+    h->split_ws = nullptr;
+    h->split_ws_cap = 0;
+    release_graphs(h);
+  }
+  cudaError_t e = cudaMalloc(&h->split_ws, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(h, FTDX_ERR_ALLOC, "cudaMalloc(%zu) for split-K partials: %s", bytes,
+                cudaGetErrorString(e));
+  }
+  h->split_ws_cap = bytes;
+  return FTDX_OK;
+}
+
 ftdx_status ensure_aux(ftdx_handle h, size_t bytes, cudaStream_t s) {
   if (bytes <= h->aux_cap) return FTDX_OK;
   if (stream_capturing(s))
@@ -110,9 +131,10 @@ ftdx_status ensure_aux(ftdx_handle h, size_t bytes, cudaStream_t s) {
 // Lower-triangle tile list for `batch` channels of N inputs, channel-major so
 // that concurrently running CTAs share a channel's operand in L2.
 ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
-                     const Plan** out, bool pair) {
-  // kblocks < 2^23 (K <= 2^30), so pair plans never share a key with others
-  auto key = std::make_tuple(N, pair ? kblocks + (1 << 24) : kblocks, batch);
+                     const Plan** out, bool pair, int splits) {
+  // kblocks < 2^23 (K <= 2^30) and splits <= 32, so pair and split-K plans
+  // never share a key with others
+  auto key = std::make_tuple(N, kblocks + (pair ? (1 << 24) : 0) + ((splits - 1) << 25), batch);
   auto it = h->plans.find(key);
   if (it != h->plans.end()) {
     *out = it->second.get();
@@ -123,18 +145,26 @@ ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t 
                 "tile plan for N=%d batch=%d built while capturing; call ftdx_init_herk first", N,
                 batch);
   const int nb = (N + kTile - 1) / kTile;
-  std::vector<ChanDesc> chans(batch);
+  // split-K: channel entry c*splits + s covers k-blocks [kb0, kb0 + kblocks) of
+  // channel c and writes partial triangle c*splits + s
+  std::vector<ChanDesc> chans(size_t(batch) * splits);
   std::vector<TileDesc> tiles;
-  tiles.reserve(size_t(batch) * nb * (nb + 1) / 2);
+  tiles.reserve(size_t(batch) * splits * nb * (nb + 1) / 2);
   for (int c = 0; c < batch; ++c) {
-    chans[c].n = N;
-    chans[c].kblocks = kblocks;
-    chans[c].row0 = int64_t(c) * N;
-    chans[c].out0 = int64_t(c) * (int64_t(N) * (N + 1) / 2);
-    chans[c].out_ptr = 0;
-    for (int ti = 0; ti < nb; ++ti)
-      for (int tj = 0; tj <= (pair ? ti / 2 : ti); ++tj)
-        tiles.push_back(TileDesc{c, uint16_t(ti), uint16_t(tj)});
+    for (int sp = 0; sp < splits; ++sp) {
+      const int vc = c * splits + sp;
+      const int kb_lo = int(int64_t(sp) * kblocks / splits);
+      const int kb_hi = int(int64_t(sp + 1) * kblocks / splits);
+      chans[vc].n = N;
+      chans[vc].kblocks = kb_hi - kb_lo;
+      chans[vc].kb0 = kb_lo;
+      chans[vc].row0 = int64_t(c) * N;
+      chans[vc].out0 = int64_t(vc) * (int64_t(N) * (N + 1) / 2);
+      chans[vc].out_ptr = 0;
+      for (int ti = 0; ti < nb; ++ti)
+        for (int tj = 0; tj <= (pair ? ti / 2 : ti); ++tj)
+          tiles.push_back(TileDesc{vc, uint16_t(ti), uint16_t(tj)});
+    }
   }
   auto p = std::make_unique<Plan>();
   p->num_tiles = int(tiles.size());
@@ -285,6 +315,7 @@ ftdx_status ftdx_destroy(ftdx_handle h) {
   for (auto e : h->event_pool) cudaEventDestroy(e);
   if (h->z) cudaFree(h->z);
   if (h->aux) cudaFree(h->aux);
+  if (h->split_ws) cudaFree(h->split_ws);
   if (h->d_status) cudaFree(h->d_status);
   if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
   delete h;

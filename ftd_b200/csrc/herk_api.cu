@@ -131,9 +131,17 @@ bool use_pair(ftdx_handle h, const Strategy& strat) {
   return strat.store_mode == 2 && pair_grid_limit(h) >= 2;
 }
 
+// Split-K count a call actually uses: none for Kahan, the XEngine formats and
+// NVFP4; at most one split per k-block.
+int effective_splits(const HerkCall& c, const Strategy& strat) {
+  if (strat.splits <= 1 || c.comp || c.out_format != 0 || is_fp4(c)) return 1;
+  const int kblocks = int(round_up(c.K, kStageK) / kStageK);
+  return std::min(strat.splits, kblocks);
+}
+
 // Workspace and tile plan for a call; allocates, so never while capturing.
 ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan** plan,
-                    bool pair = false) {
+                    bool pair = false, int splits = 1) {
   const int64_t Kp = round_up(c.K, kStageK);
   const int64_t zpitch = is_split(c) ? 2 * Kp : Kp;
   const int64_t rows = int64_t(c.N) * c.batch;
@@ -144,15 +152,21 @@ ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan
     st = ensure_aux(h, size_t(12) * size_t(c.batch) + 256, s);
     if (st != FTDX_OK) return st;
   }
-  return get_plan(h, c.N, int(Kp / kStageK), c.batch, s, plan, pair);
+  if (splits > 1) {
+    st = ensure_split_ws(h, size_t(splits) * size_t(c.batch) *
+                                size_t(int64_t(c.N) * (c.N + 1) / 2) * sizeof(float2), s);
+    if (st != FTDX_OK) return st;
+  }
+  return get_plan(h, c.N, int(Kp / kStageK), c.batch, s, plan, pair, splits);
 }
 
 // Promotion kernel + correlator kernel on stream s.
 ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, cudaStream_t s) {
   if (is_fp4(c)) return launch_fp4(h, c, s);
   const bool pair = use_pair(h, strat);
+  const int splits = effective_splits(c, strat);
   const Plan* plan = nullptr;
-  ftdx_status st = prepare(h, c, s, &plan, pair);
+  ftdx_status st = prepare(h, c, s, &plan, pair, splits);
   if (st != FTDX_OK) return st;
   const int64_t Kp = round_up(c.K, kStageK);
   const int64_t zpitch = is_split(c) ? 2 * Kp : Kp;
@@ -220,6 +234,13 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
     args.kahan = 1;
     args.out2 = c.comp;
   }
+  if (splits > 1) {  // partial triangles, reduced below
+    args.out = h->split_ws;
+    args.out_fp16 = 0;
+    args.alpha = 1.f;
+    args.beta = 0.f;
+    args.chan_scale = nullptr;
+  }
   if (pair) {
     // persistent pairs, at most as many as can be resident together
     const int limit = pair_grid_limit(h);
@@ -237,6 +258,13 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
     e = launch_herk_fp8(tmZ, args, grid, s);
   }
   if (e != cudaSuccess) return cuda_fail(h, e, "correlator kernel launch");
+  if (splits > 1) {
+    e = launch_split_reduce(reinterpret_cast<const float2*>(h->split_ws), c.C,
+                            c.output == FTDX_OUT_FP16 ? 1 : 0, int64_t(c.N) * (c.N + 1) / 2,
+                            c.batch, splits, c.alpha, c.beta,
+                            c.input == FTDX_IN_FP32 ? out_scale : nullptr, h->sm_count, s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "split-K reduction launch");
+  }
   return FTDX_OK;
 }
 
@@ -254,9 +282,15 @@ ftdx_status run_tune(ftdx_handle h, const HerkCall& c, cudaStream_t s, TuneEntry
   ftdx_status st = prepare(h, c, s, &plan);
   if (st != FTDX_OK) return st;
   TuneEntry best;
+  std::vector<Strategy> cands = default_candidates(h, c.output == FTDX_OUT_FP32, !is_fp4(c));
+  const int kblocks = int(round_up(c.K, kStageK) / kStageK);
+  if (!is_fp4(c) && !c.comp && plan->num_tiles < h->sm_count)
+    for (int sp : {2, 4, 8, 16, 32})
+      if (sp <= kblocks && plan->num_tiles * (sp / 2) < 2 * h->sm_count)
+        cands.push_back(Strategy{0, h->sm_count, sp});
   st = tune_sweep(
       h, [&](const Strategy& cand, cudaStream_t ss) { return launch_all(h, c, cand, ss); },
-      default_candidates(h, c.output == FTDX_OUT_FP32, !is_fp4(c)), s, &best);
+      cands, s, &best);
   if (st != FTDX_OK) return st;
   record_tuned(h, tune_key(h, c), best);
   if (out) *out = best;
@@ -266,13 +300,14 @@ ftdx_status run_tune(ftdx_handle h, const HerkCall& c, cudaStream_t s, TuneEntry
 ftdx_status run_graph(ftdx_handle h, const HerkCall& c, const Strategy& strat, cudaStream_t s) {
   const GraphKey key{c.A, c.C, c.N, c.K, c.batch,
                      int(c.input) | (int(c.compute) << 4) | (c.comp ? 256 : 0), int(c.output),
-                     c.alpha, c.beta, strat.store_mode, strat.grid};
+                     c.alpha, c.beta, strat.store_mode, strat.grid, strat.splits};
   return graph_launch(
       h, key,
       [&](cudaStream_t ss) {
         const Plan* plan = nullptr;
         return ss == h->capture_stream ? launch_all(h, c, strat, ss)
-                                       : prepare(h, c, ss, &plan, use_pair(h, strat));
+                                       : prepare(h, c, ss, &plan, use_pair(h, strat),
+                                                 effective_splits(c, strat));
       },
       s);
 }
@@ -317,7 +352,8 @@ ftdx_status tune_sweep(ftdx_handle h, const LaunchFn& launch, const std::vector<
     }
     ms /= reps;
     if (h->verbosity > 1)
-      fprintf(stderr, "ftdx tune: store=%d grid=%d %.4f ms\n", cand.store_mode, cand.grid, ms);
+      fprintf(stderr, "ftdx tune: store=%d grid=%d splits=%d %.4f ms\n", cand.store_mode,
+              cand.grid, cand.splits, ms);
     if (best.ms < 0.f || ms < best.ms) best = TuneEntry{cand, ms};
   }
   h->profiling = prof;
@@ -330,8 +366,8 @@ ftdx_status tune_sweep(ftdx_handle h, const LaunchFn& launch, const std::vector<
 void record_tuned(ftdx_handle h, const TuneKey& k, const TuneEntry& e) {
   h->tuned[k] = e;
   if (h->verbosity > 0)
-    fprintf(stderr, "ftdx tuned n=%d kp=%d batch=%d -> store=%d grid=%d (%.4f ms)\n", k.n, k.kp,
-            k.batch, e.st.store_mode, e.st.grid, e.ms);
+    fprintf(stderr, "ftdx tuned n=%d kp=%d batch=%d -> store=%d grid=%d splits=%d (%.4f ms)\n",
+            k.n, k.kp, k.batch, e.st.store_mode, e.st.grid, e.st.splits, e.ms);
   if (h->tune_cache.empty()) return;
   FILE* f = fopen(h->tune_cache.c_str(), "a");
   if (!f) {
@@ -339,8 +375,8 @@ void record_tuned(ftdx_handle h, const TuneKey& k, const TuneEntry& e) {
          strerror(errno));
     return;
   }
-  fprintf(f, "ftdx-tune 1 %s %d %d %d %d %d %d %d %.6f\n", k.device.c_str(), k.n, k.kp, k.batch,
-          k.input, k.output, e.st.store_mode, e.st.grid, e.ms);
+  fprintf(f, "ftdx-tune 2 %s %d %d %d %d %d %d %d %d %.6f\n", k.device.c_str(), k.n, k.kp,
+          k.batch, k.input, k.output, e.st.store_mode, e.st.grid, e.st.splits, e.ms);
   fclose(f);
 }
 
@@ -394,7 +430,8 @@ void release_graphs(ftdx_handle h) {
 }
 
 // Text cache, one entry per line:
-//   ftdx-tune 1 <device> <N> <Kp> <batch> <input> <output> <store_mode> <grid> <ms>
+//   ftdx-tune 2 <device> <N> <Kp> <batch> <input> <output> <store_mode> <grid> <splits> <ms>
+// (version 1 lines, without <splits>, are read as splits = 1).
 // Unreadable or malformed lines are skipped and counted.
 void load_tune_cache(ftdx_handle h) {
   h->cache_bad_lines = 0;
@@ -409,10 +446,14 @@ void load_tune_cache(ftdx_handle h) {
     int ver = 0;
     TuneKey k;
     TuneEntry e;
-    if (!(is >> magic >> ver >> dev >> k.n >> k.kp >> k.batch >> k.input >> k.output >>
-          e.st.store_mode >> e.st.grid >> e.ms) ||
-        magic != "ftdx-tune" || ver != 1 || (k.n < 1 && k.n != -1) || k.kp < 1 || k.batch < 1 ||
-        e.st.store_mode < 0 || e.st.store_mode > 2 || e.st.grid < 0 || !(e.ms >= 0.f)) {
+    bool ok = static_cast<bool>(is >> magic >> ver >> dev >> k.n >> k.kp >> k.batch >> k.input >>
+                                k.output >> e.st.store_mode >> e.st.grid);
+    e.st.splits = 1;
+    if (ok && ver == 2) ok = static_cast<bool>(is >> e.st.splits);
+    if (ok) ok = static_cast<bool>(is >> e.ms);
+    if (!ok || magic != "ftdx-tune" || (ver != 1 && ver != 2) || (k.n < 1 && k.n != -1) ||
+        k.kp < 1 || k.batch < 1 || e.st.store_mode < 0 || e.st.store_mode > 2 || e.st.grid < 0 ||
+        e.st.splits < 1 || e.st.splits > 32 || !(e.ms >= 0.f)) {
       ++h->cache_bad_lines;
       continue;
     }
@@ -676,6 +717,22 @@ ftdx_status ftdx_herk_kahan(ftdx_handle h, const void* A, void* sum, void* comp,
   return launch_all(h, c, strat, static_cast<cudaStream_t>(stream));
 }
 
+ftdx_status ftdx_set_split_k(ftdx_handle h, int splits) {
+  if (!h) return FTDX_ERR_INVALID_ARG;
+  if (splits < 1 || splits > 32)
+    return fail(h, FTDX_ERR_INVALID_ARG, "set_split_k: splits must be 1..32 (got %d)", splits);
+  h->default_strategy.splits = splits;
+  return FTDX_OK;
+}
+
+int ftdx_tuned_split_k(ftdx_handle h, int N, int K, int batch, ftdx_input input,
+                       ftdx_output output) {
+  if (!h) return -1;
+  const HerkCall c{nullptr, nullptr, N, K, batch, input, output, 1.f, 0.f};
+  auto it = h->tuned.find(tune_key(h, c));
+  return it == h->tuned.end() ? -1 : it->second.st.splits;
+}
+
 ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid) {
   if (!h) return FTDX_ERR_INVALID_ARG;
   if (store_mode < 0 || store_mode > 2 || grid < -1)
@@ -686,7 +743,7 @@ ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid) {
     if (pair_grid_limit(h) < 2)
       return fail(h, FTDX_ERR_UNSUPPORTED, "set_strategy: no CTA pair fits on this device");
   }
-  h->default_strategy = Strategy{store_mode, grid};
+  h->default_strategy = Strategy{store_mode, grid, h->default_strategy.splits};
   return FTDX_OK;
 }
 

@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
           const int kk = kb - seg * cd.kblocks;
           const int sa = seg == 0 ? args.seg_a[0] : (seg == 1 ? args.seg_a[1] : args.seg_a[2]);
           const int sb = seg == 0 ? args.seg_b[0] : (seg == 1 ? args.seg_b[1] : args.seg_b[2]);
-          const int32_t kA = (sa + kk) * kStageK, kB = (sb + kk) * kStageK;
+          const int32_t kA = (sa + cd.kb0 + kk) * kStageK, kB = (sb + cd.kb0 + kk) * kStageK;
           const bool share = diag && sa == sb;
           mbar_arrive_expect_tx(full_bar(stage), share ? 2 * kPlaneBytes : kStageBytes);
           tma_load_3d(plane_addr(stage, 0), &tmZ, kA, rowJ, 0, full_bar(stage));
@@ -754,7 +754,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
           const int kk = kb - seg * cd.kblocks;
           const int sa = seg == 0 ? args.seg_a[0] : (seg == 1 ? args.seg_a[1] : args.seg_a[2]);
           const int sb = seg == 0 ? args.seg_b[0] : (seg == 1 ? args.seg_b[1] : args.seg_b[2]);
-          const int32_t kA = (sa + kk) * kStageK, kB = (sb + kk) * kStageK;
+          const int32_t kA = (sa + cd.kb0 + kk) * kStageK, kB = (sb + cd.kb0 + kk) * kStageK;
           if (leader) mbar_arrive_expect_tx(full_bar(stage), 2 * kPairStageBytes);
           const uint32_t fb = map_shared(full_bar(stage), 0);
           tma_load_3d_pair(plane(stage, 0), &tmZ, kA, rowJ, 0, fb);
@@ -990,6 +990,54 @@ cudaError_t launch_herk_fp8_pair(const CUtensorMap& tmZ, const HerkArgs& a, int 
                                  cudaStream_t s) {
   if (grid < 2 || (grid & 1)) return cudaErrorInvalidConfiguration;
   return a.out_fp16 ? launch_pair_t<__half>(tmZ, a, grid, s) : launch_pair_t<float>(tmZ, a, grid, s);
+}
+
+// Split-K: the correlator wrote `splits` partial triangles per channel
+// (ws[c*splits + s][P]); C = alpha * cs_c * sum_s partial_s + beta * C.  The
+// partials of integer inputs are exact integers, so the sum is too.
+template <typename Out2>
+__global__ void __launch_bounds__(256) split_reduce_kernel(const float2* __restrict__ ws,
+                                                           Out2* __restrict__ out, int64_t P,
+                                                           int batch, int splits, float alpha,
+                                                           float beta,
+                                                           const float* __restrict__ chan_scale) {
+  const int64_t total = int64_t(batch) * P;
+  for (int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < total;
+       x += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t c = x / P, p = x - c * P;
+    const float2* w = ws + c * splits * P + p;
+    float re = 0.f, im = 0.f;
+    for (int s = 0; s < splits; ++s) {
+      const float2 v = __ldcs(w + int64_t(s) * P);
+      re += v.x;
+      im += v.y;
+    }
+    const float sc = alpha * (chan_scale ? chan_scale[c] : 1.f);
+    re *= sc;
+    im *= sc;
+    if (beta != 0.f) {
+      const float2 o = get(out + x);
+      re += beta * o.x;
+      im += beta * o.y;
+    }
+    put(out + x, re, im);
+  }
+}
+
+cudaError_t launch_split_reduce(const float2* ws, void* out, int out_fp16, int64_t P, int batch,
+                                int splits, float alpha, float beta, const float* chan_scale,
+                                int sm_count, cudaStream_t s) {
+  const int64_t total = int64_t(batch) * P;
+  int64_t blocks = (total + 255) / 256;
+  if (blocks > int64_t(sm_count) * 16) blocks = int64_t(sm_count) * 16;
+  if (blocks < 1) blocks = 1;
+  if (out_fp16)
+    split_reduce_kernel<__half2><<<unsigned(blocks), 256, 0, s>>>(
+        ws, static_cast<__half2*>(out), P, batch, splits, alpha, beta, chan_scale);
+  else
+    split_reduce_kernel<float2><<<unsigned(blocks), 256, 0, s>>>(
+        ws, static_cast<float2*>(out), P, batch, splits, alpha, beta, chan_scale);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s) {

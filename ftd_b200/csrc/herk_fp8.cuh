@@ -59,6 +59,8 @@ struct ChanDesc {
   int64_t row0;
   int64_t out0;
   int64_t out_ptr;
+  int32_t kb0;  // first k-block (split-K: each split is its own channel entry)
+  int32_t pad;
 };
 
 // One channel of a batched call with its own input geometry: the promotion
@@ -139,6 +141,10 @@ cudaError_t launch_fp16_to_planes(const void* a16, uint8_t* z, int64_t rows, int
 cudaError_t launch_gather_qc_to_planes(const GatherDesc* g, int nch, int max_n, uint8_t* z,
                                        int64_t total_rows, int Kp, cudaStream_t s);
 cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s);
+// Split-K reduction: C[c] = alpha * cs_c * sum_s ws[c*splits + s] + beta * C[c].
+cudaError_t launch_split_reduce(const float2* ws, void* out, int out_fp16, int64_t P, int batch,
+                                int splits, float alpha, float beta, const float* chan_scale,
+                                int sm_count, cudaStream_t s);
 // CTA-pair variant: tiles of 256 column x 128 row inputs (TileDesc::tj counts
 // 256-input blocks); tmZ covers three planes (Re, Im, -Re), boxes of 128
 // rows; grid even.

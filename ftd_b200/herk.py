@@ -219,9 +219,17 @@ class Correlator:
             return None
         return {"store_mode": sm.value, "grid": g.value, "ms": ms.value}
 
-    def set_strategy(self, store_mode: int = 0, grid: int = 0) -> None:
-        """Strategy of untuned calls; grid=-1 is a plain one-tile-per-CTA launch."""
+    def set_strategy(self, store_mode: int = 0, grid: int = 0, splits: int | None = None) -> None:
+        """Strategy of untuned calls; grid=-1 is a plain one-tile-per-CTA launch;
+        splits = split-K ranges (None leaves it unchanged)."""
         check(self._h, self._L.ftdx_set_strategy(self._h, store_mode, grid), "ftdx_set_strategy")
+        if splits is not None:
+            check(self._h, self._L.ftdx_set_split_k(self._h, splits), "ftdx_set_split_k")
+
+    def tuned_split_k(self, N: int, K: int, batch: int, input: int = IN_INT4,
+                      output: int = OUT_FP32) -> int:
+        """Split-K count the autotuner recorded for this shape (-1: none)."""
+        return int(self._L.ftdx_tuned_split_k(self._h, N, K, batch, input, output))
 
     def set_graph_mode(self, enable: bool) -> None:
         check(self._h, self._L.ftdx_set_graph_mode(self._h, int(bool(enable))),

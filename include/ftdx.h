@@ -319,6 +319,18 @@ FTDX_API int ftdx_graph_count(ftdx_handle h);
  * store_mode 2 for uniform calls. */
 FTDX_API ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid);
 
+/* Split-K for untuned calls: K is cut into `splits` (1..32) ranges of
+ * k-blocks, each correlated into its own partial triangle, and a reduction
+ * pass adds them (C = alpha * sum + beta * C).  Fills the GPU when a call has
+ * fewer tiles than SMs (few inputs, long integrations); integer inputs stay
+ * exact.  Not used with Kahan accumulation, the XEngine formats or NVFP4.
+ * The autotuner also times split-K candidates for such calls and records the
+ * choice in the cache (version 2 lines); ftdx_tuned_split_k returns it (-1: no
+ * tuned entry). */
+FTDX_API ftdx_status ftdx_set_split_k(ftdx_handle h, int splits);
+FTDX_API int ftdx_tuned_split_k(ftdx_handle h, int N, int K, int batch, ftdx_input input,
+                                ftdx_output output);
+
 /* ---- correlation without any allocation -----------------------------------
  * No counterpart in the reference.  For callers that must not have the
  * library allocate GPU memory once they run: real-time pipelines that size

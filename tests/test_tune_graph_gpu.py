@@ -31,7 +31,7 @@ def test_tune_writes_and_reloads_cache(tmp_path):
         # the sweep leaves a correct result behind
         assert np.array_equal(C.cpu().numpy(), oracle.herk_qc(qc, N, K, B).astype(np.float32))
     lines = open(path).read().splitlines()
-    assert len(lines) == 1 and lines[0].startswith("ftdx-tune 1 ")
+    assert len(lines) == 1 and lines[0].startswith("ftdx-tune 2 ")
     with Correlator(tune_cache=path) as c2:  # a new handle reads it back
         got = c2.lookup_tuned(N, K, B)
         assert got is not None and got["store_mode"] == win["store_mode"]

@@ -19,7 +19,7 @@ def _sizes(N, K, batch):
     Kp = (K + 127) // 128 * 128
     nb = (N + 127) // 128
     tiles = batch * nb * (nb + 1) // 2
-    plan = batch * 32 + tiles * 8
+    plan = batch * 40 + tiles * 8  # ChanDesc (40 B) per channel, TileDesc (8 B) per tile
     z_off = (256 + plan + 1023) // 1024 * 1024
     return z_off + 2 * N * batch * Kp
 
