@@ -55,7 +55,8 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-peak", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the extra workload legs")
-    p.add_argument("--leg", default=None, choices=["nvfp4", "raw", "imaging", "xengine"],
+    p.add_argument("--leg", default=None,
+                   choices=["nvfp4", "raw", "imaging", "xengine", "splitk"],
                    help="run one extra workload alone and print its JSON (profiling cases); "
                         "nvfp4 uses --inputs/--channels/--k")
     p.add_argument("--strategy", default=None,
@@ -362,12 +363,13 @@ def run_ours(args, rank, world, dist):
     if not args.no_e2e:
         e2e = run_e2e(torch, args, dev, qc, N, K, B, flops, world, dist)
 
-    batched = precision = differentiation = raw_layout = imaging = xengine = None
+    batched = precision = differentiation = raw_layout = imaging = xengine = splitk = None
     if not args.no_extra:
         batched = run_batched_leg(torch, dev)
         raw_layout = run_ftd_leg(torch, dev)
         imaging = run_imaging_leg(torch, dev)
         xengine = run_xengine_leg(torch, dev)
+        splitk = run_splitk_leg(torch, dev)
         precision = run_precision_leg(torch, dev)
         differentiation = run_diff_leg(torch, dev)
 
@@ -416,6 +418,7 @@ def run_ours(args, rank, world, dist):
         "raw_layout_fused_corner_turn": raw_layout,
         "imaging_from_triangles": imaging,
         "xengine_upper_triangle": xengine,
+        "split_k_long_integration": splitk,
         "precision_modes": precision,
         "adjoint_and_gain_gradient": differentiation,
         "clocks": clk,
@@ -545,6 +548,30 @@ def run_xengine_leg(torch, dev, n_ant=2048, K=1024, batch=128, seed=9):
                         f"-> packed upper triangles (FP32)",
             "value": herk_flops(n_ant, K, batch) / (ms * 1e-3) / 1e12, "unit": UNIT,
             "ms_per_step": ms}
+
+
+def run_splitk_leg(torch, dev, N=256, K=65536, B=4, seed=10):
+    """Few inputs, long integration (256 inputs x 4 channels x K = 65536: 12
+    tiles for 148 SMs): the plain persistent launch against the autotuned
+    strategy, which splits K."""
+    from ftd_b200 import Correlator, tri_size
+    from ftd_b200._lib import IN_INT4, OUT_FP32
+    qc = make_qc(torch, B, N, K, dev, seed=seed)
+    C = torch.empty(B, tri_size(N), 2, device=dev)
+    flops = herk_flops(N, K, B)
+    with Correlator(device=dev.index) as c:
+        plain = _timed(torch, lambda: c.herk(qc, C, N, K, B, input=IN_INT4, output=OUT_FP32,
+                                             tune=False), reps=10)
+        c.tune(qc, C, N, K, B)
+        splits = c.tuned_split_k(N, K, B)
+        tuned = _timed(torch, lambda: c.herk(qc, C, N, K, B, input=IN_INT4, output=OUT_FP32,
+                                             tune=True), reps=10)
+        if c.device_status() != 0:
+            raise RuntimeError("device status after the split-K leg")
+    return {"workload": f"split-K: {N} inputs x {B} channels x K={K}",
+            "value": flops / (tuned * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": tuned,
+            "tuned_splits": splits,
+            "unsplit": {"value": flops / (plain * 1e-3) / 1e12, "ms_per_step": plain}}
 
 
 def _timed(torch, fn, reps=5, warm=2):
@@ -715,6 +742,8 @@ def run_leg(args):
         out = run_ftd_leg(torch, dev)
     elif args.leg == "imaging":
         out = run_imaging_leg(torch, dev)
+    elif args.leg == "splitk":
+        out = run_splitk_leg(torch, dev)
     else:
         out = run_xengine_leg(torch, dev)
     print(json.dumps(out), flush=True)
