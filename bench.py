@@ -56,9 +56,9 @@ def parse():
     p.add_argument("--no-peak", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the extra workload legs")
     p.add_argument("--leg", default=None,
-                   choices=["nvfp4", "raw", "imaging", "xengine", "splitk"],
+                   choices=["nvfp4", "nvfp4split", "raw", "imaging", "xengine", "splitk"],
                    help="run one extra workload alone and print its JSON (profiling cases); "
-                        "nvfp4 uses --inputs/--channels/--k")
+                        "nvfp4 and nvfp4split use --inputs/--channels/--k")
     p.add_argument("--strategy", default=None,
                    help="STORE_MODE,GRID: fix the correlator strategy instead of autotuning "
                         "(0 direct stores, 1 bulk stores, 2 CTA-pair kernel)")
@@ -595,8 +595,8 @@ def run_precision_leg(torch, dev, N=4096, B=64, K=1024, seed=4, n_err=512):
     an FP64 correlation (torch, on the device) of the first n_err inputs of
     two channels: |dR_ij| / sqrt(R_ii R_jj), cross- and auto-correlations."""
     from ftd_b200 import Correlator, tri_size
-    from ftd_b200._lib import (COMPUTE_FP4, COMPUTE_FP8, COMPUTE_FP8_SPLIT, IN_FP32,
-                               OUT_FP32)
+    from ftd_b200._lib import (COMPUTE_FP4, COMPUTE_FP4_SPLIT, COMPUTE_FP8, COMPUTE_FP8_SPLIT,
+                               IN_FP32, OUT_FP32)
     g = torch.Generator(device=dev).manual_seed(seed)
     rms = torch.exp(torch.empty(B, device=dev).uniform_(float(__import__("math").log(0.1)),
                                                          float(__import__("math").log(10.0)),
@@ -625,7 +625,8 @@ def run_precision_leg(torch, dev, N=4096, B=64, K=1024, seed=4, n_err=512):
     out = {}
     with Correlator(device=dev.index) as c:
         for name, mode in [("fp8_channel_scaled", COMPUTE_FP8), ("fp8_hi_lo_split", COMPUTE_FP8_SPLIT),
-                           ("nvfp4_block16", COMPUTE_FP4)]:
+                           ("nvfp4_block16", COMPUTE_FP4),
+                           ("nvfp4_hi_lo_split", COMPUTE_FP4_SPLIT)]:
             def step():
                 c.herk(V, C, N, K, B, input=IN_FP32, compute=mode, output=OUT_FP32, tune=False)
             ms = _timed(torch, step)
@@ -714,21 +715,23 @@ def run_e2e(torch, args, dev, qc_dev, N, K, B, flops, world, dist):
                     "host wall time"}
 
 
-def run_nvfp4_case(torch, dev, N, K, B, reps=5, seed=1):
+def run_nvfp4_case(torch, dev, N, K, B, reps=5, seed=1, split=False):
     """NVFP4 correlation of seeded Gaussian FP32 complex voltages [B][N][K]:
     reps calls, the whole FP4 path (amax, quantisation, row power, correlator)
-    timed with CUDA events."""
+    timed with CUDA events.  split: the hi + lo mode (four products)."""
     from ftd_b200 import Correlator, tri_size
-    from ftd_b200._lib import COMPUTE_FP4, IN_FP32, OUT_FP32
+    from ftd_b200._lib import COMPUTE_FP4, COMPUTE_FP4_SPLIT, IN_FP32, OUT_FP32
+    mode = COMPUTE_FP4_SPLIT if split else COMPUTE_FP4
     g = torch.Generator(device=dev).manual_seed(seed)
     A = torch.randn(B, N, K, 2, device=dev, generator=g)
     C = torch.empty(B, tri_size(N), 2, device=dev)
     with Correlator(device=dev.index) as c:
-        ms = _timed(torch, lambda: c.herk(A, C, N, K, B, input=IN_FP32, compute=COMPUTE_FP4,
+        ms = _timed(torch, lambda: c.herk(A, C, N, K, B, input=IN_FP32, compute=mode,
                                           output=OUT_FP32, tune=False), reps=reps)
         if c.device_status() != 0:
             raise RuntimeError("device status after the NVFP4 case")
-    return {"workload": f"NVFP4: {N} inputs x {B} channels x K={K}, Gaussian FP32 complex",
+    return {"workload": f"NVFP4{' hi+lo' if split else ''}: {N} inputs x {B} channels x K={K}, "
+                        f"Gaussian FP32 complex",
             "value": herk_flops(N, K, B) / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms}
 
 
@@ -738,6 +741,8 @@ def run_leg(args):
     torch.cuda.set_device(dev)
     if args.leg == "nvfp4":
         out = run_nvfp4_case(torch, dev, args.inputs, args.k, args.channels)
+    elif args.leg == "nvfp4split":
+        out = run_nvfp4_case(torch, dev, args.inputs, args.k, args.channels, split=True)
     elif args.leg == "raw":
         out = run_ftd_leg(torch, dev)
     elif args.leg == "imaging":

@@ -20,7 +20,7 @@ STATUS_NAMES = {
 
 # enum values (include/ftdx.h)
 IN_FP16, IN_INT4, IN_FP32 = 0, 1, 2
-COMPUTE_FP8, COMPUTE_FP6, COMPUTE_FP4, COMPUTE_FP8_SPLIT = 0, 1, 2, 3
+COMPUTE_FP8, COMPUTE_FP6, COMPUTE_FP4, COMPUTE_FP8_SPLIT, COMPUTE_FP4_SPLIT = 0, 1, 2, 3, 4
 OUT_FP16, OUT_FP32 = 0, 1
 FORMAT_PACKED_TRIANGLE = 0
 LAYOUT_TIME_ANT_CHAN_POL, LAYOUT_CHAN_POL_ANT_TIME = 0, 1

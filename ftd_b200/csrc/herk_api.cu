@@ -32,7 +32,9 @@ struct HerkCall {
 };
 
 bool is_split(const HerkCall& c) { return c.compute == FTDX_COMPUTE_FP8_SPLIT; }
-bool is_fp4(const HerkCall& c) { return c.compute == FTDX_COMPUTE_FP4; }
+bool is_fp4(const HerkCall& c) {
+  return c.compute == FTDX_COMPUTE_FP4 || c.compute == FTDX_COMPUTE_FP4_SPLIT;
+}
 
 ftdx_status validate(ftdx_handle h, const HerkCall& c, ftdx_compute compute, ftdx_format format) {
   if (!c.A || !c.C) return fail(h, FTDX_ERR_INVALID_ARG, "herk: null A or C");
@@ -47,11 +49,11 @@ ftdx_status validate(ftdx_handle h, const HerkCall& c, ftdx_compute compute, ftd
     return fail(h, FTDX_ERR_INVALID_ARG, "herk: only the packed triangle format exists");
   if (compute == FTDX_COMPUTE_FP8_SPLIT && c.input != FTDX_IN_FP32)
     return fail(h, FTDX_ERR_INVALID_ARG, "herk: split FP8 needs FP32 input");
-  if (compute == FTDX_COMPUTE_FP4 &&
+  if ((compute == FTDX_COMPUTE_FP4 || compute == FTDX_COMPUTE_FP4_SPLIT) &&
       (c.input != FTDX_IN_FP32 || c.output != FTDX_OUT_FP32 || c.comp != nullptr))
     return fail(h, FTDX_ERR_UNSUPPORTED, "herk: NVFP4 needs FP32 input and FP32 output");
   if (compute != FTDX_COMPUTE_FP8 && compute != FTDX_COMPUTE_FP8_SPLIT &&
-      compute != FTDX_COMPUTE_FP4)
+      compute != FTDX_COMPUTE_FP4 && compute != FTDX_COMPUTE_FP4_SPLIT)
     return fail(h, FTDX_ERR_UNSUPPORTED, "herk: compute precision %d not implemented for "
                 "this entry point", int(compute));
   if (c.input == FTDX_IN_FP32 && (reinterpret_cast<uintptr_t>(c.A) & 7) != 0)
@@ -109,7 +111,8 @@ ftdx_status get_fp4_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStrea
 
 ftdx_status launch_fp4(ftdx_handle h, const HerkCall& c, cudaStream_t s) {
   const int64_t rows = int64_t(c.N) * c.batch;
-  ftdx_status st = ensure_workspace(h, nvfp4_workspace_bytes(rows, c.K), s);
+  const int split = c.compute == FTDX_COMPUTE_FP4_SPLIT ? 1 : 0;
+  ftdx_status st = ensure_workspace(h, nvfp4_workspace_bytes(rows, c.K, split), s);
   if (st == FTDX_OK) st = ensure_aux(h, size_t(12) * size_t(c.batch) + 256, s);
   const Plan* plan = nullptr;
   if (st == FTDX_OK) st = get_fp4_plan(h, c.N, nvfp4_kblocks(c.K), c.batch, s, &plan);
@@ -122,7 +125,7 @@ ftdx_status launch_fp4(ftdx_handle h, const HerkCall& c, cudaStream_t s) {
     ScopedTimer tm(h, s, 0);
     e = launch_nvfp4(c.A, rows, c.K, c.N, c.batch, h->z, gscale, out_scale, amax,
                      plan->d_tiles, plan->d_chans, plan->num_tiles, c.C, c.alpha, c.beta,
-                     h->d_status, h->sm_count, tensor_map_encoder(), s);
+                     h->d_status, h->sm_count, tensor_map_encoder(), s, split);
   }
   return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "NVFP4 launch");
 }

@@ -58,6 +58,11 @@ __device__ __forceinline__ float ue4m3_value(uint32_t c) {
 __device__ __forceinline__ uint32_t fp4x2(float a, float b) {
   return uint32_t(__nv_cvt_float2_to_fp4x2(make_float2(a, b), __NV_E2M1, cudaRoundNearest));
 }
+// Values of a byte of two E2M1 codes.
+__device__ __forceinline__ float2 fp4x2_value(uint32_t byte) {
+  const __half2_raw h = __nv_cvt_fp4x2_to_halfraw2(__nv_fp4x2_storage_t(byte), __NV_E2M1);
+  return __half22float2(__half2(h));
+}
 
 __global__ void fp4_scale_kernel(const uint32_t* __restrict__ amax_bits, int batch,
                                  float* __restrict__ gscale, float* __restrict__ out_scale) {
@@ -70,10 +75,15 @@ __global__ void fp4_scale_kernel(const uint32_t* __restrict__ amax_bits, int bat
 }
 
 // One thread: one 16-value block (8 complex samples) of one input row.
+// split: each operand row holds the hi half (pitch bytes) then the lo half,
+// lo = E2M1 of the residual x - hi with its own block scale (same global
+// scale), so hi + lo carries about twice the bits; the scale rows likewise.
 __global__ void __launch_bounds__(256) nvfp4_quantize_kernel(
     const float2* __restrict__ a, uint8_t* __restrict__ z, uint8_t* __restrict__ sf,
-    int64_t rows, int K, int pitch, int sfpitch, int n, const float* __restrict__ gscale) {
+    int64_t rows, int K, int pitch, int sfpitch, int n, const float* __restrict__ gscale,
+    int split) {
   const int blocks_per_row = pitch / 8;  // 8 bytes of E2M1 per block
+  const int rpitch = split ? 2 * pitch : pitch, rsf = split ? 2 * sfpitch : sfpitch;
   const int64_t total = rows * blocks_per_row;
   for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
        idx += int64_t(gridDim.x) * blockDim.x) {
@@ -100,10 +110,36 @@ __global__ void __launch_bounds__(256) nvfp4_quantize_kernel(
       xw[q >> 2] |= fp4x2(re, im) << (8 * (q & 3));
       yw[q >> 2] |= fp4x2(im, -re) << (8 * (q & 3));
     }
-    *reinterpret_cast<uint2*>(z + (2 * r) * pitch + 8 * b) = make_uint2(xw[0], xw[1]);
-    *reinterpret_cast<uint2*>(z + (2 * r + 1) * pitch + 8 * b) = make_uint2(yw[0], yw[1]);
-    sf[(2 * r) * sfpitch + b] = uint8_t(bc);
-    sf[(2 * r + 1) * sfpitch + b] = uint8_t(bc);
+    *reinterpret_cast<uint2*>(z + (2 * r) * rpitch + 8 * b) = make_uint2(xw[0], xw[1]);
+    *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + 8 * b) = make_uint2(yw[0], yw[1]);
+    sf[(2 * r) * rsf + b] = uint8_t(bc);
+    sf[(2 * r + 1) * rsf + b] = uint8_t(bc);
+    if (split) {
+      // residual of the hi quantisation, then its own block scale
+      const float step = bc ? g * ue4m3_value(bc) : 0.f;
+      float amax2 = 0.f;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const float2 h = fp4x2_value((xw[q >> 2] >> (8 * (q & 3))) & 0xFFu);
+        x[2 * q] -= h.x * step;
+        x[2 * q + 1] -= h.y * step;
+        amax2 = fmaxf(amax2, fmaxf(fabsf(x[2 * q]), fabsf(x[2 * q + 1])));
+      }
+      const uint32_t bc2 = ue4m3_ceil(amax2 / (6.f * g));
+      const float inv2 = bc2 ? 1.f / (g * ue4m3_value(bc2)) : 0.f;
+      uint32_t xl[2] = {0u, 0u}, yl[2] = {0u, 0u};
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const float re = x[2 * q] * inv2, im = x[2 * q + 1] * inv2;
+        xl[q >> 2] |= fp4x2(re, im) << (8 * (q & 3));
+        yl[q >> 2] |= fp4x2(im, -re) << (8 * (q & 3));
+      }
+      *reinterpret_cast<uint2*>(z + (2 * r) * rpitch + pitch + 8 * b) = make_uint2(xl[0], xl[1]);
+      *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + pitch + 8 * b) =
+          make_uint2(yl[0], yl[1]);
+      sf[(2 * r) * rsf + sfpitch + b] = uint8_t(bc2);
+      sf[(2 * r + 1) * rsf + sfpitch + b] = uint8_t(bc2);
+    }
   }
 }
 
@@ -139,6 +175,10 @@ struct Fp4Args {
   const float* chan_scale;
   uint32_t* status;
   const float* row_power;  // exact sum_t |v_t|^2 per input row (the autocorrelations)
+  // K segments (hi + lo split: hi.hi, hi.lo, lo.hi, lo.lo): segment s pairs
+  // A k-blocks seg_a[s] + kk with B k-blocks seg_b[s] + kk; nseg = 1: plain
+  int nseg;
+  int seg_a[4], seg_b[4];
 };
 
 __global__ void __launch_bounds__(k4Threads, 1)
@@ -204,17 +244,19 @@ __global__ void __launch_bounds__(k4Threads, 1)
         const ChanDesc cd = args.chans[td.ch];
         const int32_t rowA = int32_t(cd.row0 + int64_t(td.tj) * k4J);        // x-row view
         const int32_t rowB = int32_t(2 * (cd.row0 + int64_t(td.ti) * k4I));  // all rows
-        for (int kb = 0; kb < cd.kblocks; ++kb) {
+        for (int kb = 0; kb < cd.kblocks * args.nseg; ++kb) {
           if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
             atomicOr(args.status, kStatusTimeoutProducer);
             ok = false;
             break;
           }
+          const int seg = kb / cd.kblocks, kk = kb - seg * cd.kblocks;
+          const int ka = args.seg_a[seg] + kk, kbb = args.seg_b[seg] + kk;
           mbar_arrive_expect_tx(full_bar(stage), k4StageBytes);
-          tma_load_2d(a_addr(stage), &tmA, kb * k4KB, rowA, full_bar(stage));
-          tma_load_2d(b_addr(stage), &tmB, kb * k4KB, rowB, full_bar(stage));
-          tma_load_2d(sfa_addr(stage), &tmSa, kb * 16, rowA, full_bar(stage));
-          tma_load_2d(sfb_addr(stage), &tmSb, kb * 16, rowB, full_bar(stage));
+          tma_load_2d(a_addr(stage), &tmA, ka * k4KB, rowA, full_bar(stage));
+          tma_load_2d(b_addr(stage), &tmB, kbb * k4KB, rowB, full_bar(stage));
+          tma_load_2d(sfa_addr(stage), &tmSa, ka * 16, rowA, full_bar(stage));
+          tma_load_2d(sfb_addr(stage), &tmSb, kbb * 16, rowB, full_bar(stage));
           ++issued;
           if (++stage == k4Stages) {
             stage = 0;
@@ -250,7 +292,7 @@ __global__ void __launch_bounds__(k4Threads, 1)
         }
         tc_fence_after();
         const uint32_t d = tmem_base + uint32_t(acc * k4AccCols);
-        for (int kb = 0; kb < cd.kblocks; ++kb) {
+        for (int kb = 0; kb < cd.kblocks * args.nseg; ++kb) {
           if (!mbar_wait(full_bar(stage), phase, abort_flag) ||
               !mbar_wait(sf_bar(stage), phase, abort_flag)) {
             atomicOr(args.status, kStatusTimeoutMma);
@@ -293,7 +335,7 @@ __global__ void __launch_bounds__(k4Threads, 1)
     for (int t = blockIdx.x; t < args.num_tiles; t += gridDim.x) {
       const ChanDesc cd = args.chans[args.tiles[t].ch];
       bool ok = true;
-      for (int kb = 0; kb < cd.kblocks; ++kb) {
+      for (int kb = 0; kb < cd.kblocks * args.nseg; ++kb) {
         ok = __all_sync(0xffffffffu, mbar_wait(full_bar(stage), phase, abort_flag));
         if (!ok) break;
         uint32_t wa[16], wb[16];
@@ -393,9 +435,10 @@ __global__ void __launch_bounds__(k4Threads, 1)
 
 }  // namespace
 
-// Workspace: E2M1 operand rows (2 per input), then their scale bytes.
-size_t nvfp4_workspace_bytes(int64_t rows, int K) {
-  const int64_t pitch = (2 * int64_t(K) + 255) / 256 * 128;  // bytes per operand row
+// Workspace: E2M1 operand rows (2 per input; twice as long when split), then
+// their scale bytes, then the row powers.
+size_t nvfp4_workspace_bytes(int64_t rows, int K, int split) {
+  const int64_t pitch = (2 * int64_t(K) + 255) / 256 * 128 * (split ? 2 : 1);
   return size_t(2 * rows * pitch) + size_t(2 * rows * (pitch / 8)) + size_t(4 * rows) + 4096;
 }
 
@@ -405,14 +448,15 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
                          float* gscale, float* out_scale, uint32_t* amax_bits,
                          const TileDesc* tiles, const ChanDesc* chans, int num_tiles, void* C,
                          float alpha, float beta, uint32_t* status, int sm_count, void* encode_fn,
-                         cudaStream_t s) {
+                         cudaStream_t s, int split) {
   auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(encode_fn);
   if (!encode) return cudaErrorInvalidValue;
-  const int64_t pitch = (2 * int64_t(K) + 255) / 256 * 128;
+  const int64_t pitch = (2 * int64_t(K) + 255) / 256 * 128;  // one half (hi or lo)
   const int64_t sfpitch = pitch / 8;
+  const int64_t rpitch = split ? 2 * pitch : pitch, rsf = split ? 2 * sfpitch : sfpitch;
   uint8_t* z = ws;
-  uint8_t* sf = ws + ((2 * rows * pitch + 1023) / 1024) * 1024;
-  float* power = reinterpret_cast<float*>(sf + ((2 * rows * sfpitch + 1023) / 1024) * 1024);
+  uint8_t* sf = ws + ((2 * rows * rpitch + 1023) / 1024) * 1024;
+  float* power = reinterpret_cast<float*>(sf + ((2 * rows * rsf + 1023) / 1024) * 1024);
   // channel amax -> global scales -> quantise
   cudaError_t e = cudaMemsetAsync(amax_bits, 0, sizeof(uint32_t) * size_t(batch), s);
   if (e != cudaSuccess) return e;
@@ -424,7 +468,7 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
   if (blocks > int64_t(sm_count) * 16) blocks = int64_t(sm_count) * 16;
   nvfp4_quantize_kernel<<<unsigned(blocks), 256, 0, s>>>(static_cast<const float2*>(A), z, sf,
                                                           rows, K, int(pitch), int(sfpitch), n,
-                                                          gscale);
+                                                          gscale, split);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
 
@@ -439,10 +483,10 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
                   CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   };
-  if (enc2(&tmA, z, pitch, rows, 2 * pitch, k4KB, CU_TENSOR_MAP_SWIZZLE_128B) != CUDA_SUCCESS ||
-      enc2(&tmB, z, pitch, 2 * rows, pitch, k4KB, CU_TENSOR_MAP_SWIZZLE_128B) != CUDA_SUCCESS ||
-      enc2(&tmSa, sf, sfpitch, rows, 2 * sfpitch, 16, CU_TENSOR_MAP_SWIZZLE_NONE) != CUDA_SUCCESS ||
-      enc2(&tmSb, sf, sfpitch, 2 * rows, sfpitch, 16, CU_TENSOR_MAP_SWIZZLE_NONE) != CUDA_SUCCESS)
+  if (enc2(&tmA, z, rpitch, rows, 2 * rpitch, k4KB, CU_TENSOR_MAP_SWIZZLE_128B) != CUDA_SUCCESS ||
+      enc2(&tmB, z, rpitch, 2 * rows, rpitch, k4KB, CU_TENSOR_MAP_SWIZZLE_128B) != CUDA_SUCCESS ||
+      enc2(&tmSa, sf, rsf, rows, 2 * rsf, 16, CU_TENSOR_MAP_SWIZZLE_NONE) != CUDA_SUCCESS ||
+      enc2(&tmSb, sf, rsf, 2 * rows, rsf, 16, CU_TENSOR_MAP_SWIZZLE_NONE) != CUDA_SUCCESS)
     return cudaErrorInvalidValue;
   {
     int64_t pb = (rows * 32 + 255) / 256;
@@ -452,6 +496,16 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
     if (e != cudaSuccess) return e;
   }
   Fp4Args args{tiles, chans, num_tiles, C, alpha, beta, out_scale, status, power};
+  args.nseg = 1;
+  if (split) {
+    // hi.hi + hi.lo + lo.hi, lo at L k-blocks into each row; lo.lo (the square
+    // of the residual, ~1/64 of the signal) is left out as in split FP8, and the
+    // autocorrelations come from the exact row powers either way
+    const int L = int(pitch / k4KB);
+    const int sa[3] = {0, 0, L}, sb[3] = {0, L, 0};
+    args.nseg = 3;
+    for (int q = 0; q < 3; ++q) args.seg_a[q] = sa[q], args.seg_b[q] = sb[q];
+  }
   static bool attr = false;
   if (!attr) {
     e = cudaFuncSetAttribute(herk_fp4_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

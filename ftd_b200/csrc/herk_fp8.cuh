@@ -166,13 +166,13 @@ cudaError_t launch_channel_amax(const void* a, int64_t per_chan, int batch, uint
                                 int sm_count, cudaStream_t s);
 // NVFP4 correlator for float complex input (herk_fp4.cu).  Tiles: ti over 64
 // row inputs, tj over 128 column inputs; kblocks = nvfp4_kblocks(K).
-size_t nvfp4_workspace_bytes(int64_t rows, int K);
+size_t nvfp4_workspace_bytes(int64_t rows, int K, int split = 0);
 int nvfp4_kblocks(int K);
 cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, uint8_t* ws,
                          float* gscale, float* out_scale, uint32_t* amax_bits,
                          const TileDesc* tiles, const ChanDesc* chans, int num_tiles, void* C,
                          float alpha, float beta, uint32_t* status, int sm_count, void* encode_fn,
-                         cudaStream_t s);
+                         cudaStream_t s, int split = 0);
 // Float complex [rows][K] -> scaled E4M3 planes of pitch zpitch (precision.cu).
 cudaError_t launch_float_to_planes(const void* a, uint8_t* z, int64_t rows, int K, int Kp,
                                    int zpitch, int n, int batch, int split, float* qscale,

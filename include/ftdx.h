@@ -62,7 +62,9 @@ typedef enum ftdx_compute {
                                   FP32: E4M3 with a per-channel scale */
   FTDX_COMPUTE_FP6 = 1,
   FTDX_COMPUTE_FP4 = 2,        /* NVFP4: E2M1 with one E4M3 scale per 16 values (FP32 input) */
-  FTDX_COMPUTE_FP8_SPLIT = 3   /* FP32 input: hi + lo E4M3, hi.hi^H + hi.lo^H + lo.hi^H */
+  FTDX_COMPUTE_FP8_SPLIT = 3,  /* FP32 input: hi + lo E4M3, hi.hi^H + hi.lo^H + lo.hi^H */
+  FTDX_COMPUTE_FP4_SPLIT = 4   /* FP32 input: hi + lo NVFP4 (lo = NVFP4 of the residual, own
+                                  block scales), hi.hi^H + hi.lo^H + lo.hi^H; FP32 output */
 } ftdx_compute;
 typedef enum ftdx_output { FTDX_OUT_FP16 = 0, FTDX_OUT_FP32 = 1 } ftdx_output;
 typedef enum ftdx_format { FTDX_FORMAT_PACKED_TRIANGLE = 0 } ftdx_format;
