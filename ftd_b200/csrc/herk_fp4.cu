@@ -143,20 +143,39 @@ __global__ void __launch_bounds__(256) nvfp4_quantize_kernel(
   }
 }
 
-// Autocorrelation of every input row, sum_t |v_t|^2, accumulated in FP64
-// (one warp per row).
-__global__ void __launch_bounds__(256) row_power_kernel(const float2* __restrict__ a, int64_t rows,
-                                                        int K, float* __restrict__ power) {
-  const int lane = threadIdx.x & 31;
-  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < rows;
-       r += (int64_t(gridDim.x) * blockDim.x) >> 5) {
+// One pass over the FP32 input for both statistics the quantiser and the
+// epilogue need: the autocorrelation of every input row, sum_t |v_t|^2
+// accumulated in FP64 in a fixed order (one warp per row, so the result is
+// deterministic), and the channel max |Re|, |Im| (block reduce, one atomicMax
+// per block; NaN counts as 0).  Grid (x, channel); warps of a channel's
+// blocks stride over its n rows.
+__global__ void __launch_bounds__(256) fp4_stats_kernel(const float2* __restrict__ a, int n, int K,
+                                                        float* __restrict__ power,
+                                                        uint32_t* __restrict__ amax_bits) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = blockIdx.y;
+  const int wpb = blockDim.x >> 5;
+  float m = 0.f;
+  for (int w = blockIdx.x * wpb + warp; w < n; w += gridDim.x * wpb) {
+    const int64_t r = int64_t(c) * n + w;
+    const float2* p = a + r * K;
     double acc = 0.0;
     for (int t = lane; t < K; t += 32) {
-      const float2 v = __ldg(a + r * K + t);
+      const float2 v = __ldg(p + t);
       acc += double(v.x) * v.x + double(v.y) * v.y;
+      m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) power[r] = float(acc);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ float wm[32];
+  if (lane == 0) wm[warp] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < wpb; ++q) m = fmaxf(m, wm[q]);
+    if (!(m == m)) m = 0.f;
+    atomicMax(amax_bits + c, __float_as_uint(m));
   }
 }
 
@@ -457,11 +476,19 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
   uint8_t* z = ws;
   uint8_t* sf = ws + ((2 * rows * rpitch + 1023) / 1024) * 1024;
   float* power = reinterpret_cast<float*>(sf + ((2 * rows * rsf + 1023) / 1024) * 1024);
-  // channel amax -> global scales -> quantise
+  // row powers + channel amax (one pass) -> global scales -> quantise
   cudaError_t e = cudaMemsetAsync(amax_bits, 0, sizeof(uint32_t) * size_t(batch), s);
   if (e != cudaSuccess) return e;
-  e = launch_channel_amax(A, int64_t(n) * K, batch, amax_bits, sm_count, s);
-  if (e != cudaSuccess) return e;
+  {
+    int bx = (n + 7) / 8;
+    const int cap = (sm_count * 8 + batch - 1) / batch;
+    if (bx > cap) bx = cap;
+    if (bx < 1) bx = 1;
+    fp4_stats_kernel<<<dim3(unsigned(bx), unsigned(batch)), 256, 0, s>>>(
+        static_cast<const float2*>(A), n, K, power, amax_bits);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   fp4_scale_kernel<<<(batch + 127) / 128, 128, 0, s>>>(amax_bits, batch, gscale, out_scale);
   const int64_t work = rows * (pitch / 8);
   int64_t blocks = (work + 255) / 256;
@@ -488,13 +515,6 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
       enc2(&tmSa, sf, rsf, rows, 2 * rsf, 16, CU_TENSOR_MAP_SWIZZLE_NONE) != CUDA_SUCCESS ||
       enc2(&tmSb, sf, rsf, 2 * rows, rsf, 16, CU_TENSOR_MAP_SWIZZLE_NONE) != CUDA_SUCCESS)
     return cudaErrorInvalidValue;
-  {
-    int64_t pb = (rows * 32 + 255) / 256;
-    if (pb > int64_t(sm_count) * 16) pb = int64_t(sm_count) * 16;
-    row_power_kernel<<<unsigned(pb), 256, 0, s>>>(static_cast<const float2*>(A), rows, K, power);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-  }
   Fp4Args args{tiles, chans, num_tiles, C, alpha, beta, out_scale, status, power};
   args.nseg = 1;
   if (split) {
