@@ -380,7 +380,9 @@ def run_ours(args, rank, world, dist):
     if rank != 0:
         return 0
     achieved = flops / (herk_ms * 1e-3) / 1e12
-    kernel_name = "herk_fp8_pair_kernel" if tuned.get("store_mode") == 2 else "herk_fp8_tc_kernel"
+    mode = int(tuned.get("store_mode") or 0)  # + 4: packed FP6 operand planes
+    kernel_name = "herk_fp8_pair_kernel" if (mode & 3) == 2 else "herk_fp8_tc_kernel"
+    prep_name = "qc_to_planes6_kernel" if mode & 4 else "qc_to_planes_kernel"
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "herk_fp8_traffic.json")
     if os.path.exists(tfile):
@@ -408,7 +410,7 @@ def run_ours(args, rank, world, dist):
                      "peak_source": "cuBLASLt dense FP8 e4m3 GEMM 8192^3 (torch._scaled_mm), "
                                     "measured in this run",
                      "frac_of_nominal_4500": achieved / NOMINAL_FP8_TFLOPS},
-        "kernels": {kernel_name + "_ms": herk_ms, "qc_to_planes_kernel_ms": prep_ms},
+        "kernels": {kernel_name + "_ms": herk_ms, prep_name + "_ms": prep_ms},
         "gpu_launches": 2 * args.steps,
         "strategy": {"tuned": tuned, "graph_replay": True},
         "plain_per_channel": plain,

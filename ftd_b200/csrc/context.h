@@ -27,10 +27,12 @@ struct Plan {
   ~Plan();
 };
 
+constexpr int kStoreFp6 = 4;
 // Launch strategy of the correlator kernel; chosen by the autotuner.
 struct Strategy {
   // 0: direct stores, 1: shared-memory staging + bulk copies,
-  // 2: CTA-pair kernel (256 x 128 tiles on two SMs, direct stores)
+  // 2: CTA-pair kernel (256 x 128 tiles on two SMs, direct stores);
+  // + kStoreFp6: operands as packed FP6 E3M2 planes (QC input, exact)
   int store_mode = 0;
   int grid = 0;        // persistent CTAs (0: one per SM); -1: one CTA per tile (not persistent)
   int splits = 1;      // split-K: K is cut into this many ranges, partials summed afterwards
@@ -128,8 +130,10 @@ ftdx_status ensure_aux(ftdx_handle h, size_t bytes, cudaStream_t s);
 ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
                      const Plan** out, bool pair = false, int splits = 1);
 ftdx_status ensure_split_ws(ftdx_handle h, size_t bytes, cudaStream_t s);
+// fp6: planes of packed E3M2 codes (the kernels' fp6 operand form)
 ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t Kp,
-                              CUtensorMap* tm, int box_rows = kTile, int nplanes = 2);
+                              CUtensorMap* tm, int box_rows = kTile, int nplanes = 2,
+                              bool fp6 = false);
 // Even number of CTAs of the pair kernel that can be resident at once.
 int pair_grid_limit(ftdx_handle h);
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }

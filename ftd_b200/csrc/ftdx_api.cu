@@ -199,14 +199,19 @@ int pair_grid_limit(ftdx_handle h) {
 // Tensor map over the operand planes Z[nplanes][rows][Kp] (bytes): box of
 // 128 samples x box_rows rows x 1 plane, 128-byte swizzle.
 ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t Kp,
-                              CUtensorMap* tm, int box_rows, int nplanes) {
+                              CUtensorMap* tm, int box_rows, int nplanes, bool fp6) {
   auto enc = get_encode_fn();
   if (!enc) return fail(h, FTDX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
   const cuuint32_t estr[3] = {1, 1, 1};
+  // fp6: Kp packed 6-bit codes per row (3 Kp / 4 bytes; Kp is a multiple of
+  // 128, so the row pitch is a multiple of 32 bytes as the 16 x U6 type needs),
+  // unpacked by the TMA to one byte per code in shared memory
+  const int64_t pitch = fp6 ? Kp / 4 * 3 : Kp;
   const cuuint64_t dims[3] = {cuuint64_t(Kp), cuuint64_t(rows), cuuint64_t(nplanes)};
-  const cuuint64_t strides[2] = {cuuint64_t(Kp), cuuint64_t(rows * Kp)};
+  const cuuint64_t strides[2] = {cuuint64_t(pitch), cuuint64_t(rows * pitch)};
   const cuuint32_t box[3] = {cuuint32_t(kStageK), cuuint32_t(box_rows), 1};
-  CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, z, dims, strides, box, estr,
+  CUresult r = enc(tm, fp6 ? CU_TENSOR_MAP_DATA_TYPE_16U6_ALIGN16B : CU_TENSOR_MAP_DATA_TYPE_UINT8,
+                   3, z, dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(h, FTDX_ERR_CUDA, "tensor map encode failed: %d", int(r));

@@ -52,8 +52,12 @@ ftdx_status validate(ftdx_handle h, const HerkCall& c, ftdx_compute compute, ftd
   if ((compute == FTDX_COMPUTE_FP4 || compute == FTDX_COMPUTE_FP4_SPLIT) &&
       (c.input != FTDX_IN_FP32 || c.output != FTDX_OUT_FP32 || c.comp != nullptr))
     return fail(h, FTDX_ERR_UNSUPPORTED, "herk: NVFP4 needs FP32 input and FP32 output");
+  if (compute == FTDX_COMPUTE_FP6 && (c.input != FTDX_IN_INT4 || c.comp != nullptr))
+    return fail(h, FTDX_ERR_UNSUPPORTED, "herk: FP6 compute needs INT4 input (block-scaled FP6 "
+                "of FP16/FP32 input is not implemented)");
   if (compute != FTDX_COMPUTE_FP8 && compute != FTDX_COMPUTE_FP8_SPLIT &&
-      compute != FTDX_COMPUTE_FP4 && compute != FTDX_COMPUTE_FP4_SPLIT)
+      compute != FTDX_COMPUTE_FP4 && compute != FTDX_COMPUTE_FP4_SPLIT &&
+      compute != FTDX_COMPUTE_FP6)
     return fail(h, FTDX_ERR_UNSUPPORTED, "herk: compute precision %d not implemented for "
                 "this entry point", int(compute));
   if (c.input == FTDX_IN_FP32 && (reinterpret_cast<uintptr_t>(c.A) & 7) != 0)
@@ -112,7 +116,7 @@ ftdx_status get_fp4_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStrea
 ftdx_status launch_fp4(ftdx_handle h, const HerkCall& c, cudaStream_t s) {
   const int64_t rows = int64_t(c.N) * c.batch;
   const int split = c.compute == FTDX_COMPUTE_FP4_SPLIT ? 1 : 0;
-  ftdx_status st = ensure_workspace(h, nvfp4_workspace_bytes(rows, c.K, split), s);
+  ftdx_status st = ensure_workspace(h, nvfp4_workspace_bytes(c.N, c.batch, c.K, split), s);
   if (st == FTDX_OK) st = ensure_aux(h, size_t(12) * size_t(c.batch) + 256, s);
   const Plan* plan = nullptr;
   if (st == FTDX_OK) st = get_fp4_plan(h, c.N, nvfp4_kblocks(c.K), c.batch, s, &plan);
@@ -130,8 +134,14 @@ ftdx_status launch_fp4(ftdx_handle h, const HerkCall& c, cudaStream_t s) {
   return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "NVFP4 launch");
 }
 
+// Calls whose operands may take the packed FP6 form: QC input through the
+// plain promotion (E3M2 holds every QC value, so results stay exact).
+bool fp6_ok(const HerkCall& c) {
+  return c.input == FTDX_IN_INT4 && !c.ftd && !c.xeng && !is_split(c) && !is_fp4(c);
+}
+
 bool use_pair(ftdx_handle h, const Strategy& strat) {
-  return strat.store_mode == 2 && pair_grid_limit(h) >= 2;
+  return (strat.store_mode & 3) == 2 && pair_grid_limit(h) >= 2;
 }
 
 // Split-K count a call actually uses: none for Kahan, the XEngine formats and
@@ -174,6 +184,7 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   const int64_t Kp = round_up(c.K, kStageK);
   const int64_t zpitch = is_split(c) ? 2 * Kp : Kp;
   const int64_t rows = int64_t(c.N) * c.batch;
+  const bool fp6 = ((strat.store_mode & kStoreFp6) || c.compute == FTDX_COMPUTE_FP6) && fp6_ok(c);
   float* qscale = reinterpret_cast<float*>(h->aux);
   float* out_scale = qscale + c.batch;
   uint32_t* amax = reinterpret_cast<uint32_t*>(out_scale + c.batch);
@@ -200,8 +211,10 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
       e = launch_ftd_to_planes(static_cast<const uint8_t*>(c.A), h->z, g, int(d.layout),
                                h->sm_count, s);
     } else if (c.input == FTDX_IN_INT4) {
-      e = launch_qc_to_planes(static_cast<const uint8_t*>(c.A), h->z, rows, c.K, int(Kp), s,
-                              pair);
+      e = fp6 ? launch_qc_to_planes6(static_cast<const uint8_t*>(c.A), h->z, rows, c.K, int(Kp),
+                                     s, pair)
+              : launch_qc_to_planes(static_cast<const uint8_t*>(c.A), h->z, rows, c.K, int(Kp),
+                                    s, pair);
     } else {
       if (c.input == FTDX_IN_FP16)
         e = launch_fp16_to_planes(c.A, h->z, rows, c.K, int(Kp), s);
@@ -213,14 +226,15 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   }
   if (e != cudaSuccess) return cuda_fail(h, e, "operand promotion launch");
   CUtensorMap tmZ;
-  st = encode_planes_map(h, h->z, rows, zpitch, &tmZ, kTile, pair ? 3 : 2);
+  st = encode_planes_map(h, h->z, rows, zpitch, &tmZ, kTile, pair ? 3 : 2, fp6);
   if (st != FTDX_OK) return st;
   HerkArgs args = herk_args_default();
   args.tiles = plan->d_tiles;
   args.chans = plan->d_chans;
   args.num_tiles = plan->num_tiles;
   args.out_fp16 = (c.output == FTDX_OUT_FP16) ? 1 : 0;
-  args.bulk_store = strat.store_mode == 1 ? 1 : 0;
+  args.bulk_store = (strat.store_mode & 3) == 1 ? 1 : 0;
+  args.fp6 = fp6 ? 1 : 0;
   args.out_format = c.out_format;
   args.out = c.C;
   args.alpha = c.alpha;
@@ -432,6 +446,9 @@ void release_graphs(ftdx_handle h) {
   h->graphs.clear();
 }
 
+// Store modes 0..2, each optionally + kStoreFp6.
+static bool valid_store_mode(int m) { return m >= 0 && (m & 3) <= 2 && (m & ~(3 | kStoreFp6)) == 0; }
+
 // Text cache, one entry per line:
 //   ftdx-tune 2 <device> <N> <Kp> <batch> <input> <output> <store_mode> <grid> <splits> <ms>
 // (version 1 lines, without <splits>, are read as splits = 1).
@@ -455,7 +472,7 @@ void load_tune_cache(ftdx_handle h) {
     if (ok && ver == 2) ok = static_cast<bool>(is >> e.st.splits);
     if (ok) ok = static_cast<bool>(is >> e.ms);
     if (!ok || magic != "ftdx-tune" || (ver != 1 && ver != 2) || (k.n < 1 && k.n != -1) ||
-        k.kp < 1 || k.batch < 1 || e.st.store_mode < 0 || e.st.store_mode > 2 || e.st.grid < 0 ||
+        k.kp < 1 || k.batch < 1 || !valid_store_mode(e.st.store_mode) || e.st.grid < 0 ||
         e.st.splits < 1 || e.st.splits > 32 || !(e.ms >= 0.f)) {
       ++h->cache_bad_lines;
       continue;
@@ -738,10 +755,10 @@ int ftdx_tuned_split_k(ftdx_handle h, int N, int K, int batch, ftdx_input input,
 
 ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid) {
   if (!h) return FTDX_ERR_INVALID_ARG;
-  if (store_mode < 0 || store_mode > 2 || grid < -1)
+  if (!valid_store_mode(store_mode) || grid < -1)
     return fail(h, FTDX_ERR_INVALID_ARG, "set_strategy: store_mode %d / grid %d", store_mode,
                 grid);
-  if (store_mode == 2) {
+  if ((store_mode & 3) == 2) {
     cudaSetDevice(h->device);
     if (pair_grid_limit(h) < 2)
       return fail(h, FTDX_ERR_UNSUPPORTED, "set_strategy: no CTA pair fits on this device");

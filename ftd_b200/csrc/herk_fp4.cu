@@ -12,12 +12,14 @@
 //
 // herk_fp4_tc_kernel: persistent tcgen05 kernel, tile = 128 column inputs j
 // (MMA M, x rows) x 64 row inputs i (MMA N = 128: their x and y rows).  TMA
-// brings per stage 128 B of K (256 E2M1 values) of A and B plus their 16
-// scale bytes per row; four scale-factor warps copy the scales into TMEM in
-// the layout tcgen05.mma kind::mxf4nvf4.block_scale expects (row m of a
-// 128-row operand at lane m%32 of every lane quarter, column m/32, byte = the
-// 16-element block within the 64-element k-step); one thread issues the
-// MMAs (M=128, N=128, K=64); four epilogue warps store the packed triangle.
+// brings per stage 128 B of K (256 E2M1 values) of A and B, and a bulk copy
+// their four 512-byte scale atoms (written in that form by the quantiser);
+// the MMA thread copies each atom into TMEM with tcgen05.cp (the layout
+// tcgen05.mma kind::mxf4nvf4.block_scale reads: row m of a 128-row operand at
+// lane m%32 of every lane quarter, column m/32, byte = the 16-element block
+// within the 64-element k-step) and issues the MMAs (M=128, N=128, K=64)
+// behind it in the same tcgen05 pipe; four epilogue warps store the packed
+// triangle.
 #include <cuda_fp4.h>
 #include <cudaTypedefs.h>
 #include <cuda_fp8.h>
@@ -39,7 +41,7 @@ constexpr int k4Stages = 5;
 constexpr int k4AccCols = 128;                // (Re, Im) column pairs of 64 inputs
 constexpr int k4SfCol0 = 2 * k4AccCols;       // TMEM columns of the scale-factor slots
 constexpr int k4SfColsPerStage = 32;          // 4 k-steps x (4 SFA + 4 SFB) columns
-constexpr int k4Threads = 320;                // TMA, MMA, 4 epilogue, 4 scale-factor warps
+constexpr int k4Threads = 192;                // TMA, MMA, 4 epilogue warps
 constexpr size_t k4Smem = 1024 + size_t(k4Stages) * k4StageBytes + 256;
 
 // E4M3 bits of a non-negative float, rounded up to the next representable
@@ -74,16 +76,37 @@ __global__ void fp4_scale_kernel(const uint32_t* __restrict__ amax_bits, int bat
   out_scale[c] = g * g;
 }
 
+// Block scales in the tcgen05 scale-factor atom: one 512-byte atom per 128
+// operand rows and k-step (64 E2M1 values = 4 blocks); row m of the group at
+// byte 16 (m % 32) + 4 (m / 32) + block.  A tcgen05.cp 32x128b.warpx4 of an
+// atom gives the TMEM layout the block-scaled MMA reads (row m at lane
+// m % 32 of every lane quarter, column m / 32, byte = block).  Groups are
+// per channel (ceil(rows_c / 128) of them), so that every tile's 128 rows are
+// one group.
+struct SfGeom {
+  int n;      // inputs per channel
+  int gA;     // groups of the x-row (A) scales per channel: ceil(n / 128)
+  int gB;     // groups of the x/y-row (B) scales per channel: ceil(2n / 128)
+  int nks;    // k-steps per row (both halves when split)
+};
+__device__ __forceinline__ int64_t sf_atom_byte(int64_t group, int nks, int ks, int m, int blk) {
+  return (group * nks + ks) * 512 + (m & 31) * 16 + ((m >> 5) & 3) * 4 + blk;
+}
+
 // One thread: one 16-value block (8 complex samples) of one input row.
 // split: each operand row holds the hi half (pitch bytes) then the lo half,
 // lo = E2M1 of the residual x - hi with its own block scale (same global
-// scale), so hi + lo carries about twice the bits; the scale rows likewise.
+// scale), so hi + lo carries about twice the bits; the scales likewise (the
+// lo k-steps follow the hi ones).  Scales go to sfa (x rows, per input) and
+// sfb (x and y rows, two per input).
 __global__ void __launch_bounds__(256) nvfp4_quantize_kernel(
-    const float2* __restrict__ a, uint8_t* __restrict__ z, uint8_t* __restrict__ sf,
-    int64_t rows, int K, int pitch, int sfpitch, int n, const float* __restrict__ gscale,
-    int split) {
+    const float2* __restrict__ a, uint8_t* __restrict__ z, uint8_t* __restrict__ sfa,
+    uint8_t* __restrict__ sfb, int64_t rows, int K, int pitch, SfGeom sg,
+    const float* __restrict__ gscale, int split) {
+  const int n = sg.n;
   const int blocks_per_row = pitch / 8;  // 8 bytes of E2M1 per block
-  const int rpitch = split ? 2 * pitch : pitch, rsf = split ? 2 * sfpitch : sfpitch;
+  const int rpitch = split ? 2 * pitch : pitch;
+  const int ksh = pitch / 32;            // k-steps per half
   const int64_t total = rows * blocks_per_row;
   for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
        idx += int64_t(gridDim.x) * blockDim.x) {
@@ -112,8 +135,13 @@ __global__ void __launch_bounds__(256) nvfp4_quantize_kernel(
     }
     *reinterpret_cast<uint2*>(z + (2 * r) * rpitch + 8 * b) = make_uint2(xw[0], xw[1]);
     *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + 8 * b) = make_uint2(yw[0], yw[1]);
-    sf[(2 * r) * rsf + b] = uint8_t(bc);
-    sf[(2 * r + 1) * rsf + b] = uint8_t(bc);
+    const int c = int(r / n), w = int(r - int64_t(c) * n);
+    const int64_t ga = int64_t(c) * sg.gA + (w >> 7);
+    const int64_t gb = int64_t(c) * sg.gB + ((2 * w) >> 7);
+    const int ks = b >> 2, blk = b & 3;
+    sfa[sf_atom_byte(ga, sg.nks, ks, w & 127, blk)] = uint8_t(bc);
+    sfb[sf_atom_byte(gb, sg.nks, ks, (2 * w) & 127, blk)] = uint8_t(bc);
+    sfb[sf_atom_byte(gb, sg.nks, ks, (2 * w + 1) & 127, blk)] = uint8_t(bc);
     if (split) {
       // residual of the hi quantisation, then its own block scale
       const float step = bc ? g * ue4m3_value(bc) : 0.f;
@@ -137,8 +165,9 @@ __global__ void __launch_bounds__(256) nvfp4_quantize_kernel(
       *reinterpret_cast<uint2*>(z + (2 * r) * rpitch + pitch + 8 * b) = make_uint2(xl[0], xl[1]);
       *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + pitch + 8 * b) =
           make_uint2(yl[0], yl[1]);
-      sf[(2 * r) * rsf + sfpitch + b] = uint8_t(bc2);
-      sf[(2 * r + 1) * rsf + sfpitch + b] = uint8_t(bc2);
+      sfa[sf_atom_byte(ga, sg.nks, ksh + ks, w & 127, blk)] = uint8_t(bc2);
+      sfb[sf_atom_byte(gb, sg.nks, ksh + ks, (2 * w) & 127, blk)] = uint8_t(bc2);
+      sfb[sf_atom_byte(gb, sg.nks, ksh + ks, (2 * w + 1) & 127, blk)] = uint8_t(bc2);
     }
   }
 }
@@ -194,6 +223,9 @@ struct Fp4Args {
   const float* chan_scale;
   uint32_t* status;
   const float* row_power;  // exact sum_t |v_t|^2 per input row (the autocorrelations)
+  const uint8_t* sfa;      // scale atoms of the x rows (A)
+  const uint8_t* sfb;      // scale atoms of the x/y rows (B)
+  int gA, gB, nks;         // SfGeom: groups per channel, k-steps per row
   // K segments (hi + lo split: hi.hi, hi.lo, lo.hi, lo.lo): segment s pairs
   // A k-blocks seg_a[s] + kk with B k-blocks seg_b[s] + kk; nseg = 1: plain
   int nseg;
@@ -202,7 +234,6 @@ struct Fp4Args {
 
 __global__ void __launch_bounds__(k4Threads, 1)
     herk_fp4_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                       const __grid_constant__ CUtensorMap tmSa, const __grid_constant__ CUtensorMap tmSb,
                        const Fp4Args args) {
   extern __shared__ uint8_t smem_dyn[];
   uint8_t* smem = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
@@ -213,7 +244,6 @@ __global__ void __launch_bounds__(k4Threads, 1)
   const uint32_t bar0 = smem_u32(bars);
   auto full_bar = [&](int s) { return bar0 + 8u * s; };
   auto empty_bar = [&](int s) { return bar0 + 8u * (k4Stages + s); };
-  auto sf_bar = [&](int s) { return bar0 + 8u * (2 * k4Stages + s); };
   auto tfull_bar = [&](int b) { return bar0 + 8u * (3 * k4Stages + b); };
   auto tempty_bar = [&](int b) { return bar0 + 8u * (3 * k4Stages + 2 + b); };
   const uint32_t done_bar = bar0 + 8u * (3 * k4Stages + 4);
@@ -227,7 +257,6 @@ __global__ void __launch_bounds__(k4Threads, 1)
     for (int s = 0; s < k4Stages; ++s) {
       mbar_init(full_bar(s), 1);
       mbar_init(empty_bar(s), 1);
-      mbar_init(sf_bar(s), 4);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(tfull_bar(b), 1);
@@ -240,8 +269,6 @@ __global__ void __launch_bounds__(k4Threads, 1)
   if (warp == 0 && lane == 0) {
     tma_prefetch_desc(&tmA);
     tma_prefetch_desc(&tmB);
-    tma_prefetch_desc(&tmSa);
-    tma_prefetch_desc(&tmSb);
   }
   if (warp == 1) {
     tmem_alloc(smem_u32(tmem_slot), 512);
@@ -263,6 +290,8 @@ __global__ void __launch_bounds__(k4Threads, 1)
         const ChanDesc cd = args.chans[td.ch];
         const int32_t rowA = int32_t(cd.row0 + int64_t(td.tj) * k4J);        // x-row view
         const int32_t rowB = int32_t(2 * (cd.row0 + int64_t(td.ti) * k4I));  // all rows
+        const uint8_t* sfA = args.sfa + (int64_t(td.ch) * args.gA + td.tj) * args.nks * 512;
+        const uint8_t* sfB = args.sfb + (int64_t(td.ch) * args.gB + td.ti) * args.nks * 512;
         for (int kb = 0; kb < cd.kblocks * args.nseg; ++kb) {
           if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
             atomicOr(args.status, kStatusTimeoutProducer);
@@ -274,8 +303,8 @@ __global__ void __launch_bounds__(k4Threads, 1)
           mbar_arrive_expect_tx(full_bar(stage), k4StageBytes);
           tma_load_2d(a_addr(stage), &tmA, ka * k4KB, rowA, full_bar(stage));
           tma_load_2d(b_addr(stage), &tmB, kbb * k4KB, rowB, full_bar(stage));
-          tma_load_2d(sfa_addr(stage), &tmSa, ka * 16, rowA, full_bar(stage));
-          tma_load_2d(sfb_addr(stage), &tmSb, kbb * 16, rowB, full_bar(stage));
+          bulk_load(sfa_addr(stage), sfA + int64_t(ka) * 4 * 512, k4Sf, full_bar(stage));
+          bulk_load(sfb_addr(stage), sfB + int64_t(kbb) * 4 * 512, k4Sf, full_bar(stage));
           ++issued;
           if (++stage == k4Stages) {
             stage = 0;
@@ -312,14 +341,19 @@ __global__ void __launch_bounds__(k4Threads, 1)
         tc_fence_after();
         const uint32_t d = tmem_base + uint32_t(acc * k4AccCols);
         for (int kb = 0; kb < cd.kblocks * args.nseg; ++kb) {
-          if (!mbar_wait(full_bar(stage), phase, abort_flag) ||
-              !mbar_wait(sf_bar(stage), phase, abort_flag)) {
+          if (!mbar_wait(full_bar(stage), phase, abort_flag)) {
             atomicOr(args.status, kStatusTimeoutMma);
             ok = false;
             break;
           }
           tc_fence_after();
           const uint32_t sf0 = tmem_base + uint32_t(k4SfCol0 + stage * k4SfColsPerStage);
+#pragma unroll
+          for (int s = 0; s < 4; ++s) {
+            tmem_cp_32x128b_warpx4(sf0 + 4 * s, sdesc_none_kmajor(sfa_addr(stage) + 512 * s, 128));
+            tmem_cp_32x128b_warpx4(sf0 + 16 + 4 * s,
+                                   sdesc_none_kmajor(sfb_addr(stage) + 512 * s, 128));
+          }
 #pragma unroll
           for (int s = 0; s < 4; ++s) {
             mma_nvf4(d, sdesc_sw128_kmajor(a_addr(stage) + 32 * s),
@@ -342,48 +376,6 @@ __global__ void __launch_bounds__(k4Threads, 1)
       mma_commit(done_bar);
       volatile int never = 0;
       if (!mbar_wait(done_bar, 0, &never)) atomicOr(args.status, kStatusTimeoutOther);
-    }
-  } else if (warp >= 6) {
-    // ------------------------------------------------ scale factors -> TMEM
-    // Warp w fills its lane quarter (w % 4) with the replicated layout: lane
-    // l, column c of a k-step holds the 4 block scales of row l + 32c.
-    const int q = warp & 3;
-    const uint32_t lane_base = uint32_t(q * 32) << 16;
-    int stage = 0;
-    uint32_t phase = 0;
-    for (int t = blockIdx.x; t < args.num_tiles; t += gridDim.x) {
-      const ChanDesc cd = args.chans[args.tiles[t].ch];
-      bool ok = true;
-      for (int kb = 0; kb < cd.kblocks * args.nseg; ++kb) {
-        ok = __all_sync(0xffffffffu, mbar_wait(full_bar(stage), phase, abort_flag));
-        if (!ok) break;
-        uint32_t wa[16], wb[16];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const uint4 va = *reinterpret_cast<const uint4*>(smem + (sfa_addr(stage) - smem0) +
-                                                           16 * (lane + 32 * c));
-          const uint4 vb = *reinterpret_cast<const uint4*>(smem + (sfb_addr(stage) - smem0) +
-                                                           16 * (lane + 32 * c));
-          wa[0 * 4 + c] = va.x; wa[1 * 4 + c] = va.y; wa[2 * 4 + c] = va.z; wa[3 * 4 + c] = va.w;
-          wb[0 * 4 + c] = vb.x; wb[1 * 4 + c] = vb.y; wb[2 * 4 + c] = vb.z; wb[3 * 4 + c] = vb.w;
-        }
-        const uint32_t col = tmem_base + lane_base + uint32_t(k4SfCol0 + stage * k4SfColsPerStage);
-        __syncwarp();
-        tmem_st_32x32b_x16(col, wa);
-        tmem_st_32x32b_x16(col + 16, wb);
-        tmem_wait_st();
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(sf_bar(stage));
-        if (++stage == k4Stages) {
-          stage = 0;
-          phase ^= 1u;
-        }
-      }
-      if (!ok) {
-        if (lane == 0) atomicOr(args.status, kStatusTimeoutOther);
-        break;
-      }
     }
   } else {
     // ------------------------------------------------ epilogue (warps 2..5)
@@ -456,9 +448,32 @@ __global__ void __launch_bounds__(k4Threads, 1)
 
 // Workspace: E2M1 operand rows (2 per input; twice as long when split), then
 // their scale bytes, then the row powers.
-size_t nvfp4_workspace_bytes(int64_t rows, int K, int split) {
-  const int64_t pitch = (2 * int64_t(K) + 255) / 256 * 128 * (split ? 2 : 1);
-  return size_t(2 * rows * pitch) + size_t(2 * rows * (pitch / 8)) + size_t(4 * rows) + 4096;
+namespace {
+// Workspace carve-up of one NVFP4 call (every part 1 KB aligned).
+struct Fp4Ws {
+  int64_t pitch, rpitch;   // E2M1 bytes per operand row: one half, whole row
+  SfGeom sg;
+  int64_t z_bytes, sfa_bytes, sfb_bytes, total;
+};
+Fp4Ws fp4_ws(int n, int batch, int K, int split) {
+  Fp4Ws w;
+  const int64_t rows = int64_t(n) * batch;
+  w.pitch = (2 * int64_t(K) + 255) / 256 * 128;
+  w.rpitch = split ? 2 * w.pitch : w.pitch;
+  w.sg = SfGeom{n, (n + 127) / 128, (2 * n + 127) / 128, int(w.rpitch / 32)};
+  auto up = [](int64_t b) { return (b + 1023) / 1024 * 1024; };
+  w.z_bytes = up(2 * rows * w.rpitch);
+  w.sfa_bytes = up(int64_t(batch) * w.sg.gA * w.sg.nks * 512);
+  w.sfb_bytes = up(int64_t(batch) * w.sg.gB * w.sg.nks * 512);
+  w.total = w.z_bytes + w.sfa_bytes + w.sfb_bytes + up(4 * rows);
+  return w;
+}
+}  // namespace
+
+// Workspace: E2M1 operand rows (2 per input; twice as long when split), the
+// scale atoms of the A and B views, the row powers.
+size_t nvfp4_workspace_bytes(int n, int batch, int K, int split) {
+  return size_t(fp4_ws(n, batch, K, split).total);
 }
 
 int nvfp4_kblocks(int K) { return int((2 * int64_t(K) + 255) / 256); }
@@ -470,14 +485,21 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
                          cudaStream_t s, int split) {
   auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(encode_fn);
   if (!encode) return cudaErrorInvalidValue;
-  const int64_t pitch = (2 * int64_t(K) + 255) / 256 * 128;  // one half (hi or lo)
-  const int64_t sfpitch = pitch / 8;
-  const int64_t rpitch = split ? 2 * pitch : pitch, rsf = split ? 2 * sfpitch : sfpitch;
+  const Fp4Ws w = fp4_ws(n, batch, K, split);
+  const int64_t pitch = w.pitch, rpitch = w.rpitch;  // one half (hi or lo), whole row
   uint8_t* z = ws;
-  uint8_t* sf = ws + ((2 * rows * rpitch + 1023) / 1024) * 1024;
-  float* power = reinterpret_cast<float*>(sf + ((2 * rows * rsf + 1023) / 1024) * 1024);
+  uint8_t* sfa = ws + w.z_bytes;
+  uint8_t* sfb = sfa + w.sfa_bytes;
+  float* power = reinterpret_cast<float*>(sfb + w.sfb_bytes);
+  // rows of a partial 128-row group get no scales from the quantiser: zero them
+  // (their products land only in outputs the epilogue skips)
+  cudaError_t e;
+  if ((n & 127) != 0) {
+    e = cudaMemsetAsync(sfa, 0, size_t(w.sfa_bytes + w.sfb_bytes), s);
+    if (e != cudaSuccess) return e;
+  }
   // row powers + channel amax (one pass) -> global scales -> quantise
-  cudaError_t e = cudaMemsetAsync(amax_bits, 0, sizeof(uint32_t) * size_t(batch), s);
+  e = cudaMemsetAsync(amax_bits, 0, sizeof(uint32_t) * size_t(batch), s);
   if (e != cudaSuccess) return e;
   {
     int bx = (n + 7) / 8;
@@ -493,13 +515,13 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
   const int64_t work = rows * (pitch / 8);
   int64_t blocks = (work + 255) / 256;
   if (blocks > int64_t(sm_count) * 16) blocks = int64_t(sm_count) * 16;
-  nvfp4_quantize_kernel<<<unsigned(blocks), 256, 0, s>>>(static_cast<const float2*>(A), z, sf,
-                                                          rows, K, int(pitch), int(sfpitch), n,
-                                                          gscale, split);
+  nvfp4_quantize_kernel<<<unsigned(blocks), 256, 0, s>>>(static_cast<const float2*>(A), z, sfa,
+                                                          sfb, rows, K, int(pitch), w.sg, gscale,
+                                                          split);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
 
-  CUtensorMap tmA, tmB, tmSa, tmSb;
+  CUtensorMap tmA, tmB;
   const cuuint32_t estr[2] = {1, 1};
   auto enc2 = [&](CUtensorMap* m, void* base, int64_t inner, int64_t nrows, int64_t stride,
                   uint32_t box0, CUtensorMapSwizzle sw) {
@@ -511,11 +533,10 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   };
   if (enc2(&tmA, z, rpitch, rows, 2 * rpitch, k4KB, CU_TENSOR_MAP_SWIZZLE_128B) != CUDA_SUCCESS ||
-      enc2(&tmB, z, rpitch, 2 * rows, rpitch, k4KB, CU_TENSOR_MAP_SWIZZLE_128B) != CUDA_SUCCESS ||
-      enc2(&tmSa, sf, rsf, rows, 2 * rsf, 16, CU_TENSOR_MAP_SWIZZLE_NONE) != CUDA_SUCCESS ||
-      enc2(&tmSb, sf, rsf, 2 * rows, rsf, 16, CU_TENSOR_MAP_SWIZZLE_NONE) != CUDA_SUCCESS)
+      enc2(&tmB, z, rpitch, 2 * rows, rpitch, k4KB, CU_TENSOR_MAP_SWIZZLE_128B) != CUDA_SUCCESS)
     return cudaErrorInvalidValue;
-  Fp4Args args{tiles, chans, num_tiles, C, alpha, beta, out_scale, status, power};
+  Fp4Args args{tiles, chans, num_tiles, C, alpha, beta, out_scale, status, power,
+               sfa, sfb, w.sg.gA, w.sg.gB, w.sg.nks};
   args.nseg = 1;
   if (split) {
     // hi.hi + hi.lo + lo.hi, lo at L k-blocks into each row; lo.lo (the square
@@ -534,7 +555,7 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
     attr = true;
   }
   const int grid = num_tiles < sm_count ? num_tiles : sm_count;
-  herk_fp4_tc_kernel<<<grid, k4Threads, k4Smem, s>>>(tmA, tmB, tmSa, tmSb, args);
+  herk_fp4_tc_kernel<<<grid, k4Threads, k4Smem, s>>>(tmA, tmB, args);
   return cudaGetLastError();
 }
 

@@ -78,6 +78,62 @@ __global__ void __launch_bounds__(256) qc_to_planes_kernel(const uint8_t* __rest
   }
 }
 
+// FP6 operand planes: as qc_to_planes_kernel, but each plane row holds Kp
+// E3M2 codes packed 16 per 12 bytes (row pitch 3 Kp / 4 bytes), the global
+// form of the TMA's 16 x U6 type.  Exact for QC input, 3/4 of the FP8 bytes.
+__global__ void __launch_bounds__(256) qc_to_planes6_kernel(const uint8_t* __restrict__ qc,
+                                                            uint8_t* __restrict__ z, int64_t rows,
+                                                            int K, int Kp, int rows_per_block,
+                                                            int neg_plane) {
+  const int chunks = Kp >> 4;
+  const int64_t pitch = int64_t(Kp) * 3 / 4;
+  const int64_t r0 = int64_t(blockIdx.x) * rows_per_block;
+  const int64_t nrows64 = rows - r0 < rows_per_block ? rows - r0 : rows_per_block;
+  const int nloc = int(nrows64) * chunks;
+  const int64_t plane = rows * pitch;
+  const bool vec = ((K & 15) == 0) && ((reinterpret_cast<uintptr_t>(qc) & 15) == 0);
+  for (int l = threadIdx.x; l < nloc; l += blockDim.x) {
+    const int rl = l / chunks;
+    const int g = l - rl * chunks;
+    const int t0 = g << 4;
+    const int64_t r = r0 + rl;
+    const uint8_t* src = qc + r * K + t0;
+    uint32_t w[4];
+    if (vec && t0 + 16 <= K) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(src));
+      w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        uint32_t acc = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int t = t0 + 4 * q + b;
+          const uint32_t byte = (t < K) ? uint32_t(__ldg(src + 4 * q + b)) : 0u;
+          acc |= byte << (8 * b);
+        }
+        w[q] = acc;
+      }
+    }
+    uint32_t re[4], im[4], pr[3], pi[3];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) qc4_to_e3m2(w[q], re[q], im[q]);
+    pack16_u6(re, pr);
+    pack16_u6(im, pi);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(z + r * pitch + 12 * g);
+    dst[0] = pr[0], dst[1] = pr[1], dst[2] = pr[2];
+    uint32_t* dsti = reinterpret_cast<uint32_t*>(z + plane + r * pitch + 12 * g);
+    dsti[0] = pi[0], dsti[1] = pi[1], dsti[2] = pi[2];
+    if (neg_plane) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) re[q] ^= 0x20202020u;
+      pack16_u6(re, pr);
+      uint32_t* dstn = reinterpret_cast<uint32_t*>(z + 2 * plane + r * pitch + 12 * g);
+      dstn[0] = pr[0], dstn[1] = pr[1], dstn[2] = pr[2];
+    }
+  }
+}
+
 // Plane 2 = plane 0 with every E4M3 sign flipped (-Re), for inputs whose
 // promotion kernel writes two planes.  n16 = plane bytes / 16.
 __global__ void __launch_bounds__(256) negate_plane_kernel(uint4* __restrict__ z, int64_t n16) {
@@ -394,7 +450,8 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
           const int sb = seg == 0 ? args.seg_b[0] : (seg == 1 ? args.seg_b[1] : args.seg_b[2]);
           const int32_t kA = (sa + cd.kb0 + kk) * kStageK, kB = (sb + cd.kb0 + kk) * kStageK;
           const bool share = diag && sa == sb;
-          mbar_arrive_expect_tx(full_bar(stage), share ? 2 * kPlaneBytes : kStageBytes);
+          const uint32_t bytes = share ? 2 * kPlaneBytes : kStageBytes;  // FP8 planes
+          mbar_arrive_expect_tx(full_bar(stage), args.fp6 ? bytes / 4 * 3 : bytes);
           tma_load_3d(plane_addr(stage, 0), &tmZ, kA, rowJ, 0, full_bar(stage));
           tma_load_3d(plane_addr(stage, 1), &tmZ, kA, rowJ, 1, full_bar(stage));
           if (!share) {
@@ -425,8 +482,9 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   } else if (warp == 1) {
     // ------------------------------------------------ MMA issuer
     if (lane == 0) {
-      constexpr uint32_t idesc = idesc_f32acc(0, 0, kTile, kTile);
-      constexpr uint32_t idesc_neg = idesc_f32acc(0, 0, kTile, kTile, 1);
+      const uint32_t fmt = args.fp6 ? kFmtE3M2 : kFmtE4M3;
+      const uint32_t idesc = idesc_f32acc(fmt, fmt, kTile, kTile);
+      const uint32_t idesc_neg = idesc_f32acc(fmt, fmt, kTile, kTile, 1);
       int stage = 0;
       uint32_t phase = 0;
       int acc = 0;
@@ -755,7 +813,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
           const int sa = seg == 0 ? args.seg_a[0] : (seg == 1 ? args.seg_a[1] : args.seg_a[2]);
           const int sb = seg == 0 ? args.seg_b[0] : (seg == 1 ? args.seg_b[1] : args.seg_b[2]);
           const int32_t kA = (sa + cd.kb0 + kk) * kStageK, kB = (sb + cd.kb0 + kk) * kStageK;
-          if (leader) mbar_arrive_expect_tx(full_bar(stage), 2 * kPairStageBytes);
+          if (leader)  // both CTAs' loads; packed FP6 planes deliver 3/4 of the bytes
+            mbar_arrive_expect_tx(full_bar(stage), args.fp6 ? 2 * kPairStageBytes / 4 * 3
+                                                            : 2 * kPairStageBytes);
           const uint32_t fb = map_shared(full_bar(stage), 0);
           tma_load_3d_pair(plane(stage, 0), &tmZ, kA, rowJ, 0, fb);
           tma_load_3d_pair(plane(stage, 1), &tmZ, kA, rowJ, 1, fb);
@@ -772,7 +832,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
   } else if (warp == 1) {
     // ------------------------------------------------ MMA issuer (leader CTA)
     if (lane == 0 && leader) {
-      constexpr uint32_t idesc = idesc_f32acc(0, 0, 256, 2 * kTile);
+      const uint32_t fmt = args.fp6 ? kFmtE3M2 : kFmtE4M3;
+      const uint32_t idesc = idesc_f32acc(fmt, fmt, 256, 2 * kTile);
       int stage = 0, acc = 0;
       uint32_t phase = 0, acc_phase = 0;
       bool ok = true;
@@ -908,6 +969,15 @@ cudaError_t launch_qc_to_planes(const uint8_t* qc, uint8_t* z, int64_t rows, int
   const int rpb = rows_per_block(Kp >> 4);
   const int64_t blocks = (rows + rpb - 1) / rpb;
   qc_to_planes_kernel<<<unsigned(blocks), 256, 0, s>>>(qc, z, rows, K, Kp, rpb, neg_plane ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_qc_to_planes6(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
+                                 cudaStream_t s, bool neg_plane) {
+  const int rpb = rows_per_block(Kp >> 4);
+  const int64_t blocks = (rows + rpb - 1) / rpb;
+  qc_to_planes6_kernel<<<unsigned(blocks), 256, 0, s>>>(qc, z, rows, K, Kp, rpb,
+                                                         neg_plane ? 1 : 0);
   return cudaGetLastError();
 }
 

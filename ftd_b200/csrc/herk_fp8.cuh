@@ -100,6 +100,9 @@ struct HerkArgs {
   int32_t kahan;            // 1: Kahan-accumulate into out (sum) and out2 (compensation)
   const float* chan_scale;  // per-channel result multiplier (nullptr: 1)
   void* out2;
+  // 1: Z holds packed FP6 E3M2 planes (TMA 16 x U6 type): the MMAs read E3M2
+  // operands and each load delivers 3/4 of the FP8 bytes
+  int32_t fp6;
 };
 
 // A plain single-segment argument block.
@@ -114,6 +117,9 @@ inline HerkArgs herk_args_default() {
 // neg_plane: also write plane 2 = -Re (CTA-pair kernel operand)
 cudaError_t launch_qc_to_planes(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
                                 cudaStream_t s, bool neg_plane = false);
+// Packed FP6 E3M2 planes (row pitch 3 Kp / 4 bytes) for the fp6 operand form.
+cudaError_t launch_qc_to_planes6(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
+                                 cudaStream_t s, bool neg_plane = false);
 // Raw packet-ordered QC input (corner_turn.cu): geometry of the promotion.
 struct FtdGeom {
   int n_ant, n_chan, n_pol, n_ti;  // antennas, channels, polarisations, time_inner
@@ -166,7 +172,7 @@ cudaError_t launch_channel_amax(const void* a, int64_t per_chan, int batch, uint
                                 int sm_count, cudaStream_t s);
 // NVFP4 correlator for float complex input (herk_fp4.cu).  Tiles: ti over 64
 // row inputs, tj over 128 column inputs; kblocks = nvfp4_kblocks(K).
-size_t nvfp4_workspace_bytes(int64_t rows, int K, int split = 0);
+size_t nvfp4_workspace_bytes(int n, int batch, int K, int split = 0);
 int nvfp4_kblocks(int K);
 cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, uint8_t* ws,
                          float* gscale, float* out_scale, uint32_t* amax_bits,

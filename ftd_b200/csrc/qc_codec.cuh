@@ -21,6 +21,37 @@ __device__ __forceinline__ void qc4_to_e4m3(uint32_t w, uint32_t& re, uint32_t& 
   im = __byte_perm(kLo, kHi, si) | ((w << 4) & 0x80808080u);
 }
 
+// Four QC bytes -> FP6 E3M2 codes (one per byte, bits 5:0) of the four Re
+// and the four Im parts.  E3M2 (bias 3, two mantissa bits) holds the integers
+// 0..7 exactly: codes 00 0C 10 12 14 15 16 17; the sign is bit 5.
+__device__ __forceinline__ void qc4_to_e3m2(uint32_t w, uint32_t& re, uint32_t& im) {
+  constexpr uint32_t kLo = 0x12100C00u, kHi = 0x17161514u;
+  const uint32_t mr = (w >> 4) & 0x07070707u;
+  const uint32_t mi = w & 0x07070707u;
+  uint32_t sr = mr | (mr >> 4);
+  sr = (sr & 0xFFu) | ((sr >> 8) & 0xFF00u);
+  uint32_t si = mi | (mi >> 4);
+  si = (si & 0xFFu) | ((si >> 8) & 0xFF00u);
+  re = __byte_perm(kLo, kHi, sr) | ((w >> 2) & 0x20202020u);
+  im = __byte_perm(kLo, kHi, si) | ((w << 2) & 0x20202020u);
+}
+
+// Sixteen 6-bit codes (one per byte of c[0..3], byte b of c[q] = element
+// 4q + b) -> the 12-byte packed group of the TMA's 16 x U6 type: element e at
+// bits [6e, 6e + 6) of the little-endian 96-bit group.
+__device__ __forceinline__ void pack16_u6(const uint32_t (&c)[4], uint32_t (&p)[3]) {
+  uint32_t t[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const uint32_t w = c[q];
+    t[q] = (w & 0x3Fu) | (((w >> 8) & 0x3Fu) << 6) | (((w >> 16) & 0x3Fu) << 12) |
+           (((w >> 24) & 0x3Fu) << 18);
+  }
+  p[0] = t[0] | (t[1] << 24);
+  p[1] = (t[1] >> 8) | (t[2] << 16);
+  p[2] = (t[2] >> 16) | (t[3] << 8);
+}
+
 // Four (4,4)b two's-complement bytes (low nibble Re, high nibble Im, each in
 // [-8, 7]: the XEngine's packet format, promote_data.cuh:66-67) -> E4M3 bytes
 // of the Re and of the Im parts.  Nibbles 0..7 are 0..7; 8..15 are -8..-1,

@@ -111,6 +111,17 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* m, 
       : "memory");
 }
 
+// Bulk copy global -> shared (async proxy), completing on mbarrier `bar`.
+// Addresses 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_load(uint32_t sdst, const void* gsrc, uint32_t bytes,
+                                          uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(sdst),
+      "l"(gsrc), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
 // Bulk copy shared -> global (async proxy).  Addresses 16-byte aligned,
 // size a multiple of 16.
 __device__ __forceinline__ void bulk_store(void* gdst, uint32_t ssrc, uint32_t bytes) {
@@ -340,10 +351,31 @@ __device__ __forceinline__ uint64_t sdesc_sw128_kmajor(uint32_t saddr) {
   return d;
 }
 
+// Descriptor of an unswizzled K-major shared-memory source: rows of 16 bytes
+// back to back, 8-row core matrices `sbo` bytes apart (tcgen05.cp sources).
+__device__ __forceinline__ uint64_t sdesc_none_kmajor(uint32_t saddr, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4);  // start address  [0,14)
+  d |= static_cast<uint64_t>(sbo >> 4) << 16;            // LBO (one core matrix along K)
+  d |= static_cast<uint64_t>(sbo >> 4) << 32;            // SBO: 8-row core-matrix stride
+  d |= static_cast<uint64_t>(1) << 46;                   // descriptor version (sm100)
+  return d;                                              // layout 0: no swizzle
+}
+
+// Shared memory -> TMEM: 32 rows of 128 bits into lanes 0..31 of columns
+// taddr..taddr+3, replicated into all four lane quarters.  Ordered before the
+// tcgen05.mma this thread issues next.
+__device__ __forceinline__ void tmem_cp_32x128b_warpx4(uint32_t taddr, uint64_t sdesc) {
+  asm volatile("tcgen05.cp.cta_group::1.32x128b.warpx4 [%0], %1;" ::"r"(taddr), "l"(sdesc)
+               : "memory");
+}
+
 // Instruction descriptor for kind::f8f6f4 / kind::f16 dense MMA with FP32
 // accumulation and K-major A and B.
 //   a_fmt/b_fmt: f8f6f4 -> 0 = E4M3; f16 -> 0 = F16, 1 = BF16.
 //   neg_a: negate A (valid for kind::f16 and kind::f8f6f4).
+// kind::f8f6f4 operand formats (instruction descriptor a/b format fields).
+constexpr uint32_t kFmtE4M3 = 0, kFmtE3M2 = 4;
 __host__ __device__ constexpr uint32_t idesc_f32acc(uint32_t a_fmt, uint32_t b_fmt, uint32_t M,
                                                     uint32_t N, uint32_t neg_a = 0) {
   return (1u << 4)                 // D format: F32

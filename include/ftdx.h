@@ -60,7 +60,8 @@ typedef enum ftdx_input {
 typedef enum ftdx_compute {
   FTDX_COMPUTE_FP8 = 0,        /* INT4: exact; FP16: unscaled E4M3 (as the reference);
                                   FP32: E4M3 with a per-channel scale */
-  FTDX_COMPUTE_FP6 = 1,
+  FTDX_COMPUTE_FP6 = 1,        /* INT4 input only: E3M2 operands (every QC value exact), so
+                                  the result equals FP8's; other inputs: UNSUPPORTED */
   FTDX_COMPUTE_FP4 = 2,        /* NVFP4: E2M1 with one E4M3 scale per 16 values (FP32 input) */
   FTDX_COMPUTE_FP8_SPLIT = 3,  /* FP32 input: hi + lo E4M3, hi.hi^H + hi.lo^H + lo.hi^H */
   FTDX_COMPUTE_FP4_SPLIT = 4   /* FP32 input: hi + lo NVFP4 (lo = NVFP4 of the residual, own

@@ -74,6 +74,15 @@ int main() {
     printf("CutlassComplexGemm::herk rc=%d mismatch=%d\n", rc, int(got != ref));
     ++fails;
   }
+  // FP6 compute on INT4 input: E3M2 operands, exact, so the same triangles
+  cudaMemset(d_c, 0, B * P * 8);
+  rc = api.herk(d_qc, d_c, N, K, B, InputPrecision::INT4, ComputePrecision::FP6,
+                OutputPrecision::FP32, OutputFormat::PackedTriangle, 1.0f, 0.0f, nullptr, false);
+  cudaMemcpy(got.data(), d_c, B * P * 8, cudaMemcpyDeviceToHost);
+  if (rc != 0 || got != ref) {
+    printf("CutlassComplexGemm::herk FP6 rc=%d mismatch=%d\n", rc, int(got != ref));
+    ++fails;
+  }
   // FP4 compute is not provided by this entry point: a non-zero status, no throw
   if (api.herk(d_qc, d_c, N, K, B, InputPrecision::INT4, ComputePrecision::FP4,
                OutputPrecision::FP32) == 0) {
