@@ -629,8 +629,8 @@ def run_precision_leg(torch, dev, N=4096, B=64, K=1024, seed=4, n_err=512):
         for name, mode in [("fp8_channel_scaled", COMPUTE_FP8), ("fp8_hi_lo_split", COMPUTE_FP8_SPLIT),
                            ("nvfp4_block16", COMPUTE_FP4),
                            ("nvfp4_hi_lo_split", COMPUTE_FP4_SPLIT)]:
-            def step():
-                c.herk(V, C, N, K, B, input=IN_FP32, compute=mode, output=OUT_FP32, tune=False)
+            def step():  # autotuned per mode: the sweep runs in the first (untimed) call
+                c.herk(V, C, N, K, B, input=IN_FP32, compute=mode, output=OUT_FP32, tune=True)
             ms = _timed(torch, step)
             if c.device_status() != 0:
                 raise RuntimeError("device wait timed out in the precision leg")
@@ -717,10 +717,11 @@ def run_e2e(torch, args, dev, qc_dev, N, K, B, flops, world, dist):
                     "host wall time"}
 
 
-def run_nvfp4_case(torch, dev, N, K, B, reps=5, seed=1, split=False):
+def run_nvfp4_case(torch, dev, N, K, B, reps=5, seed=1, split=False, store_mode=None):
     """NVFP4 correlation of seeded Gaussian FP32 complex voltages [B][N][K]:
-    reps calls, the whole FP4 path (amax, quantisation, row power, correlator)
-    timed with CUDA events.  split: the hi + lo mode (four products)."""
+    reps calls, the whole FP4 path (statistics, quantisation, correlator)
+    timed with CUDA events.  split: the hi + lo mode (three products).
+    store_mode 0 / 2: single-CTA / CTA-pair kernel (None: autotuned)."""
     from ftd_b200 import Correlator, tri_size
     from ftd_b200._lib import COMPUTE_FP4, COMPUTE_FP4_SPLIT, IN_FP32, OUT_FP32
     mode = COMPUTE_FP4_SPLIT if split else COMPUTE_FP4
@@ -728,12 +729,20 @@ def run_nvfp4_case(torch, dev, N, K, B, reps=5, seed=1, split=False):
     A = torch.randn(B, N, K, 2, device=dev, generator=g)
     C = torch.empty(B, tri_size(N), 2, device=dev)
     with Correlator(device=dev.index) as c:
+        if store_mode is not None:
+            c.set_strategy(store_mode, 0)
+        tune = store_mode is None
+        c.herk(A, C, N, K, B, input=IN_FP32, compute=mode, output=OUT_FP32, tune=tune)
         ms = _timed(torch, lambda: c.herk(A, C, N, K, B, input=IN_FP32, compute=mode,
-                                          output=OUT_FP32, tune=False), reps=reps)
+                                          output=OUT_FP32, tune=tune), reps=reps)
+        tuned = c.lookup_tuned(N, K, B, input=IN_FP32, output=OUT_FP32) if tune else None
         if c.device_status() != 0:
             raise RuntimeError("device status after the NVFP4 case")
+    kernel = ("herk_fp4_pair_kernel" if (store_mode if store_mode is not None else
+                                         (tuned or {}).get("store_mode", 0)) == 2
+              else "herk_fp4_tc_kernel")
     return {"workload": f"NVFP4{' hi+lo' if split else ''}: {N} inputs x {B} channels x K={K}, "
-                        f"Gaussian FP32 complex",
+                        f"Gaussian FP32 complex", "kernel": kernel,
             "value": herk_flops(N, K, B) / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms}
 
 
@@ -742,9 +751,12 @@ def run_leg(args):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
     if args.leg == "nvfp4":
-        out = run_nvfp4_case(torch, dev, args.inputs, args.k, args.channels)
+        sm = int(args.strategy.split(",")[0]) if args.strategy else None
+        out = run_nvfp4_case(torch, dev, args.inputs, args.k, args.channels, store_mode=sm)
     elif args.leg == "nvfp4split":
-        out = run_nvfp4_case(torch, dev, args.inputs, args.k, args.channels, split=True)
+        sm = int(args.strategy.split(",")[0]) if args.strategy else None
+        out = run_nvfp4_case(torch, dev, args.inputs, args.k, args.channels, split=True,
+                             store_mode=sm)
     elif args.leg == "raw":
         out = run_ftd_leg(torch, dev)
     elif args.leg == "imaging":

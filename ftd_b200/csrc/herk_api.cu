@@ -74,12 +74,13 @@ ftdx_status validate(ftdx_handle h, const HerkCall& c, ftdx_compute compute, ftd
   return FTDX_OK;
 }
 
-// Tile plan of the NVFP4 kernel: ti over 64 row inputs, tj over 128 column
-// inputs, tiles holding at least one j <= i.  Cached with a negative kblocks
-// key so it never collides with the FP8 plans.
+// Tile plan of the NVFP4 kernels, tiles holding at least one j <= i: single
+// CTA: ti over 64 row inputs, tj over 128 column inputs; pair: ti over 112,
+// tj over 256 (nvfp4_pair_tiles).  Cached with a negative kblocks key so it
+// never collides with the FP8 plans.
 ftdx_status get_fp4_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
-                         const Plan** out) {
-  const auto key = std::make_tuple(N, -1 - kblocks, batch);
+                         const Plan** out, bool pair) {
+  const auto key = std::make_tuple(N, -1 - kblocks - (pair ? (1 << 24) : 0), batch);
   auto it = h->plans.find(key);
   if (it != h->plans.end()) {
     *out = it->second.get();
@@ -92,6 +93,10 @@ ftdx_status get_fp4_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStrea
   std::vector<TileDesc> tiles;
   for (int c = 0; c < batch; ++c) {
     chans[c] = ChanDesc{N, kblocks, int64_t(c) * N, int64_t(c) * (int64_t(N) * (N + 1) / 2), 0};
+    if (pair) {
+      nvfp4_pair_tiles(N, c, tiles);
+      continue;
+    }
     for (int ti = 0; ti < ni; ++ti)
       for (int tj = 0; tj < nj && tj * 128 <= ti * 64 + 63; ++tj)
         tiles.push_back(TileDesc{c, uint16_t(ti), uint16_t(tj)});
@@ -113,13 +118,16 @@ ftdx_status get_fp4_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStrea
   return FTDX_OK;
 }
 
-ftdx_status launch_fp4(ftdx_handle h, const HerkCall& c, cudaStream_t s) {
+// store mode 2 (the CTA-pair strategy) selects the NVFP4 pair kernel too.
+ftdx_status launch_fp4(ftdx_handle h, const HerkCall& c, const Strategy& strat, cudaStream_t s) {
   const int64_t rows = int64_t(c.N) * c.batch;
   const int split = c.compute == FTDX_COMPUTE_FP4_SPLIT ? 1 : 0;
-  ftdx_status st = ensure_workspace(h, nvfp4_workspace_bytes(c.N, c.batch, c.K, split), s);
+  const int pair = ((strat.store_mode & 3) == 2 && nvfp4_pair_limit() >= 1) ? 1 : 0;
+  ftdx_status st = ensure_workspace(h, nvfp4_workspace_bytes(c.N, c.batch, c.K, split, pair), s);
   if (st == FTDX_OK) st = ensure_aux(h, size_t(12) * size_t(c.batch) + 256, s);
   const Plan* plan = nullptr;
-  if (st == FTDX_OK) st = get_fp4_plan(h, c.N, nvfp4_kblocks(c.K), c.batch, s, &plan);
+  if (st == FTDX_OK)
+    st = get_fp4_plan(h, c.N, nvfp4_kblocks(c.K), c.batch, s, &plan, pair != 0);
   if (st != FTDX_OK) return st;
   float* gscale = reinterpret_cast<float*>(h->aux);
   float* out_scale = gscale + c.batch;
@@ -129,7 +137,7 @@ ftdx_status launch_fp4(ftdx_handle h, const HerkCall& c, cudaStream_t s) {
     ScopedTimer tm(h, s, 0);
     e = launch_nvfp4(c.A, rows, c.K, c.N, c.batch, h->z, gscale, out_scale, amax,
                      plan->d_tiles, plan->d_chans, plan->num_tiles, c.C, c.alpha, c.beta,
-                     h->d_status, h->sm_count, tensor_map_encoder(), s, split);
+                     h->d_status, h->sm_count, tensor_map_encoder(), s, split, pair);
   }
   return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "NVFP4 launch");
 }
@@ -175,7 +183,7 @@ ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan
 
 // Promotion kernel + correlator kernel on stream s.
 ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, cudaStream_t s) {
-  if (is_fp4(c)) return launch_fp4(h, c, s);
+  if (is_fp4(c)) return launch_fp4(h, c, strat, s);
   const bool pair = use_pair(h, strat);
   const int splits = effective_splits(c, strat);
   const Plan* plan = nullptr;
@@ -299,7 +307,11 @@ ftdx_status run_tune(ftdx_handle h, const HerkCall& c, cudaStream_t s, TuneEntry
   ftdx_status st = prepare(h, c, s, &plan);
   if (st != FTDX_OK) return st;
   TuneEntry best;
-  std::vector<Strategy> cands = default_candidates(h, c.output == FTDX_OUT_FP32, !is_fp4(c));
+  // NVFP4: the single-CTA and the pair kernel (store modes and grids do not apply)
+  std::vector<Strategy> cands =
+      is_fp4(c) ? std::vector<Strategy>{Strategy{0, h->sm_count}}
+                : default_candidates(h, c.output == FTDX_OUT_FP32, true);
+  if (is_fp4(c) && nvfp4_pair_limit() >= 1) cands.push_back(Strategy{2, 0});
   const int kblocks = int(round_up(c.K, kStageK) / kStageK);
   if (!is_fp4(c) && !c.comp && plan->num_tiles < h->sm_count)
     for (int sp : {2, 4, 8, 16, 32})

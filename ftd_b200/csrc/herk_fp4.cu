@@ -81,16 +81,21 @@ __global__ void fp4_scale_kernel(const uint32_t* __restrict__ amax_bits, int bat
 // byte 16 (m % 32) + 4 (m / 32) + block.  A tcgen05.cp 32x128b.warpx4 of an
 // atom gives the TMEM layout the block-scaled MMA reads (row m at lane
 // m % 32 of every lane quarter, column m / 32, byte = block).  Groups are
-// per channel (ceil(rows_c / 128) of them), so that every tile's 128 rows are
-// one group.
+// per channel and follow the kernel's tiles, so that one tile's rows are one
+// group: A groups of 128 x rows; B groups of `gbrows` x/y rows (128 for the
+// single-CTA kernel, 224 for the CTA pair), stored as `nsub` consecutive
+// atoms per k-step (rows 0..127, 128..255 of the group).
 struct SfGeom {
-  int n;      // inputs per channel
-  int gA;     // groups of the x-row (A) scales per channel: ceil(n / 128)
-  int gB;     // groups of the x/y-row (B) scales per channel: ceil(2n / 128)
-  int nks;    // k-steps per row (both halves when split)
+  int n;       // inputs per channel
+  int gA;      // A groups per channel
+  int gB;      // B groups per channel
+  int nks;     // k-steps per row (both halves when split)
+  int gbrows;  // operand rows per B group
+  int nsub;    // atoms per B group and k-step: ceil(gbrows / 128)
 };
-__device__ __forceinline__ int64_t sf_atom_byte(int64_t group, int nks, int ks, int m, int blk) {
-  return (group * nks + ks) * 512 + (m & 31) * 16 + ((m >> 5) & 3) * 4 + blk;
+__device__ __forceinline__ int64_t sf_atom_byte(int64_t group, int nks, int nsub, int ks, int m,
+                                                int blk) {
+  return ((group * nks + ks) * nsub + (m >> 7)) * 512 + (m & 31) * 16 + ((m >> 5) & 3) * 4 + blk;
 }
 
 // One thread: one 16-value block (8 complex samples) of one input row.
@@ -137,11 +142,12 @@ __global__ void __launch_bounds__(256) nvfp4_quantize_kernel(
     *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + 8 * b) = make_uint2(yw[0], yw[1]);
     const int c = int(r / n), w = int(r - int64_t(c) * n);
     const int64_t ga = int64_t(c) * sg.gA + (w >> 7);
-    const int64_t gb = int64_t(c) * sg.gB + ((2 * w) >> 7);
+    const int64_t gb = int64_t(c) * sg.gB + (2 * w) / sg.gbrows;
+    const int ob = (2 * w) % sg.gbrows;  // x row in the group; y row next (gbrows is even)
     const int ks = b >> 2, blk = b & 3;
-    sfa[sf_atom_byte(ga, sg.nks, ks, w & 127, blk)] = uint8_t(bc);
-    sfb[sf_atom_byte(gb, sg.nks, ks, (2 * w) & 127, blk)] = uint8_t(bc);
-    sfb[sf_atom_byte(gb, sg.nks, ks, (2 * w + 1) & 127, blk)] = uint8_t(bc);
+    sfa[sf_atom_byte(ga, sg.nks, 1, ks, w & 127, blk)] = uint8_t(bc);
+    sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ks, ob, blk)] = uint8_t(bc);
+    sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ks, ob + 1, blk)] = uint8_t(bc);
     if (split) {
       // residual of the hi quantisation, then its own block scale
       const float step = bc ? g * ue4m3_value(bc) : 0.f;
@@ -165,9 +171,9 @@ __global__ void __launch_bounds__(256) nvfp4_quantize_kernel(
       *reinterpret_cast<uint2*>(z + (2 * r) * rpitch + pitch + 8 * b) = make_uint2(xl[0], xl[1]);
       *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + pitch + 8 * b) =
           make_uint2(yl[0], yl[1]);
-      sfa[sf_atom_byte(ga, sg.nks, ksh + ks, w & 127, blk)] = uint8_t(bc2);
-      sfb[sf_atom_byte(gb, sg.nks, ksh + ks, (2 * w) & 127, blk)] = uint8_t(bc2);
-      sfb[sf_atom_byte(gb, sg.nks, ksh + ks, (2 * w + 1) & 127, blk)] = uint8_t(bc2);
+      sfa[sf_atom_byte(ga, sg.nks, 1, ksh + ks, w & 127, blk)] = uint8_t(bc2);
+      sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ksh + ks, ob, blk)] = uint8_t(bc2);
+      sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ksh + ks, ob + 1, blk)] = uint8_t(bc2);
     }
   }
 }
@@ -444,6 +450,252 @@ __global__ void __launch_bounds__(k4Threads, 1)
   }
 }
 
+// ---------------------------------------------------------------- CTA pair
+// herk_fp4_pair_kernel: the same product on a CTA pair (cluster of 2), as the
+// FP8 pair kernel.  Tile = 256 column inputs j (MMA M = 256: 128 x rows per
+// CTA) x 112 row inputs i (MMA N = 224: their x and y rows, 112 per CTA), so
+// each CTA's shared memory feeds twice the MMA work per operand byte of the
+// single-CTA kernel.  Every load of both CTAs completes on the leader's full
+// barrier; the leader's MMA thread copies each stage's scale atoms into both
+// CTAs' TMEM (tcgen05.cp.cta_group::2: each CTA from its own shared memory;
+// SFA = its own 128 rows, SFB = all 224 rows, loaded by both) and issues the
+// MMAs behind them in the same pipe, so one TMEM scale slot per stage
+// suffices: 2 x 224 accumulator columns + 16 SFA + 32 SFB columns of 512.
+constexpr int k4pJ = 256;                     // j inputs per pair tile
+constexpr int k4pI = 112;                     // i inputs per pair tile
+constexpr int k4pN = 2 * k4pI;                // MMA N: x/y rows of the i inputs
+constexpr int k4pA = 128 * k4KB;              // 16 KB: this CTA's 128 x rows
+constexpr int k4pB = k4pI * k4KB;             // 14 KB: this CTA's 112 x/y rows
+constexpr int k4pSfa = 4 * 512;               // 4 k-steps x one atom
+constexpr int k4pSfb = 4 * 2 * 512;           // 4 k-steps x two atoms (224 rows)
+constexpr int k4pStageBytes = k4pA + k4pB + k4pSfa + k4pSfb;  // 36 KB (multiple of 1 KB)
+constexpr int k4pStages = 6;
+constexpr int k4pAccCols = k4pN;              // one accumulator: 224 columns
+constexpr int k4pSfaCol = 2 * k4pAccCols;     // 448: 4 k-steps x 4 columns
+constexpr int k4pSfbCol = k4pSfaCol + 16;     // 464: 4 k-steps x 8 columns (..495)
+constexpr int k4pThreads = 192;               // TMA, MMA, 4 epilogue warps
+constexpr size_t k4pSmem = 1024 + size_t(k4pStages) * k4pStageBytes + 256;
+static_assert(k4pSfbCol + 32 <= 512, "TMEM columns");
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(k4pThreads, 1)
+    herk_fp4_pair_kernel(const __grid_constant__ CUtensorMap tmA,
+                         const __grid_constant__ CUtensorMap tmB,
+                         const __grid_constant__ CUtensorMap tmSa,
+                         const __grid_constant__ CUtensorMap tmSb, const Fp4Args args) {
+  extern __shared__ uint8_t smem_dyn[];
+  uint8_t* smem = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + k4pStages * k4pStageBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * k4pStages + 5);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const uint32_t smem0 = smem_u32(smem);
+  const uint32_t bar0 = smem_u32(bars);
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (k4pStages + s); };
+  auto tfull_bar = [&](int b) { return bar0 + 8u * (2 * k4pStages + b); };
+  auto tempty_bar = [&](int b) { return bar0 + 8u * (2 * k4pStages + 2 + b); };
+  const uint32_t done_bar = bar0 + 8u * (2 * k4pStages + 4);
+  auto a_addr = [&](int s) { return smem0 + uint32_t(s * k4pStageBytes); };
+  auto b_addr = [&](int s) { return smem0 + uint32_t(s * k4pStageBytes + k4pA); };
+  auto sfa_addr = [&](int s) { return smem0 + uint32_t(s * k4pStageBytes + k4pA + k4pB); };
+  auto sfb_addr = [&](int s) {
+    return smem0 + uint32_t(s * k4pStageBytes + k4pA + k4pB + k4pSfa);
+  };
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+  const int pair = int(blockIdx.x >> 1), npairs = int(gridDim.x >> 1);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < k4pStages; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(tfull_bar(b), 1);
+      mbar_init(tempty_bar(b), 2 * 4);  // the epilogue warps of both CTAs
+    }
+    mbar_init(done_bar, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    tma_prefetch_desc(&tmA);
+    tma_prefetch_desc(&tmB);
+    tma_prefetch_desc(&tmSa);
+    tma_prefetch_desc(&tmSb);
+  }
+  if (warp == 1) {
+    tmem_alloc_pair(smem_u32(tmem_slot), 512);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // both CTAs' barriers exist before any cross-CTA signal
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------------------------ TMA producer (both CTAs)
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      for (int t = pair; t < args.num_tiles; t += npairs) {
+        const TileDesc td = args.tiles[t];
+        const ChanDesc cd = args.chans[td.ch];
+        const int32_t rowA = int32_t(cd.row0 + int64_t(td.tj) * k4pJ + 128 * rank);  // x rows
+        const int32_t rowB = int32_t(2 * cd.row0 + int64_t(td.ti) * k4pN + k4pI * rank);
+        const int64_t ga = int64_t(td.ch) * args.gA + 2 * int64_t(td.tj) + rank;
+        const int64_t gb = int64_t(td.ch) * args.gB + td.ti;
+        bool ok = true;
+        for (int kb = 0; kb < cd.kblocks * args.nseg; ++kb) {
+          if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
+            atomicOr(args.status, kStatusTimeoutProducer);
+            ok = false;
+            break;
+          }
+          const int seg = kb / cd.kblocks, kk = kb - seg * cd.kblocks;
+          const int ka = args.seg_a[seg] + kk, kbb = args.seg_b[seg] + kk;
+          if (leader) mbar_arrive_expect_tx(full_bar(stage), 2 * k4pStageBytes);
+          const uint32_t fb = map_shared(full_bar(stage), 0);
+          tma_load_2d_pair(a_addr(stage), &tmA, ka * k4KB, rowA, fb);
+          tma_load_2d_pair(b_addr(stage), &tmB, kbb * k4KB, rowB, fb);
+          // scale atoms as rows of 256 bytes: SFA (ga, 4 ka ..): 8 rows, SFB: 16
+          tma_load_2d_pair(sfa_addr(stage), &tmSa, 0, int32_t((ga * args.nks + 4 * ka) * 2), fb);
+          tma_load_2d_pair(sfb_addr(stage), &tmSb, 0, int32_t((gb * args.nks + 4 * kbb) * 4), fb);
+          if (++stage == k4pStages) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+        if (!ok) break;
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------ MMA issuer (leader CTA)
+    if (lane == 0 && leader) {
+      constexpr uint32_t idesc = idesc_nvf4(256, k4pN);
+      const uint32_t sfa_t = tmem_base + uint32_t(k4pSfaCol);
+      const uint32_t sfb_t = tmem_base + uint32_t(k4pSfbCol);
+      int stage = 0, acc = 0;
+      uint32_t phase = 0, acc_phase = 0;
+      bool ok = true;
+      for (int t = pair; t < args.num_tiles && ok; t += npairs) {
+        const ChanDesc cd = args.chans[args.tiles[t].ch];
+        if (!mbar_wait(tempty_bar(acc), acc_phase ^ 1u, abort_flag)) {
+          atomicOr(args.status, kStatusTimeoutMma);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + uint32_t(acc * k4pAccCols);
+        for (int kb = 0; kb < cd.kblocks * args.nseg; ++kb) {
+          if (!mbar_wait(full_bar(stage), phase, abort_flag)) {
+            atomicOr(args.status, kStatusTimeoutMma);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          // the previous stage's MMAs read these columns: the copies queue
+          // behind them in the tcgen05 pipe
+#pragma unroll
+          for (int s = 0; s < 4; ++s) {
+            tmem_cp_32x128b_warpx4_pair(sfa_t + 4 * s,
+                                        sdesc_none_kmajor(sfa_addr(stage) + 512 * s, 128));
+            tmem_cp_32x128b_warpx4_pair(sfb_t + 8 * s,
+                                        sdesc_none_kmajor(sfb_addr(stage) + 1024 * s, 128));
+            tmem_cp_32x128b_warpx4_pair(sfb_t + 8 * s + 4,
+                                        sdesc_none_kmajor(sfb_addr(stage) + 1024 * s + 512, 128));
+          }
+#pragma unroll
+          for (int s = 0; s < 4; ++s) {
+            mma_nvf4_pair(d, sdesc_sw128_kmajor(a_addr(stage) + 32 * s),
+                          sdesc_sw128_kmajor(b_addr(stage) + 32 * s), idesc, sfa_t + 4 * s,
+                          sfb_t + 8 * s, (kb | s) != 0);
+          }
+          mma_commit_pair(empty_bar(stage));
+          mma_commit_pair(map_shared(empty_bar(stage), 1));
+          if (++stage == k4pStages) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+        if (!ok) break;
+        mma_commit_pair(tfull_bar(acc));
+        mma_commit_pair(map_shared(tfull_bar(acc), 1));
+        if (++acc == 2) {
+          acc = 0;
+          acc_phase ^= 1u;
+        }
+      }
+      mma_commit_pair(done_bar);
+      volatile int never = 0;
+      if (!mbar_wait(done_bar, 0, &never)) atomicOr(args.status, kStatusTimeoutOther);
+    }
+  } else {
+    // ------------------------------------------------ epilogue (warps 2..5, both CTAs)
+    const int q = warp & 3;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    float2* out = static_cast<float2*>(args.out);
+    for (int t = pair; t < args.num_tiles; t += npairs) {
+      const TileDesc td = args.tiles[t];
+      const ChanDesc cd = args.chans[td.ch];
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(tfull_bar(acc), acc_phase, abort_flag));
+      if (!ok) {
+        if (lane == 0) atomicOr(args.status, kStatusTimeoutEpilogue);
+        break;
+      }
+      tc_fence_after();
+      const int n = cd.n;
+      const int jw = int(td.tj) * k4pJ + 128 * int(rank) + q * 32;
+      const int j = jw + lane;
+      const int ib = int(td.ti) * k4pI;
+      const float sc = args.alpha * (args.chan_scale ? args.chan_scale[td.ch] : 1.f);
+      float2* outc = out + cd.out0;
+      const uint32_t tb = tmem_base + (uint32_t(q * 32) << 16) + uint32_t(acc * k4pAccCols);
+#pragma unroll 1
+      for (int c = 0; c < k4pAccCols / 32; ++c) {
+        const int i0 = ib + 16 * c;
+        if (i0 + 15 < jw || i0 >= n) continue;  // warp-uniform: nothing to store
+        uint32_t r[32];
+        __syncwarp();
+        tmem_ld_32x32b_x32(tb + 32u * c, r);
+        tmem_wait_ld();
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+          const int i = i0 + m;
+          if (i < n && j <= i) {
+            float vr = (i == j) ? args.row_power[cd.row0 + i] * args.alpha
+                                : __uint_as_float(r[2 * m]) * sc;
+            float vi = (i == j) ? 0.f : __uint_as_float(r[2 * m + 1]) * sc;
+            float2* p = outc + int64_t(i) * (i + 1) / 2 + j;
+            if (args.beta != 0.f) {
+              const float2 o = *p;
+              vr += args.beta * o.x;
+              vi += args.beta * o.y;
+            }
+            __stcs(p, make_float2(vr, vi));
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster_relaxed(map_shared(tempty_bar(acc), 0));
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1u;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // neither CTA leaves while the other may still signal it
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc_pair(tmem_base, 512);
+  }
+}
+
 }  // namespace
 
 // Workspace: E2M1 operand rows (2 per input; twice as long when split), then
@@ -455,16 +707,20 @@ struct Fp4Ws {
   SfGeom sg;
   int64_t z_bytes, sfa_bytes, sfb_bytes, total;
 };
-Fp4Ws fp4_ws(int n, int batch, int K, int split) {
+Fp4Ws fp4_ws(int n, int batch, int K, int split, int pair) {
   Fp4Ws w;
   const int64_t rows = int64_t(n) * batch;
   w.pitch = (2 * int64_t(K) + 255) / 256 * 128;
   w.rpitch = split ? 2 * w.pitch : w.pitch;
-  w.sg = SfGeom{n, (n + 127) / 128, (2 * n + 127) / 128, int(w.rpitch / 32)};
+  const int nks = int(w.rpitch / 32);
+  if (pair)  // A: both 128-row halves of every 256-input tile; B: 224-row groups
+    w.sg = SfGeom{n, 2 * ((n + k4pJ - 1) / k4pJ), (2 * n + k4pN - 1) / k4pN, nks, k4pN, 2};
+  else
+    w.sg = SfGeom{n, (n + 127) / 128, (2 * n + 127) / 128, nks, 128, 1};
   auto up = [](int64_t b) { return (b + 1023) / 1024 * 1024; };
   w.z_bytes = up(2 * rows * w.rpitch);
   w.sfa_bytes = up(int64_t(batch) * w.sg.gA * w.sg.nks * 512);
-  w.sfb_bytes = up(int64_t(batch) * w.sg.gB * w.sg.nks * 512);
+  w.sfb_bytes = up(int64_t(batch) * w.sg.gB * w.sg.nks * w.sg.nsub * 512);
   w.total = w.z_bytes + w.sfa_bytes + w.sfb_bytes + up(4 * rows);
   return w;
 }
@@ -472,8 +728,36 @@ Fp4Ws fp4_ws(int n, int batch, int K, int split) {
 
 // Workspace: E2M1 operand rows (2 per input; twice as long when split), the
 // scale atoms of the A and B views, the row powers.
-size_t nvfp4_workspace_bytes(int n, int batch, int K, int split) {
-  return size_t(fp4_ws(n, batch, K, split).total);
+size_t nvfp4_workspace_bytes(int n, int batch, int K, int split, int pair) {
+  return size_t(fp4_ws(n, batch, K, split, pair).total);
+}
+
+// Pairs of the NVFP4 pair kernel that can be resident at once (0: none).
+int nvfp4_pair_limit() {
+  static int limit = -1;
+  if (limit < 0) {
+    limit = 0;
+    if (cudaFuncSetAttribute(herk_fp4_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(k4pSmem)) == cudaSuccess) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(2, 1, 1);
+      cfg.blockDim = dim3(k4pThreads, 1, 1);
+      cfg.dynamicSmemBytes = k4pSmem;
+      int n = 0;
+      if (cudaOccupancyMaxActiveClusters(&n, herk_fp4_pair_kernel, &cfg) == cudaSuccess) limit = n;
+    }
+    cudaGetLastError();
+  }
+  return limit;
+}
+
+// Tile list of the pair kernel for one channel of n inputs: tj over 256
+// column inputs, ti over 112 row inputs, tiles holding some j <= i.
+void nvfp4_pair_tiles(int n, int ch, std::vector<TileDesc>& out) {
+  const int ni = (n + k4pI - 1) / k4pI, nj = (n + k4pJ - 1) / k4pJ;
+  for (int ti = 0; ti < ni; ++ti)
+    for (int tj = 0; tj < nj && tj * k4pJ <= ti * k4pI + k4pI - 1; ++tj)
+      out.push_back(TileDesc{ch, uint16_t(ti), uint16_t(tj)});
 }
 
 int nvfp4_kblocks(int K) { return int((2 * int64_t(K) + 255) / 256); }
@@ -482,19 +766,20 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
                          float* gscale, float* out_scale, uint32_t* amax_bits,
                          const TileDesc* tiles, const ChanDesc* chans, int num_tiles, void* C,
                          float alpha, float beta, uint32_t* status, int sm_count, void* encode_fn,
-                         cudaStream_t s, int split) {
+                         cudaStream_t s, int split, int pair) {
   auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(encode_fn);
   if (!encode) return cudaErrorInvalidValue;
-  const Fp4Ws w = fp4_ws(n, batch, K, split);
+  if (pair && nvfp4_pair_limit() < 1) return cudaErrorInvalidConfiguration;
+  const Fp4Ws w = fp4_ws(n, batch, K, split, pair);
   const int64_t pitch = w.pitch, rpitch = w.rpitch;  // one half (hi or lo), whole row
   uint8_t* z = ws;
   uint8_t* sfa = ws + w.z_bytes;
   uint8_t* sfb = sfa + w.sfa_bytes;
   float* power = reinterpret_cast<float*>(sfb + w.sfb_bytes);
-  // rows of a partial 128-row group get no scales from the quantiser: zero them
+  // rows of a partial group get no scales from the quantiser: zero them
   // (their products land only in outputs the epilogue skips)
   cudaError_t e;
-  if ((n & 127) != 0) {
+  if (n % (pair ? k4pJ : 128) != 0 || (2 * n) % w.sg.gbrows != 0) {
     e = cudaMemsetAsync(sfa, 0, size_t(w.sfa_bytes + w.sfb_bytes), s);
     if (e != cudaSuccess) return e;
   }
@@ -521,19 +806,26 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
 
-  CUtensorMap tmA, tmB;
+  CUtensorMap tmA, tmB, tmSa, tmSb;
   const cuuint32_t estr[2] = {1, 1};
   auto enc2 = [&](CUtensorMap* m, void* base, int64_t inner, int64_t nrows, int64_t stride,
-                  uint32_t box0, CUtensorMapSwizzle sw) {
+                  uint32_t box0, CUtensorMapSwizzle sw, uint32_t box1 = 128) {
     const cuuint64_t dims[2] = {cuuint64_t(inner), cuuint64_t(nrows)};
     const cuuint64_t str[1] = {cuuint64_t(stride)};
-    const cuuint32_t box[2] = {box0, 128};
+    const cuuint32_t box[2] = {box0, box1};
     return encode(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, str, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   };
   if (enc2(&tmA, z, rpitch, rows, 2 * rpitch, k4KB, CU_TENSOR_MAP_SWIZZLE_128B) != CUDA_SUCCESS ||
-      enc2(&tmB, z, rpitch, 2 * rows, rpitch, k4KB, CU_TENSOR_MAP_SWIZZLE_128B) != CUDA_SUCCESS)
+      enc2(&tmB, z, rpitch, 2 * rows, rpitch, k4KB, CU_TENSOR_MAP_SWIZZLE_128B,
+           pair ? k4pI : 128) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  if (pair &&  // scale atoms as rows of 256 bytes: 4 atoms (SFA) / 8 atoms (SFB) per stage
+      (enc2(&tmSa, sfa, 256, w.sfa_bytes / 256, 256, 256, CU_TENSOR_MAP_SWIZZLE_NONE, 8) !=
+           CUDA_SUCCESS ||
+       enc2(&tmSb, sfb, 256, w.sfb_bytes / 256, 256, 256, CU_TENSOR_MAP_SWIZZLE_NONE, 16) !=
+           CUDA_SUCCESS))
     return cudaErrorInvalidValue;
   Fp4Args args{tiles, chans, num_tiles, C, alpha, beta, out_scale, status, power,
                sfa, sfb, w.sg.gA, w.sg.gB, w.sg.nks};
@@ -546,6 +838,12 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
     const int sa[3] = {0, 0, L}, sb[3] = {0, L, 0};
     args.nseg = 3;
     for (int q = 0; q < 3; ++q) args.seg_a[q] = sa[q], args.seg_b[q] = sb[q];
+  }
+  if (pair) {
+    const int limit = nvfp4_pair_limit();
+    const int pairs = num_tiles < limit ? num_tiles : limit;
+    herk_fp4_pair_kernel<<<2 * pairs, k4pThreads, k4pSmem, s>>>(tmA, tmB, tmSa, tmSb, args);
+    return cudaGetLastError();
   }
   static bool attr = false;
   if (!attr) {

@@ -16,12 +16,16 @@ pytestmark = pytest.mark.gpu
 DEV = "cuda:0"
 
 
-def run_float(v, compute):
+def run_float(v, compute, store_mode=None):
+    """store_mode 0 / 2 picks the NVFP4 single-CTA / pair kernel (None: tuned)."""
     B, N, K = v.shape
     A = torch.from_numpy(np.ascontiguousarray(v).view(np.float32).reshape(B, N, K, 2)).to(DEV)
     C = torch.full((B, tri_size(N), 2), float("nan"), device=DEV)
     with Correlator() as c:
-        c.herk(A, C, N, K, B, input=IN_FP32, compute=compute, output=OUT_FP32)
+        if store_mode is not None:
+            c.set_strategy(store_mode, 0)
+        c.herk(A, C, N, K, B, input=IN_FP32, compute=compute, output=OUT_FP32,
+               tune=store_mode is None)
         assert c.device_status() == 0
     torch.cuda.synchronize()
     return C.cpu().numpy()
@@ -93,7 +97,8 @@ def test_kahan_accumulation_across_dumps():
 E2M1 = np.array([0.0, 0.5, 1.0, 1.5, 2.0, 3.0, 4.0, 6.0])
 
 
-def test_nvfp4_exactly_representable_input_is_exact():
+@pytest.mark.parametrize("store_mode", [0, 2])
+def test_nvfp4_exactly_representable_input_is_exact(store_mode):
     # Every block of 8 complex samples holds E2M1 values times a per-block power
     # of two, with one component at 6 x that power: the quantiser's block scales
     # come out exact (448, 224, 112 in UE4M3) and so does every element, so the
@@ -110,10 +115,10 @@ def test_nvfp4_exactly_representable_input_is_exact():
     pw[:, 0, 0, 0] = 1.0                              # channel max = 6
     v = (blocks * pw).reshape(B, N, K, 2)
     vc = (v[..., 0] + 1j * v[..., 1]).astype(np.complex64)
-    got = run_float(vc, COMPUTE_FP4)
+    got = run_float(vc, COMPUTE_FP4, store_mode)
     ref = oracle.herk_c128(vc.astype(np.complex128), N, K, B)
     err = np.abs(got - ref).max() / np.abs(ref).max()
-    print("nvfp4 exact-input max rel err", err)
+    print("nvfp4 exact-input max rel err", store_mode, err)
     assert err < 1e-6
 
 
@@ -140,7 +145,8 @@ def test_nvfp4_error_without_rfi():
     assert err["rms_offdiag_norm"] < 1e-2 and err["max_offdiag_norm"] < 3e-2
 
 
-def test_nvfp4_split_exactly_representable_input_is_exact():
+@pytest.mark.parametrize("store_mode", [0, 2])
+def test_nvfp4_split_exactly_representable_input_is_exact(store_mode):
     # input that NVFP4 holds exactly: the residual is zero, every lo block scale
     # is zero, and the split mode gives the plain NVFP4 result (same rtol 1e-6)
     from ftd_b200._lib import COMPUTE_FP4, COMPUTE_FP4_SPLIT
@@ -154,11 +160,11 @@ def test_nvfp4_split_exactly_representable_input_is_exact():
     v = (blocks * pw).reshape(B, N, K, 2)
     vc = (v[..., 0] + 1j * v[..., 1]).astype(np.complex64)
     ref = oracle.herk_c128(vc.astype(np.complex128), N, K, B)
-    got = run_float(vc, COMPUTE_FP4_SPLIT)
+    got = run_float(vc, COMPUTE_FP4_SPLIT, store_mode)
     err = np.abs(got - ref).max() / np.abs(ref).max()
-    print("nvfp4 split exact-input max rel err", err)
+    print("nvfp4 split exact-input max rel err", store_mode, err)
     assert err < 1e-6
-    assert np.array_equal(got, run_float(vc, COMPUTE_FP4))
+    assert np.array_equal(got, run_float(vc, COMPUTE_FP4, store_mode))
 
 
 def test_nvfp4_split_error(workload):
@@ -188,3 +194,19 @@ def test_nvfp4_split_batch_and_ragged():
     err = oracle.correlation_errors(run_float(v, COMPUTE_FP4_SPLIT), ref, N)
     print("nvfp4 split ragged", err)
     assert err["max_offdiag_norm"] < 3e-2 and err["max_auto_rel"] < 1e-5
+
+
+@pytest.mark.parametrize("compute_name", ["COMPUTE_FP4", "COMPUTE_FP4_SPLIT"])
+def test_nvfp4_pair_equals_single_cta(compute_name):
+    # the two NVFP4 kernels quantise alike and differ only in the order of
+    # the FP32 accumulation: equal to FP32 rounding of the sums (rtol 1e-5 of
+    # the largest correlation), on ragged sizes across several channels
+    import ftd_b200._lib as L
+    compute = getattr(L, compute_name)
+    B, N, K = 3, 300, 200
+    v = oracle.workload4_voltages(408, B, N, K)
+    a = run_float(v, compute, 0)
+    b = run_float(v, compute, 2)
+    assert np.isfinite(b).all()
+    scale = np.abs(a).max()
+    assert np.abs(a - b).max() <= 1e-5 * scale
