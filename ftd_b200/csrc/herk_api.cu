@@ -124,19 +124,14 @@ ftdx_status launch_fp4(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   const int split = c.compute == FTDX_COMPUTE_FP4_SPLIT ? 1 : 0;
   const int pair = ((strat.store_mode & 3) == 2 && nvfp4_pair_limit() >= 1) ? 1 : 0;
   ftdx_status st = ensure_workspace(h, nvfp4_workspace_bytes(c.N, c.batch, c.K, split, pair), s);
-  if (st == FTDX_OK) st = ensure_aux(h, size_t(12) * size_t(c.batch) + 256, s);
   const Plan* plan = nullptr;
   if (st == FTDX_OK)
     st = get_fp4_plan(h, c.N, nvfp4_kblocks(c.K), c.batch, s, &plan, pair != 0);
   if (st != FTDX_OK) return st;
-  float* gscale = reinterpret_cast<float*>(h->aux);
-  float* out_scale = gscale + c.batch;
-  uint32_t* amax = reinterpret_cast<uint32_t*>(out_scale + c.batch);
   cudaError_t e;
   {
     ScopedTimer tm(h, s, 0);
-    e = launch_nvfp4(c.A, rows, c.K, c.N, c.batch, h->z, gscale, out_scale, amax,
-                     plan->d_tiles, plan->d_chans, plan->num_tiles, c.C, c.alpha, c.beta,
+    e = launch_nvfp4(c.A, rows, c.K, c.N, c.batch, h->z, plan->d_tiles, plan->d_chans, plan->num_tiles, c.C, c.alpha, c.beta,
                      h->d_status, h->sm_count, tensor_map_encoder(), s, split, pair);
   }
   return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "NVFP4 launch");

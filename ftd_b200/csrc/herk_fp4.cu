@@ -1,14 +1,15 @@
 // herk_fp4.cu -- NVFP4 correlator for float complex voltages.
 //
-// Quantisation (nvfp4_quantize_kernel): per channel a global FP32 scale
-// g_c = amax_c / (6 * 448); per row and block of 16 values along K (8
-// complex samples, Re/Im interleaved) a UE4M3 block scale b >= amax_blk /
-// (6 g_c) (rounded up, so no element saturates); elements E2M1(v / (g_c b)),
+// Quantisation (nvfp4_prepare_kernel, one pass over the input): per input
+// row a an FP32 scale g_a = amax_a / (6 * 448); per block of 16 values along
+// K (8 complex samples, Re/Im interleaved) a UE4M3 block scale b >= amax_blk
+// / (6 g_a) (rounded up, so no element saturates); elements E2M1(v / (g_a b)),
 // round to nearest even.  Each input row a becomes two operand rows with the
 // same block scales: x_a = (re, im)_t and y_a = (im, -re)_t, so that
 //   x_j . x_i = Re R_ij and x_j . y_i = Im R_ij
-// (the FP4 MMA has no negate bit; the sign lives in the y row).  The result
-// is multiplied by g_c^2 in the epilogue.
+// (the FP4 MMA has no negate bit; the sign lives in the y row).  The epilogue
+// multiplies each product by g_i g_j; autocorrelations come from the exact
+// FP64 row powers of the same pass.
 //
 // herk_fp4_tc_kernel: persistent tcgen05 kernel, tile = 128 column inputs j
 // (MMA M, x rows) x 64 row inputs i (MMA N = 128: their x and y rows).  TMA
@@ -41,7 +42,9 @@ constexpr int k4Stages = 5;
 constexpr int k4AccCols = 128;                // (Re, Im) column pairs of 64 inputs
 constexpr int k4SfCol0 = 2 * k4AccCols;       // TMEM columns of the scale-factor slots
 constexpr int k4SfColsPerStage = 32;          // 4 k-steps x (4 SFA + 4 SFB) columns
-constexpr int k4Threads = 192;                // TMA, MMA, 4 epilogue warps
+constexpr int k4EpiWarps = 8;                 // two per TMEM lane quarter
+constexpr int k4EpiGroups = k4EpiWarps / 4;   // warps per lane quarter (column chunks dealt round robin)
+constexpr int k4Threads = 64 + 32 * k4EpiWarps;  // TMA, MMA, epilogue warps
 constexpr size_t k4Smem = 1024 + size_t(k4Stages) * k4StageBytes + 256;
 
 // E4M3 bits of a non-negative float, rounded up to the next representable
@@ -66,16 +69,6 @@ __device__ __forceinline__ float2 fp4x2_value(uint32_t byte) {
   return __half22float2(__half2(h));
 }
 
-__global__ void fp4_scale_kernel(const uint32_t* __restrict__ amax_bits, int batch,
-                                 float* __restrict__ gscale, float* __restrict__ out_scale) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= batch) return;
-  const float m = __uint_as_float(amax_bits[c]);
-  const float g = (m > 0.f && m < 3.0e38f) ? m / (6.f * 448.f) : 1.f;
-  gscale[c] = g;
-  out_scale[c] = g * g;
-}
-
 // Block scales in the tcgen05 scale-factor atom: one 512-byte atom per 128
 // operand rows and k-step (64 E2M1 values = 4 blocks); row m of the group at
 // byte 16 (m % 32) + 4 (m / 32) + block.  A tcgen05.cp 32x128b.warpx4 of an
@@ -98,119 +91,122 @@ __device__ __forceinline__ int64_t sf_atom_byte(int64_t group, int nks, int nsub
   return ((group * nks + ks) * nsub + (m >> 7)) * 512 + (m & 31) * 16 + ((m >> 5) & 3) * 4 + blk;
 }
 
-// One thread: one 16-value block (8 complex samples) of one input row.
-// split: each operand row holds the hi half (pitch bytes) then the lo half,
-// lo = E2M1 of the residual x - hi with its own block scale (same global
-// scale), so hi + lo carries about twice the bits; the scales likewise (the
-// lo k-steps follow the hi ones).  Scales go to sfa (x rows, per input) and
-// sfb (x and y rows, two per input).
-__global__ void __launch_bounds__(256) nvfp4_quantize_kernel(
-    const float2* __restrict__ a, uint8_t* __restrict__ z, uint8_t* __restrict__ sfa,
-    uint8_t* __restrict__ sfb, int64_t rows, int K, int pitch, SfGeom sg,
-    const float* __restrict__ gscale, int split) {
-  const int n = sg.n;
-  const int blocks_per_row = pitch / 8;  // 8 bytes of E2M1 per block
+// Quantise one 16-value block (8 complex samples x[2q] = Re, x[2q+1] = Im)
+// of input row r (channel c, input w) under the row's FP32 scale g: a UE4M3
+// block scale b >= amax_blk / (6 g) (rounded up, so no element saturates) and
+// E2M1(v / (g b)), round to nearest even, into the x = (re, im) and
+// y = (im, -re) operand rows.  split: each operand row holds the hi half
+// (pitch bytes) then the lo half, lo = E2M1 of the residual x - hi with its
+// own block scale (same g), so hi + lo carries about twice the bits; the lo
+// k-steps of the scales follow the hi ones.  Scales go to sfa (x rows, per
+// input) and sfb (x and y rows, two per input).
+__device__ __forceinline__ void nvfp4_block(float (&x)[16], float g, int64_t r, int c, int w,
+                                            int b, uint8_t* __restrict__ z,
+                                            uint8_t* __restrict__ sfa, uint8_t* __restrict__ sfb,
+                                            int pitch, const SfGeom& sg, int split) {
   const int rpitch = split ? 2 * pitch : pitch;
-  const int ksh = pitch / 32;            // k-steps per half
-  const int64_t total = rows * blocks_per_row;
-  for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
-       idx += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t r = idx / blocks_per_row;
-    const int b = int(idx - r * blocks_per_row);
-    const int t0 = 8 * b;
-    float x[16];
-    float amax = 0.f;
+  const int ksh = pitch / 32;  // k-steps per half
+  float amax = 0.f;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) amax = fmaxf(amax, fabsf(x[q]));
+  const uint32_t bc = ue4m3_ceil(amax / (6.f * g));
+  const float inv = bc ? 1.f / (g * ue4m3_value(bc)) : 0.f;
+  uint32_t xw[2] = {0u, 0u}, yw[2] = {0u, 0u};
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const float re = x[2 * q] * inv, im = x[2 * q + 1] * inv;
+    xw[q >> 2] |= fp4x2(re, im) << (8 * (q & 3));
+    yw[q >> 2] |= fp4x2(im, -re) << (8 * (q & 3));
+  }
+  *reinterpret_cast<uint2*>(z + (2 * r) * rpitch + 8 * b) = make_uint2(xw[0], xw[1]);
+  *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + 8 * b) = make_uint2(yw[0], yw[1]);
+  const int64_t ga = int64_t(c) * sg.gA + (w >> 7);
+  const int64_t gb = int64_t(c) * sg.gB + (2 * w) / sg.gbrows;
+  const int ob = (2 * w) % sg.gbrows;  // x row in the group; y row next (gbrows is even)
+  const int ks = b >> 2, blk = b & 3;
+  sfa[sf_atom_byte(ga, sg.nks, 1, ks, w & 127, blk)] = uint8_t(bc);
+  sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ks, ob, blk)] = uint8_t(bc);
+  sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ks, ob + 1, blk)] = uint8_t(bc);
+  if (split) {
+    // residual of the hi quantisation, then its own block scale
+    const float step = bc ? g * ue4m3_value(bc) : 0.f;
+    float amax2 = 0.f;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const int t = t0 + q;
-      const float2 v = (t < K) ? __ldg(a + r * K + t) : make_float2(0.f, 0.f);
-      x[2 * q] = v.x;
-      x[2 * q + 1] = v.y;
-      amax = fmaxf(amax, fmaxf(fabsf(v.x), fabsf(v.y)));
+      const float2 h = fp4x2_value((xw[q >> 2] >> (8 * (q & 3))) & 0xFFu);
+      x[2 * q] -= h.x * step;
+      x[2 * q + 1] -= h.y * step;
+      amax2 = fmaxf(amax2, fmaxf(fabsf(x[2 * q]), fabsf(x[2 * q + 1])));
     }
-    const float g = gscale[r / n];
-    const uint32_t bc = ue4m3_ceil(amax / (6.f * g));
-    const float inv = bc ? 1.f / (g * ue4m3_value(bc)) : 0.f;
-    uint32_t xw[2] = {0u, 0u}, yw[2] = {0u, 0u};
+    const uint32_t bc2 = ue4m3_ceil(amax2 / (6.f * g));
+    const float inv2 = bc2 ? 1.f / (g * ue4m3_value(bc2)) : 0.f;
+    uint32_t xl[2] = {0u, 0u}, yl[2] = {0u, 0u};
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const float re = x[2 * q] * inv, im = x[2 * q + 1] * inv;
-      xw[q >> 2] |= fp4x2(re, im) << (8 * (q & 3));
-      yw[q >> 2] |= fp4x2(im, -re) << (8 * (q & 3));
+      const float re = x[2 * q] * inv2, im = x[2 * q + 1] * inv2;
+      xl[q >> 2] |= fp4x2(re, im) << (8 * (q & 3));
+      yl[q >> 2] |= fp4x2(im, -re) << (8 * (q & 3));
     }
-    *reinterpret_cast<uint2*>(z + (2 * r) * rpitch + 8 * b) = make_uint2(xw[0], xw[1]);
-    *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + 8 * b) = make_uint2(yw[0], yw[1]);
-    const int c = int(r / n), w = int(r - int64_t(c) * n);
-    const int64_t ga = int64_t(c) * sg.gA + (w >> 7);
-    const int64_t gb = int64_t(c) * sg.gB + (2 * w) / sg.gbrows;
-    const int ob = (2 * w) % sg.gbrows;  // x row in the group; y row next (gbrows is even)
-    const int ks = b >> 2, blk = b & 3;
-    sfa[sf_atom_byte(ga, sg.nks, 1, ks, w & 127, blk)] = uint8_t(bc);
-    sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ks, ob, blk)] = uint8_t(bc);
-    sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ks, ob + 1, blk)] = uint8_t(bc);
-    if (split) {
-      // residual of the hi quantisation, then its own block scale
-      const float step = bc ? g * ue4m3_value(bc) : 0.f;
-      float amax2 = 0.f;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const float2 h = fp4x2_value((xw[q >> 2] >> (8 * (q & 3))) & 0xFFu);
-        x[2 * q] -= h.x * step;
-        x[2 * q + 1] -= h.y * step;
-        amax2 = fmaxf(amax2, fmaxf(fabsf(x[2 * q]), fabsf(x[2 * q + 1])));
-      }
-      const uint32_t bc2 = ue4m3_ceil(amax2 / (6.f * g));
-      const float inv2 = bc2 ? 1.f / (g * ue4m3_value(bc2)) : 0.f;
-      uint32_t xl[2] = {0u, 0u}, yl[2] = {0u, 0u};
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const float re = x[2 * q] * inv2, im = x[2 * q + 1] * inv2;
-        xl[q >> 2] |= fp4x2(re, im) << (8 * (q & 3));
-        yl[q >> 2] |= fp4x2(im, -re) << (8 * (q & 3));
-      }
-      *reinterpret_cast<uint2*>(z + (2 * r) * rpitch + pitch + 8 * b) = make_uint2(xl[0], xl[1]);
-      *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + pitch + 8 * b) =
-          make_uint2(yl[0], yl[1]);
-      sfa[sf_atom_byte(ga, sg.nks, 1, ksh + ks, w & 127, blk)] = uint8_t(bc2);
-      sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ksh + ks, ob, blk)] = uint8_t(bc2);
-      sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ksh + ks, ob + 1, blk)] = uint8_t(bc2);
-    }
+    *reinterpret_cast<uint2*>(z + (2 * r) * rpitch + pitch + 8 * b) = make_uint2(xl[0], xl[1]);
+    *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + pitch + 8 * b) = make_uint2(yl[0], yl[1]);
+    sfa[sf_atom_byte(ga, sg.nks, 1, ksh + ks, w & 127, blk)] = uint8_t(bc2);
+    sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ksh + ks, ob, blk)] = uint8_t(bc2);
+    sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ksh + ks, ob + 1, blk)] = uint8_t(bc2);
   }
 }
 
-// One pass over the FP32 input for both statistics the quantiser and the
-// epilogue need: the autocorrelation of every input row, sum_t |v_t|^2
-// accumulated in FP64 in a fixed order (one warp per row, so the result is
-// deterministic), and the channel max |Re|, |Im| (block reduce, one atomicMax
-// per block; NaN counts as 0).  Grid (x, channel); warps of a channel's
-// blocks stride over its n rows.
-__global__ void __launch_bounds__(256) fp4_stats_kernel(const float2* __restrict__ a, int n, int K,
-                                                        float* __restrict__ power,
-                                                        uint32_t* __restrict__ amax_bits) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int c = blockIdx.y;
-  const int wpb = blockDim.x >> 5;
-  float m = 0.f;
-  for (int w = blockIdx.x * wpb + warp; w < n; w += gridDim.x * wpb) {
-    const int64_t r = int64_t(c) * n + w;
+// One warp per input row, one pass over HBM.  Pass 1 reads the row for its
+// max |Re|, |Im| (the row's FP32 scale g_r = amax_r / (6 * 448), 1 for an
+// empty row; NaN counts as 0) and its autocorrelation sum_t |v_t|^2
+// (accumulated in FP64 in a fixed order, so deterministic); pass 2 reads it
+// again, now from L2, and quantises it block by block (lane l: blocks l,
+// l + 32, ...).  The correlator multiplies each product by g_i g_j.
+__global__ void __launch_bounds__(256) nvfp4_prepare_kernel(
+    const float2* __restrict__ a, uint8_t* __restrict__ z, uint8_t* __restrict__ sfa,
+    uint8_t* __restrict__ sfb, float* __restrict__ power, float* __restrict__ rscale,
+    int64_t rows, int K, int pitch, SfGeom sg, int split) {
+  const int lane = threadIdx.x & 31;
+  const int blocks_per_row = pitch / 8;  // 8 bytes of E2M1 per block
+  const bool vec = (K & 1) == 0 && (reinterpret_cast<uintptr_t>(a) & 15) == 0;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < rows;
+       r += (int64_t(gridDim.x) * blockDim.x) >> 5) {
     const float2* p = a + r * K;
     double acc = 0.0;
+    float m = 0.f;
     for (int t = lane; t < K; t += 32) {
       const float2 v = __ldg(p + t);
       acc += double(v.x) * v.x + double(v.y) * v.y;
       m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
     }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) power[r] = float(acc);
-  }
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  __shared__ float wm[32];
-  if (lane == 0) wm[warp] = m;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int q = 1; q < wpb; ++q) m = fmaxf(m, wm[q]);
-    if (!(m == m)) m = 0.f;
-    atomicMax(amax_bits + c, __float_as_uint(m));
+    for (int o = 16; o > 0; o >>= 1) {
+      acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    const float g = (m > 0.f && m < 3.0e38f) ? m / (6.f * 448.f) : 1.f;
+    if (lane == 0) {
+      power[r] = float(acc);
+      rscale[r] = g;
+    }
+    const int c = int(r / sg.n), w = int(r - int64_t(c) * sg.n);
+    for (int b = lane; b < blocks_per_row; b += 32) {
+      const int t0 = 8 * b;
+      float x[16];
+      if (vec && t0 + 8 <= K) {
+        const float4* p4 = reinterpret_cast<const float4*>(p + t0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float4 v = __ldg(p4 + q);
+          x[4 * q] = v.x, x[4 * q + 1] = v.y, x[4 * q + 2] = v.z, x[4 * q + 3] = v.w;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float2 v = (t0 + q < K) ? __ldg(p + t0 + q) : make_float2(0.f, 0.f);
+          x[2 * q] = v.x, x[2 * q + 1] = v.y;
+        }
+      }
+      nvfp4_block(x, g, r, c, w, b, z, sfa, sfb, pitch, sg, split);
+    }
   }
 }
 
@@ -226,7 +222,7 @@ struct Fp4Args {
   int num_tiles;
   void* out;
   float alpha, beta;
-  const float* chan_scale;
+  const float* row_scale;  // g_r per input row (the products carry g_i g_j)
   uint32_t* status;
   const float* row_power;  // exact sum_t |v_t|^2 per input row (the autocorrelations)
   const uint8_t* sfa;      // scale atoms of the x rows (A)
@@ -266,7 +262,7 @@ __global__ void __launch_bounds__(k4Threads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(tfull_bar(b), 1);
-      mbar_init(tempty_bar(b), 4);
+      mbar_init(tempty_bar(b), k4EpiWarps);
     }
     mbar_init(done_bar, 1);
     *abort_flag = 0;
@@ -384,8 +380,10 @@ __global__ void __launch_bounds__(k4Threads, 1)
       if (!mbar_wait(done_bar, 0, &never)) atomicOr(args.status, kStatusTimeoutOther);
     }
   } else {
-    // ------------------------------------------------ epilogue (warps 2..5)
+    // ------------------------------------------------ epilogue (warps 2..)
+    // warp w drains lane quarter w % 4, column chunks c = (w - 2) / 4 mod groups
     const int q = warp & 3;
+    const int grp = (warp - 2) >> 2;
     int acc = 0;
     uint32_t acc_phase = 0;
     float2* out = static_cast<float2*>(args.out);
@@ -402,11 +400,11 @@ __global__ void __launch_bounds__(k4Threads, 1)
       const int jw = int(td.tj) * k4J + q * 32;
       const int j = jw + lane;
       const int ib = int(td.ti) * k4I;
-      const float sc = args.alpha * (args.chan_scale ? args.chan_scale[td.ch] : 1.f);
+      const float sc = args.alpha * (j < n ? args.row_scale[cd.row0 + j] : 0.f);  // alpha g_j
       float2* outc = out + cd.out0;
       const uint32_t tb = tmem_base + (uint32_t(q * 32) << 16) + uint32_t(acc * k4AccCols);
 #pragma unroll 1
-      for (int c = 0; c < k4AccCols / 32; ++c) {
+      for (int c = grp; c < k4AccCols / 32; c += k4EpiGroups) {
         const int i0 = ib + 16 * c;
         if (i0 + 15 < jw || i0 >= n) continue;
         uint32_t r[32];
@@ -419,9 +417,10 @@ __global__ void __launch_bounds__(k4Threads, 1)
           if (i < n && j <= i) {
             // autocorrelations come from the FP32 power pass: their NVFP4
             // estimate would carry the quantisation-noise power as a bias
+            const float sij = sc * args.row_scale[cd.row0 + i];  // alpha g_i g_j
             float vr = (i == j) ? args.row_power[cd.row0 + i] * args.alpha
-                                : __uint_as_float(r[2 * m]) * sc;
-            float vi = (i == j) ? 0.f : __uint_as_float(r[2 * m + 1]) * sc;
+                                : __uint_as_float(r[2 * m]) * sij;
+            float vi = (i == j) ? 0.f : __uint_as_float(r[2 * m + 1]) * sij;
             float2* p = outc + int64_t(i) * (i + 1) / 2 + j;
             if (args.beta != 0.f) {
               const float2 o = *p;
@@ -473,7 +472,7 @@ constexpr int k4pStages = 6;
 constexpr int k4pAccCols = k4pN;              // one accumulator: 224 columns
 constexpr int k4pSfaCol = 2 * k4pAccCols;     // 448: 4 k-steps x 4 columns
 constexpr int k4pSfbCol = k4pSfaCol + 16;     // 464: 4 k-steps x 8 columns (..495)
-constexpr int k4pThreads = 192;               // TMA, MMA, 4 epilogue warps
+constexpr int k4pThreads = 64 + 32 * k4EpiWarps;  // TMA, MMA, epilogue warps
 constexpr size_t k4pSmem = 1024 + size_t(k4pStages) * k4pStageBytes + 256;
 static_assert(k4pSfbCol + 32 <= 512, "TMEM columns");
 
@@ -512,7 +511,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(k4pThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(tfull_bar(b), 1);
-      mbar_init(tempty_bar(b), 2 * 4);  // the epilogue warps of both CTAs
+      mbar_init(tempty_bar(b), 2 * k4EpiWarps);  // the epilogue warps of both CTAs
     }
     mbar_init(done_bar, 1);
     *abort_flag = 0;
@@ -631,8 +630,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(k4pThreads, 1)
       if (!mbar_wait(done_bar, 0, &never)) atomicOr(args.status, kStatusTimeoutOther);
     }
   } else {
-    // ------------------------------------------------ epilogue (warps 2..5, both CTAs)
+    // ------------------------------------------------ epilogue (warps 2.., both CTAs)
+    // warp w drains lane quarter w % 4, column chunks c = (w - 2) / 4 mod groups
     const int q = warp & 3;
+    const int grp = (warp - 2) >> 2;
     int acc = 0;
     uint32_t acc_phase = 0;
     float2* out = static_cast<float2*>(args.out);
@@ -649,11 +650,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(k4pThreads, 1)
       const int jw = int(td.tj) * k4pJ + 128 * int(rank) + q * 32;
       const int j = jw + lane;
       const int ib = int(td.ti) * k4pI;
-      const float sc = args.alpha * (args.chan_scale ? args.chan_scale[td.ch] : 1.f);
+      const float sc = args.alpha * (j < n ? args.row_scale[cd.row0 + j] : 0.f);  // alpha g_j
       float2* outc = out + cd.out0;
       const uint32_t tb = tmem_base + (uint32_t(q * 32) << 16) + uint32_t(acc * k4pAccCols);
 #pragma unroll 1
-      for (int c = 0; c < k4pAccCols / 32; ++c) {
+      for (int c = grp; c < k4pAccCols / 32; c += k4EpiGroups) {
         const int i0 = ib + 16 * c;
         if (i0 + 15 < jw || i0 >= n) continue;  // warp-uniform: nothing to store
         uint32_t r[32];
@@ -664,9 +665,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(k4pThreads, 1)
         for (int m = 0; m < 16; ++m) {
           const int i = i0 + m;
           if (i < n && j <= i) {
+            const float sij = sc * args.row_scale[cd.row0 + i];  // alpha g_i g_j
             float vr = (i == j) ? args.row_power[cd.row0 + i] * args.alpha
-                                : __uint_as_float(r[2 * m]) * sc;
-            float vi = (i == j) ? 0.f : __uint_as_float(r[2 * m + 1]) * sc;
+                                : __uint_as_float(r[2 * m]) * sij;
+            float vi = (i == j) ? 0.f : __uint_as_float(r[2 * m + 1]) * sij;
             float2* p = outc + int64_t(i) * (i + 1) / 2 + j;
             if (args.beta != 0.f) {
               const float2 o = *p;
@@ -721,13 +723,13 @@ Fp4Ws fp4_ws(int n, int batch, int K, int split, int pair) {
   w.z_bytes = up(2 * rows * w.rpitch);
   w.sfa_bytes = up(int64_t(batch) * w.sg.gA * w.sg.nks * 512);
   w.sfb_bytes = up(int64_t(batch) * w.sg.gB * w.sg.nks * w.sg.nsub * 512);
-  w.total = w.z_bytes + w.sfa_bytes + w.sfb_bytes + up(4 * rows);
+  w.total = w.z_bytes + w.sfa_bytes + w.sfb_bytes + 2 * up(4 * rows);
   return w;
 }
 }  // namespace
 
 // Workspace: E2M1 operand rows (2 per input; twice as long when split), the
-// scale atoms of the A and B views, the row powers.
+// scale atoms of the A and B views, the row powers and the row scales.
 size_t nvfp4_workspace_bytes(int n, int batch, int K, int split, int pair) {
   return size_t(fp4_ws(n, batch, K, split, pair).total);
 }
@@ -763,7 +765,6 @@ void nvfp4_pair_tiles(int n, int ch, std::vector<TileDesc>& out) {
 int nvfp4_kblocks(int K) { return int((2 * int64_t(K) + 255) / 256); }
 
 cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, uint8_t* ws,
-                         float* gscale, float* out_scale, uint32_t* amax_bits,
                          const TileDesc* tiles, const ChanDesc* chans, int num_tiles, void* C,
                          float alpha, float beta, uint32_t* status, int sm_count, void* encode_fn,
                          cudaStream_t s, int split, int pair) {
@@ -776,6 +777,7 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
   uint8_t* sfa = ws + w.z_bytes;
   uint8_t* sfb = sfa + w.sfa_bytes;
   float* power = reinterpret_cast<float*>(sfb + w.sfb_bytes);
+  float* rscale = reinterpret_cast<float*>(sfb + w.sfb_bytes + (4 * rows + 1023) / 1024 * 1024);
   // rows of a partial group get no scales from the quantiser: zero them
   // (their products land only in outputs the epilogue skips)
   cudaError_t e;
@@ -783,26 +785,14 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
     e = cudaMemsetAsync(sfa, 0, size_t(w.sfa_bytes + w.sfb_bytes), s);
     if (e != cudaSuccess) return e;
   }
-  // row powers + channel amax (one pass) -> global scales -> quantise
-  e = cudaMemsetAsync(amax_bits, 0, sizeof(uint32_t) * size_t(batch), s);
-  if (e != cudaSuccess) return e;
+  // row scales, row powers and the E2M1 operands: one warp per row
   {
-    int bx = (n + 7) / 8;
-    const int cap = (sm_count * 8 + batch - 1) / batch;
-    if (bx > cap) bx = cap;
-    if (bx < 1) bx = 1;
-    fp4_stats_kernel<<<dim3(unsigned(bx), unsigned(batch)), 256, 0, s>>>(
-        static_cast<const float2*>(A), n, K, power, amax_bits);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    int64_t blocks = (rows + 7) / 8;
+    if (blocks > int64_t(sm_count) * 16) blocks = int64_t(sm_count) * 16;
+    nvfp4_prepare_kernel<<<unsigned(blocks), 256, 0, s>>>(static_cast<const float2*>(A), z, sfa,
+                                                           sfb, power, rscale, rows, K,
+                                                           int(pitch), w.sg, split);
   }
-  fp4_scale_kernel<<<(batch + 127) / 128, 128, 0, s>>>(amax_bits, batch, gscale, out_scale);
-  const int64_t work = rows * (pitch / 8);
-  int64_t blocks = (work + 255) / 256;
-  if (blocks > int64_t(sm_count) * 16) blocks = int64_t(sm_count) * 16;
-  nvfp4_quantize_kernel<<<unsigned(blocks), 256, 0, s>>>(static_cast<const float2*>(A), z, sfa,
-                                                          sfb, rows, K, int(pitch), w.sg, gscale,
-                                                          split);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
 
@@ -827,7 +817,7 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
        enc2(&tmSb, sfb, 256, w.sfb_bytes / 256, 256, 256, CU_TENSOR_MAP_SWIZZLE_NONE, 16) !=
            CUDA_SUCCESS))
     return cudaErrorInvalidValue;
-  Fp4Args args{tiles, chans, num_tiles, C, alpha, beta, out_scale, status, power,
+  Fp4Args args{tiles, chans, num_tiles, C, alpha, beta, rscale, status, power,
                sfa, sfb, w.sg.gA, w.sg.gB, w.sg.nks};
   args.nseg = 1;
   if (split) {

@@ -180,7 +180,6 @@ int nvfp4_kblocks(int K);
 int nvfp4_pair_limit();
 void nvfp4_pair_tiles(int n, int ch, std::vector<TileDesc>& out);
 cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, uint8_t* ws,
-                         float* gscale, float* out_scale, uint32_t* amax_bits,
                          const TileDesc* tiles, const ChanDesc* chans, int num_tiles, void* C,
                          float alpha, float beta, uint32_t* status, int sm_count, void* encode_fn,
                          cudaStream_t s, int split = 0, int pair = 0);
