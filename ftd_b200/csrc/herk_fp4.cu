@@ -173,10 +173,16 @@ __global__ void __launch_bounds__(256) nvfp4_prepare_kernel(
     const float2* p = a + r * K;
     double acc = 0.0;
     float m = 0.f;
-    for (int t = lane; t < K; t += 32) {
-      const float2 v = __ldg(p + t);
-      acc += double(v.x) * v.x + double(v.y) * v.y;
-      m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+    for (int t0 = lane; t0 < K; t0 += 128) {  // four loads in flight per lane
+      float2 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        v[u] = (t0 + 32 * u < K) ? __ldg(p + t0 + 32 * u) : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        acc += double(v[u].x) * v[u].x + double(v[u].y) * v[u].y;
+        m = fmaxf(m, fmaxf(fabsf(v[u].x), fabsf(v[u].y)));
+      }
     }
     for (int o = 16; o > 0; o >>= 1) {
       acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -233,6 +239,47 @@ struct Fp4Args {
   int nseg;
   int seg_a[4], seg_b[4];
 };
+
+// Epilogue of one 32-column accumulator chunk: rows i0..i0+15 (columns 2m,
+// 2m+1 = Re, Im of row i0+m) of lane j's column.  Element (i, j <= i < n)
+// = r * alpha g_i g_j (+ beta * old), the diagonal the exact row power;
+// sc_j = alpha g_j.  The 16 row scales arrive in one load per lane and warp
+// shuffles; chunks wholly below the diagonal and inside n store unmasked.
+// Row i0+m of the packed triangle starts m i0 + m(m+1)/2 after row i0.
+__device__ __forceinline__ void fp4_store_chunk(float2* __restrict__ outc, const uint32_t (&r)[32],
+                                                int i0, int j, int jw, int n, float sc_j,
+                                                const float* __restrict__ rs,
+                                                const float* __restrict__ pw, float alpha,
+                                                float beta, int lane) {
+  const int il = i0 + (lane & 15);
+  const float gl = il < n ? __ldg(rs + il) : 0.f;
+  const bool interior = (i0 + 15 < n) && (jw + 31 < i0);
+  float2* p0 = outc + int64_t(i0) * (i0 + 1) / 2 + j;
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    const float s = sc_j * __shfl_sync(0xffffffffu, gl, m);  // alpha g_i g_j
+    const int i = i0 + m;
+    if (interior || (i < n && j <= i)) {
+      float2* p = p0 + (int64_t(m) * i0 + m * (m + 1) / 2);
+      float vr, vi;
+      if (!interior && i == j) {
+        // autocorrelations come from the FP64 power pass: their NVFP4 estimate
+        // would carry the quantisation-noise power as a bias
+        vr = __ldg(pw + i) * alpha;
+        vi = 0.f;
+      } else {
+        vr = __uint_as_float(r[2 * m]) * s;
+        vi = __uint_as_float(r[2 * m + 1]) * s;
+      }
+      if (beta != 0.f) {
+        const float2 o = *p;
+        vr += beta * o.x;
+        vi += beta * o.y;
+      }
+      __stcs(p, make_float2(vr, vi));
+    }
+  }
+}
 
 __global__ void __launch_bounds__(k4Threads, 1)
     herk_fp4_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -411,25 +458,8 @@ __global__ void __launch_bounds__(k4Threads, 1)
         __syncwarp();
         tmem_ld_32x32b_x32(tb + 32u * c, r);
         tmem_wait_ld();
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-          const int i = i0 + m;
-          if (i < n && j <= i) {
-            // autocorrelations come from the FP32 power pass: their NVFP4
-            // estimate would carry the quantisation-noise power as a bias
-            const float sij = sc * args.row_scale[cd.row0 + i];  // alpha g_i g_j
-            float vr = (i == j) ? args.row_power[cd.row0 + i] * args.alpha
-                                : __uint_as_float(r[2 * m]) * sij;
-            float vi = (i == j) ? 0.f : __uint_as_float(r[2 * m + 1]) * sij;
-            float2* p = outc + int64_t(i) * (i + 1) / 2 + j;
-            if (args.beta != 0.f) {
-              const float2 o = *p;
-              vr += args.beta * o.x;
-              vi += args.beta * o.y;
-            }
-            __stcs(p, make_float2(vr, vi));
-          }
-        }
+        fp4_store_chunk(outc, r, i0, j, jw, n, sc, args.row_scale + cd.row0,
+                        args.row_power + cd.row0, args.alpha, args.beta, lane);
       }
       tc_fence_before();
       __syncwarp();
@@ -661,23 +691,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(k4pThreads, 1)
         __syncwarp();
         tmem_ld_32x32b_x32(tb + 32u * c, r);
         tmem_wait_ld();
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-          const int i = i0 + m;
-          if (i < n && j <= i) {
-            const float sij = sc * args.row_scale[cd.row0 + i];  // alpha g_i g_j
-            float vr = (i == j) ? args.row_power[cd.row0 + i] * args.alpha
-                                : __uint_as_float(r[2 * m]) * sij;
-            float vi = (i == j) ? 0.f : __uint_as_float(r[2 * m + 1]) * sij;
-            float2* p = outc + int64_t(i) * (i + 1) / 2 + j;
-            if (args.beta != 0.f) {
-              const float2 o = *p;
-              vr += args.beta * o.x;
-              vi += args.beta * o.y;
-            }
-            __stcs(p, make_float2(vr, vi));
-          }
-        }
+        fp4_store_chunk(outc, r, i0, j, jw, n, sc, args.row_scale + cd.row0,
+                        args.row_power + cd.row0, args.alpha, args.beta, lane);
       }
       tc_fence_before();
       __syncwarp();
