@@ -56,7 +56,8 @@ def parse():
     p.add_argument("--no-peak", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the extra workload legs")
     p.add_argument("--leg", default=None,
-                   choices=["nvfp4", "nvfp4split", "raw", "imaging", "xengine", "splitk"],
+                   choices=["nvfp4", "nvfp4split", "raw", "imaging", "xengine", "splitk",
+                            "precision"],
                    help="run one extra workload alone and print its JSON (profiling cases); "
                         "nvfp4 and nvfp4split use --inputs/--channels/--k")
     p.add_argument("--strategy", default=None,
@@ -763,6 +764,8 @@ def run_leg(args):
         out = run_imaging_leg(torch, dev)
     elif args.leg == "splitk":
         out = run_splitk_leg(torch, dev)
+    elif args.leg == "precision":
+        out = run_precision_leg(torch, dev)
     else:
         out = run_xengine_leg(torch, dev)
     print(json.dumps(out), flush=True)
