@@ -28,11 +28,13 @@ struct Plan {
 };
 
 constexpr int kStoreFp6 = 4;
+constexpr int kStoreS8 = 8;   // with store mode 2: signed 8-bit operands, kind::i8 MMAs
 // Launch strategy of the correlator kernel; chosen by the autotuner.
 struct Strategy {
   // 0: direct stores, 1: shared-memory staging + bulk copies,
   // 2: CTA-pair kernel (256 x 128 tiles on two SMs, direct stores);
-  // + kStoreFp6: operands as packed FP6 E3M2 planes (QC input, exact)
+  // + kStoreFp6: operands as packed FP6 E3M2 planes (QC input, exact);
+  // + kStoreS8 (pair only): signed 8-bit planes, integer MMAs (QC input, exact)
   int store_mode = 0;
   int grid = 0;        // persistent CTAs (0: one per SM); -1: one CTA per tile (not persistent)
   int splits = 1;      // split-K: K is cut into this many ranges, partials summed afterwards

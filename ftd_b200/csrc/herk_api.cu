@@ -188,6 +188,7 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   const int64_t zpitch = is_split(c) ? 2 * Kp : Kp;
   const int64_t rows = int64_t(c.N) * c.batch;
   const bool fp6 = ((strat.store_mode & kStoreFp6) || c.compute == FTDX_COMPUTE_FP6) && fp6_ok(c);
+  const bool s8 = !fp6 && pair && (strat.store_mode & kStoreS8) && fp6_ok(c);
   float* qscale = reinterpret_cast<float*>(h->aux);
   float* out_scale = qscale + c.batch;
   uint32_t* amax = reinterpret_cast<uint32_t*>(out_scale + c.batch);
@@ -214,10 +215,10 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
       e = launch_ftd_to_planes(static_cast<const uint8_t*>(c.A), h->z, g, int(d.layout),
                                h->sm_count, s);
     } else if (c.input == FTDX_IN_INT4) {
-      e = fp6 ? launch_qc_to_planes6(static_cast<const uint8_t*>(c.A), h->z, rows, c.K, int(Kp),
-                                     s, pair)
-              : launch_qc_to_planes(static_cast<const uint8_t*>(c.A), h->z, rows, c.K, int(Kp),
-                                    s, pair);
+      const uint8_t* qc = static_cast<const uint8_t*>(c.A);
+      e = fp6  ? launch_qc_to_planes6(qc, h->z, rows, c.K, int(Kp), s, pair)
+          : s8 ? launch_qc_to_planes_s8(qc, h->z, rows, c.K, int(Kp), s, pair)
+               : launch_qc_to_planes(qc, h->z, rows, c.K, int(Kp), s, pair);
     } else {
       if (c.input == FTDX_IN_FP16)
         e = launch_fp16_to_planes(c.A, h->z, rows, c.K, int(Kp), s);
@@ -238,6 +239,7 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   args.out_fp16 = (c.output == FTDX_OUT_FP16) ? 1 : 0;
   args.bulk_store = (strat.store_mode & 3) == 1 ? 1 : 0;
   args.fp6 = fp6 ? 1 : 0;
+  args.s8 = s8 ? 1 : 0;
   args.out_format = c.out_format;
   args.out = c.C;
   args.alpha = c.alpha;
@@ -307,6 +309,9 @@ ftdx_status run_tune(ftdx_handle h, const HerkCall& c, cudaStream_t s, TuneEntry
       is_fp4(c) ? std::vector<Strategy>{Strategy{0, h->sm_count}}
                 : default_candidates(h, c.output == FTDX_OUT_FP32, true);
   if (is_fp4(c) && nvfp4_pair_limit() >= 1) cands.push_back(Strategy{2, 0});
+  // QC input: the pair kernel on signed 8-bit operands (kind::i8, exact)
+  if (fp6_ok(c) && c.compute == FTDX_COMPUTE_FP8 && !c.comp && pair_grid_limit(h) >= 2)
+    cands.push_back(Strategy{2 | kStoreS8, pair_grid_limit(h)});
   const int kblocks = int(round_up(c.K, kStageK) / kStageK);
   if (!is_fp4(c) && !c.comp && plan->num_tiles < h->sm_count)
     for (int sp : {2, 4, 8, 16, 32})
@@ -453,8 +458,11 @@ void release_graphs(ftdx_handle h) {
   h->graphs.clear();
 }
 
-// Store modes 0..2, each optionally + kStoreFp6.
-static bool valid_store_mode(int m) { return m >= 0 && (m & 3) <= 2 && (m & ~(3 | kStoreFp6)) == 0; }
+// Store modes 0..2, each optionally + kStoreFp6, or 2 + kStoreS8.
+static bool valid_store_mode(int m) {
+  if (m < 0 || (m & 3) > 2 || (m & ~(3 | kStoreFp6 | kStoreS8)) != 0) return false;
+  return !(m & kStoreS8) || m == (2 | kStoreS8);
+}
 
 // Text cache, one entry per line:
 //   ftdx-tune 2 <device> <N> <Kp> <batch> <input> <output> <store_mode> <grid> <splits> <ms>

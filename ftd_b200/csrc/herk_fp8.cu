@@ -78,6 +78,52 @@ __global__ void __launch_bounds__(256) qc_to_planes_kernel(const uint8_t* __rest
   }
 }
 
+// Signed 8-bit operand planes: as qc_to_planes_kernel with two's-complement
+// integers instead of E4M3 codes (plane 2 = -Re by a per-byte negate).
+__global__ void __launch_bounds__(256) qc_to_planes_s8_kernel(const uint8_t* __restrict__ qc,
+                                                              uint8_t* __restrict__ z,
+                                                              int64_t rows, int K, int Kp,
+                                                              int rows_per_block, int neg_plane) {
+  const int chunks = Kp >> 4;
+  const int64_t r0 = int64_t(blockIdx.x) * rows_per_block;
+  const int64_t nrows64 = rows - r0 < rows_per_block ? rows - r0 : rows_per_block;
+  const int nloc = int(nrows64) * chunks;
+  const int64_t plane = rows * int64_t(Kp);
+  const bool vec = ((K & 15) == 0) && ((reinterpret_cast<uintptr_t>(qc) & 15) == 0);
+  for (int l = threadIdx.x; l < nloc; l += blockDim.x) {
+    const int rl = l / chunks;
+    const int t0 = (l - rl * chunks) << 4;
+    const int64_t r = r0 + rl;
+    const uint8_t* src = qc + r * K + t0;
+    uint32_t w[4];
+    if (vec && t0 + 16 <= K) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(src));
+      w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        uint32_t acc = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int t = t0 + 4 * q + b;
+          const uint32_t byte = (t < K) ? uint32_t(__ldg(src + 4 * q + b)) : 0u;
+          acc |= byte << (8 * b);
+        }
+        w[q] = acc;
+      }
+    }
+    uint32_t re[4], im[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) qc4_to_s8(w[q], re[q], im[q]);
+    uint8_t* dst = z + r * Kp + t0;
+    *reinterpret_cast<uint4*>(dst) = make_uint4(re[0], re[1], re[2], re[3]);
+    *reinterpret_cast<uint4*>(dst + plane) = make_uint4(im[0], im[1], im[2], im[3]);
+    if (neg_plane)
+      *reinterpret_cast<uint4*>(dst + 2 * plane) =
+          make_uint4(__vsub4(0u, re[0]), __vsub4(0u, re[1]), __vsub4(0u, re[2]), __vsub4(0u, re[3]));
+  }
+}
+
 // FP6 operand planes: as qc_to_planes_kernel, but each plane row holds Kp
 // E3M2 codes packed 16 per 12 bytes (row pitch 3 Kp / 4 bytes), the global
 // form of the TMA's 16 x U6 type.  Exact for QC input, 3/4 of the FP8 bytes.
@@ -833,7 +879,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
     // ------------------------------------------------ MMA issuer (leader CTA)
     if (lane == 0 && leader) {
       const uint32_t fmt = args.fp6 ? kFmtE3M2 : kFmtE4M3;
-      const uint32_t idesc = idesc_f32acc(fmt, fmt, 256, 2 * kTile);
+      const uint32_t idesc =
+          args.s8 ? idesc_s32acc_s8(256, 2 * kTile) : idesc_f32acc(fmt, fmt, 256, 2 * kTile);
       int stage = 0, acc = 0;
       uint32_t phase = 0, acc_phase = 0;
       bool ok = true;
@@ -859,8 +906,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
             const uint64_t daim = sdesc_sw128_kmajor(plane(stage, 1) + 32 * s);
             const uint64_t dbx = sdesc_sw128_kmajor(plane(stage, 2) + 32 * s);
             const uint64_t dby = sdesc_sw128_kmajor(plane(stage, 3) + 32 * s);
-            mma_f8f6f4_pair(d, dare, dbx, idesc, (kb | s) != 0);
-            mma_f8f6f4_pair(d, daim, dby, idesc, 1);
+            if (args.s8) {
+              mma_i8_pair(d, dare, dbx, idesc, (kb | s) != 0);
+              mma_i8_pair(d, daim, dby, idesc, 1);
+            } else {
+              mma_f8f6f4_pair(d, dare, dbx, idesc, (kb | s) != 0);
+              mma_f8f6f4_pair(d, daim, dby, idesc, 1);
+            }
           }
           mma_commit_pair(empty_bar(stage));
           mma_commit_pair(map_shared(empty_bar(stage), 1));
@@ -920,6 +972,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
         tmem_ld_32x32b_x32(tb + 32u * c, re);
         tmem_ld_32x32b_x32(tb + uint32_t(kTile) + 32u * c, im);
         tmem_wait_ld();
+        if (args.s8) {  // exact S32 sums -> FP32
+#pragma unroll
+          for (int m = 0; m < 32; ++m) {
+            re[m] = __float_as_uint(float(int32_t(re[m])));
+            im[m] = __float_as_uint(float(int32_t(im[m])));
+          }
+        }
         const int64_t e0 = int64_t(i0) * (i0 + 1) / 2 + j;
         if constexpr (sizeof(Out2) == 8) {
           const int jt0 = jw - q * 32;  // first column of this CTA's 128
@@ -969,6 +1028,15 @@ cudaError_t launch_qc_to_planes(const uint8_t* qc, uint8_t* z, int64_t rows, int
   const int rpb = rows_per_block(Kp >> 4);
   const int64_t blocks = (rows + rpb - 1) / rpb;
   qc_to_planes_kernel<<<unsigned(blocks), 256, 0, s>>>(qc, z, rows, K, Kp, rpb, neg_plane ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_qc_to_planes_s8(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
+                                   cudaStream_t s, bool neg_plane) {
+  const int rpb = rows_per_block(Kp >> 4);
+  const int64_t blocks = (rows + rpb - 1) / rpb;
+  qc_to_planes_s8_kernel<<<unsigned(blocks), 256, 0, s>>>(qc, z, rows, K, Kp, rpb,
+                                                           neg_plane ? 1 : 0);
   return cudaGetLastError();
 }
 

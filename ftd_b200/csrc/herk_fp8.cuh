@@ -104,6 +104,9 @@ struct HerkArgs {
   // 1: Z holds packed FP6 E3M2 planes (TMA 16 x U6 type): the MMAs read E3M2
   // operands and each load delivers 3/4 of the FP8 bytes
   int32_t fp6;
+  // 1: Z holds signed 8-bit planes (QC values exact); CTA-pair kernel only:
+  // kind::i8 MMAs into S32 accumulators, converted to FP32 by the epilogue
+  int32_t s8;
 };
 
 // A plain single-segment argument block.
@@ -118,6 +121,9 @@ inline HerkArgs herk_args_default() {
 // neg_plane: also write plane 2 = -Re (CTA-pair kernel operand)
 cudaError_t launch_qc_to_planes(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
                                 cudaStream_t s, bool neg_plane = false);
+// Signed 8-bit planes (same layout as the E4M3 planes) for the s8 operand form.
+cudaError_t launch_qc_to_planes_s8(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
+                                   cudaStream_t s, bool neg_plane = false);
 // Packed FP6 E3M2 planes (row pitch 3 Kp / 4 bytes) for the fp6 operand form.
 cudaError_t launch_qc_to_planes6(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,
                                  cudaStream_t s, bool neg_plane = false);

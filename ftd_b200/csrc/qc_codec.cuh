@@ -36,6 +36,15 @@ __device__ __forceinline__ void qc4_to_e3m2(uint32_t w, uint32_t& re, uint32_t& 
   im = __byte_perm(kLo, kHi, si) | ((w << 2) & 0x20202020u);
 }
 
+// Four QC bytes -> signed 8-bit integers (two's complement, one per byte) of
+// the four Re and the four Im parts; sign-magnitude -0 becomes 0.
+__device__ __forceinline__ void qc4_to_s8(uint32_t w, uint32_t& re, uint32_t& im) {
+  const uint32_t mr = (w >> 4) & 0x07070707u, mi = w & 0x07070707u;
+  const uint32_t sr = ((w >> 7) & 0x01010101u) * 0xFFu, si = ((w >> 3) & 0x01010101u) * 0xFFu;
+  re = __vsub4(mr ^ sr, sr);  // per byte: sign ? -m : m
+  im = __vsub4(mi ^ si, si);
+}
+
 // Sixteen 6-bit codes (one per byte of c[0..3], byte b of c[q] = element
 // 4q + b) -> the 12-byte packed group of the TMA's 16 x U6 type: element e at
 // bits [6e, 6e + 6) of the little-endian 96-bit group.

@@ -260,6 +260,16 @@ __device__ __forceinline__ void tmem_cp_32x128b_warpx4_pair(uint32_t taddr, uint
   asm volatile("tcgen05.cp.cta_group::2.32x128b.warpx4 [%0], %1;" ::"r"(taddr), "l"(sdesc)
                : "memory");
 }
+// Signed 8-bit integer MMA over the CTA pair, S32 accumulation.
+__device__ __forceinline__ void mma_i8_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                            uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
 // Arrive on an mbarrier of the pair (shared::cluster address) once all
 // previously issued pair MMAs of this thread finish.
 __device__ __forceinline__ void mma_commit_pair(uint32_t bar_cluster) {
@@ -404,6 +414,12 @@ __device__ __forceinline__ void tmem_cp_32x128b_warpx4(uint32_t taddr, uint64_t 
 //   neg_a: negate A (valid for kind::f16 and kind::f8f6f4).
 // kind::f8f6f4 operand formats (instruction descriptor a/b format fields).
 constexpr uint32_t kFmtE4M3 = 0, kFmtE3M2 = 4;
+// kind::i8: signed 8-bit A and B, S32 accumulator, K-major.
+__host__ __device__ constexpr uint32_t idesc_s32acc_s8(uint32_t M, uint32_t N) {
+  return (2u << 4)                 // D format: S32
+         | (1u << 7) | (1u << 10)  // A, B: signed 8-bit
+         | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
 __host__ __device__ constexpr uint32_t idesc_f32acc(uint32_t a_fmt, uint32_t b_fmt, uint32_t M,
                                                     uint32_t N, uint32_t neg_a = 0) {
   return (1u << 4)                 // D format: F32

@@ -93,3 +93,27 @@ def test_compute_fp6_int4_exact_and_float_refused():
         A = torch.zeros(B, N, K, 2, device=DEV)
         with pytest.raises(FtdxError):
             c.herk(A, C, N, K, B, input=IN_FP32, compute=COMPUTE_FP6, output=OUT_FP32)
+
+
+# ------------------------------------------------ signed 8-bit operands
+S8_PAIR = 2 + 8  # CTA-pair kernel with kind::i8 MMAs and S32 accumulators
+
+
+@pytest.mark.parametrize("N,K,B", [(160, 256, 3), (130, 100, 2), (300, 1000, 2)])
+def test_s8_pair_bit_exact(N, K, B):
+    qc = oracle.gaussian_qc(700 + N + K, B, N, K, sigma=3.0)
+    want = oracle.herk_qc(qc, N, K, B).astype(np.float32)
+    assert np.array_equal(run(qc, N, K, B, S8_PAIR), want)
+
+
+def test_s8_pair_all_codes_alpha_beta_fp16():
+    N, K, B = 256, 512, 2
+    rng = np.random.default_rng(71)
+    qc = rng.integers(0, 256, size=(B, N, K), dtype=np.uint8)
+    assert np.array_equal(run(qc, N, K, B, S8_PAIR),
+                          oracle.herk_qc(qc, N, K, B).astype(np.float32))
+    C0 = rng.normal(size=(B, tri_size(N), 2)).astype(np.float32)
+    assert np.array_equal(run(qc, N, K, B, 2, alpha=0.5, beta=2.0, C0=C0),
+                          run(qc, N, K, B, S8_PAIR, alpha=0.5, beta=2.0, C0=C0))
+    assert np.array_equal(run(qc, N, K, B, 2, output=OUT_FP16),
+                          run(qc, N, K, B, S8_PAIR, output=OUT_FP16))

@@ -184,6 +184,6 @@ def test_tuner_considers_pair(tmp_path):
     C = torch.empty(B, tri_size(N), 2, device=DEV)
     with Correlator(verbosity=2) as c:
         win = c.tune(d, C, N, K, B)
-        assert win["store_mode"] in (0, 1, 2)
+        assert win["store_mode"] in (0, 1, 2, 10)  # 10: pair kernel on int8 operands
         torch.cuda.synchronize()
         assert np.array_equal(C.cpu().numpy(), oracle.herk_qc(qc, N, K, B).astype(np.float32))
