@@ -117,3 +117,10 @@ def test_s8_pair_all_codes_alpha_beta_fp16():
                           run(qc, N, K, B, S8_PAIR, alpha=0.5, beta=2.0, C0=C0))
     assert np.array_equal(run(qc, N, K, B, 2, output=OUT_FP16),
                           run(qc, N, K, B, S8_PAIR, output=OUT_FP16))
+
+
+@pytest.mark.parametrize("N,K,B", [(1, 1, 1), (7, 3, 2), (129, 17, 1), (257, 129, 2)])
+@pytest.mark.parametrize("store_mode", [0 + FP6, 2 + FP6, S8_PAIR])
+def test_operand_forms_edge_sizes(N, K, B, store_mode):
+    qc = oracle.gaussian_qc(800 + N + K, B, N, K, sigma=3.0)
+    assert np.array_equal(run(qc, N, K, B, store_mode), oracle.herk_qc(qc, N, K, B).astype(np.float32))

@@ -210,3 +210,23 @@ def test_nvfp4_pair_equals_single_cta(compute_name):
     assert np.isfinite(b).all()
     scale = np.abs(a).max()
     assert np.abs(a - b).max() <= 1e-5 * scale
+
+
+@pytest.mark.parametrize("N,K,B", [(1, 1, 1), (50, 8, 2), (113, 129, 1), (257, 64, 2)])
+@pytest.mark.parametrize("store_mode", [0, 2])
+def test_nvfp4_edge_sizes(N, K, B, store_mode):
+    # fewer inputs than one tile, one sample, sizes one past the tile and
+    # k-block edges: every element written, autocorrelations exact, the
+    # cross terms within NVFP4's bound of the FP64 product
+    from ftd_b200._lib import COMPUTE_FP4, COMPUTE_FP4_SPLIT
+    rng = np.random.default_rng(N * 1000 + K)
+    v = (rng.normal(size=(B, N, K)) + 1j * rng.normal(size=(B, N, K))).astype(np.complex64)
+    ref = oracle.herk_c128(v.astype(np.complex128), N, K, B)
+    # worst single-sample case: a component near 5 in block-scale units rounds
+    # by 1 (E2M1 spacing 2 above 4), ~20% of the sample, twice in a product
+    for compute, bound in ((COMPUTE_FP4, 0.5), (COMPUTE_FP4_SPLIT, 0.1)):
+        got = run_float(v, compute, store_mode)
+        assert np.isfinite(got).all()
+        err = oracle.correlation_errors(got, ref, N)
+        assert err["max_auto_rel"] < 1e-5
+        assert err["max_offdiag_norm"] < bound, (compute, err)
