@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--no-extra", action="store_true", help="skip the extra workload legs")
     p.add_argument("--leg", default=None,
                    choices=["nvfp4", "nvfp4split", "raw", "imaging", "xengine", "splitk",
-                            "precision"],
+                            "precision", "imaging_visbf"],
                    help="run one extra workload alone and print its JSON (profiling cases); "
                         "nvfp4 and nvfp4split use --inputs/--channels/--k")
     p.add_argument("--strategy", default=None,
@@ -570,6 +570,27 @@ def run_imaging_leg(torch, dev, n_ant=2048, n_chan=64, n_pol=2, ng=2048, n_beam=
                     "inverse + beam extraction, per grid tile of the channels that fit in 64 MiB"}
 
 
+# The reference's own VisBF benchmark (pol_mode A) on GH200: 1664 antennas,
+# Nf_eff = n_ch * n_time_inner = 16 * 2 = 32 visibility sets, 4096^2 grids,
+# 6,000,000 beams, FP16 FFT; per-stage mean times in ms
+# (scripts/bench_results_GH200/stages.csv, visbf_16ch_K128; config from
+# raw_visbf_16ch_K128_20260306_115016.log).
+VISBF_GH200_MS = {"pol_reduce": 0.49, "img_scatter": 1.81, "img_fft": 11.80, "img_beam": 5.29}
+
+
+def run_imaging_visbf_leg(torch, dev):
+    """Imaging at the reference VisBF benchmark's sizes (1664 antennas, 32
+    visibility sets x 2 pols, 4096^2 grids, 6,000,000 beams), beside the
+    reference's published GH200 stage times for the same stages (pol sum,
+    scatter, FFT, beams; different hardware, FP16 FFT there, FP32 here)."""
+    out = run_imaging_leg(torch, dev, n_ant=1664, n_chan=32, n_pol=2, ng=4096,
+                          n_beam=6_000_000, seed=18)
+    ref = sum(VISBF_GH200_MS.values())
+    out["reference_gh200_ms"] = {**VISBF_GH200_MS, "sum": ref}
+    out["speedup_vs_reference_gh200"] = ref / out["ms_per_step"]
+    return out
+
+
 def run_xengine_leg(torch, dev, n_ant=2048, K=1024, batch=128, seed=9):
     """XEngine-compatible path: [batch][K][n_ant] two's-complement (4,4)b
     blocks (2048 antennas x K=1024 x 128 = 268 MB) -> packed upper triangles
@@ -801,6 +822,8 @@ def run_leg(args):
         out = run_splitk_leg(torch, dev)
     elif args.leg == "precision":
         out = run_precision_leg(torch, dev)
+    elif args.leg == "imaging_visbf":
+        out = run_imaging_visbf_leg(torch, dev)
     else:
         out = run_xengine_leg(torch, dev)
     print(json.dumps(out), flush=True)

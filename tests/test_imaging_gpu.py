@@ -85,6 +85,28 @@ def test_grid_image_beams_random(n_pol, use_taper):
     assert np.all(beams[:, 4:] == 0)
 
 
+def test_long_beam_list_sorted_gather():
+    # 70,000 beams (past the length from which the pixels are sorted once per
+    # call and gathered in image order), repeats and off-image pixels
+    # included: every beam is the direct gather's value for its own pixel
+    n_ant, n_chan, ng = 40, 3, 64
+    vis, uv, freq, taper = case(77, n_ant, n_chan, 2, ng)
+    rng = np.random.default_rng(78)
+    pix = rng.integers(-2, ng + 2, size=(70000, 2))
+    ref_img = oracle.image_from_grid(oracle.image_grid(vis, uv, freq, n_ant, ng, 1.0, taper))
+    with Correlator() as c:
+        long_b = run(c, vis, uv, freq, n_ant, ng, 0, taper, pix=pix)
+        short_b = run(c, vis, uv, freq, n_ant, ng, 0, taper, pix=pix[:1000])
+        assert c.device_status() == 0
+    # two calls grid with FP32 atomics in different orders: equal to rounding
+    np.testing.assert_allclose(long_b[:, :1000], short_b, rtol=1e-4,
+                               atol=1e-6 * np.abs(short_b).max())
+    ref = oracle.beam_intensity(ref_img, [tuple(p) for p in pix[:2000]])
+    np.testing.assert_allclose(long_b[:, :2000], ref, rtol=1e-3, atol=1e-6 * np.abs(ref).max())
+    off = (pix[:, 0] < 0) | (pix[:, 0] >= ng) | (pix[:, 1] < 0) | (pix[:, 1] >= ng)
+    assert np.all(long_b[:, off] == 0)
+
+
 def test_large_triangle_auto_cross_split():
     # 3000 antennas: packed indices past 2^22, where a float square-root decode
     # of the row misclassifies baselines; every baseline at u = v = 0 with
