@@ -354,40 +354,52 @@ std::vector<Strategy> default_candidates(ftdx_handle h, bool fp32_out, bool pair
   return v;
 }
 
+// Candidates are interleaved: two warm-up rounds, then kTuneRounds timed
+// rounds in which every candidate runs once (each launch between its own pair
+// of events), and each candidate's median decides.  A part at its power limit
+// slows as it heats; interleaving gives every candidate the same drift, where
+// timing them one after the other would favour the first ones.
 ftdx_status tune_sweep(ftdx_handle h, const LaunchFn& launch, const std::vector<Strategy>& cands,
                        cudaStream_t s, TuneEntry* best_out) {
-  cudaEvent_t e0, e1;
-  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
-    return fail(h, FTDX_ERR_CUDA, "tuner events");
+  constexpr int kTuneRounds = 5;
+  const size_t nc = cands.size();
+  std::vector<cudaEvent_t> ev(2 * nc, nullptr);
+  ftdx_status st = FTDX_OK;
+  for (auto& e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) st = fail(h, FTDX_ERR_CUDA, "tuner events");
   const bool prof = h->profiling;
   h->profiling = false;
-  ftdx_status st = FTDX_OK;
+  std::vector<std::vector<float>> times(nc);
+  for (int w = 0; w < 2 && st == FTDX_OK; ++w)
+    for (size_t i = 0; i < nc && st == FTDX_OK; ++i) st = launch(cands[i], s);
+  for (int r = 0; r < kTuneRounds && st == FTDX_OK; ++r) {
+    for (size_t i = 0; i < nc && st == FTDX_OK; ++i) {
+      cudaEventRecord(ev[2 * i], s);
+      st = launch(cands[i], s);
+      cudaEventRecord(ev[2 * i + 1], s);
+    }
+    for (size_t i = 0; i < nc && st == FTDX_OK; ++i) {
+      float ms = 0.f;
+      cudaError_t ce = cudaEventSynchronize(ev[2 * i + 1]);
+      if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
+      if (ce != cudaSuccess) st = cuda_fail(h, ce, "tuner timing");
+      times[i].push_back(ms);
+    }
+  }
   TuneEntry best;
   best.ms = -1.f;
-  for (const Strategy& cand : cands) {
-    for (int w = 0; w < 2 && st == FTDX_OK; ++w) st = launch(cand, s);
-    if (st != FTDX_OK) break;
-    cudaEventRecord(e0, s);
-    const int reps = 3;
-    for (int r = 0; r < reps && st == FTDX_OK; ++r) st = launch(cand, s);
-    cudaEventRecord(e1, s);
-    if (st != FTDX_OK) break;
-    float ms = 0.f;
-    cudaError_t ce = cudaEventSynchronize(e1);
-    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
-    if (ce != cudaSuccess) {
-      st = cuda_fail(h, ce, "tuner timing");
-      break;
-    }
-    ms /= reps;
+  for (size_t i = 0; i < nc && st == FTDX_OK; ++i) {
+    std::vector<float> t = times[i];
+    std::nth_element(t.begin(), t.begin() + t.size() / 2, t.end());
+    const float ms = t[t.size() / 2];
     if (h->verbosity > 1)
-      fprintf(stderr, "ftdx tune: store=%d grid=%d splits=%d %.4f ms\n", cand.store_mode,
-              cand.grid, cand.splits, ms);
-    if (best.ms < 0.f || ms < best.ms) best = TuneEntry{cand, ms};
+      fprintf(stderr, "ftdx tune: store=%d grid=%d splits=%d %.4f ms (median of %d)\n",
+              cands[i].store_mode, cands[i].grid, cands[i].splits, ms, kTuneRounds);
+    if (best.ms < 0.f || ms < best.ms) best = TuneEntry{cands[i], ms};
   }
   h->profiling = prof;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  for (auto e : ev)
+    if (e) cudaEventDestroy(e);
   if (st == FTDX_OK && best_out) *best_out = best;
   return st;
 }
