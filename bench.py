@@ -416,7 +416,7 @@ def run_ours(args, rank, world, dist):
             peak_source = (f"max of cuBLASLt dense FP8 e4m3 ({peak:.0f}) and INT8 "
                            f"(torch._int_mm, {p8:.0f}) GEMMs 8192^3, measured in this run")
             peak = max(peak, p8)
-    kernel_name = "herk_fp8_pair_kernel" if (mode & 3) == 2 else "herk_fp8_tc_kernel"
+    kernel_name = "herk_fp8_pair_kernel" if (mode & 3) >= 2 else "herk_fp8_tc_kernel"
     prep_name = ("qc_to_planes6_kernel" if mode & 4 else
                  "qc_to_planes_s8_kernel" if mode & 8 else "qc_to_planes_kernel")
     traffic = None

@@ -33,6 +33,7 @@ constexpr int kStoreS8 = 8;   // with store mode 2: signed 8-bit operands, kind:
 struct Strategy {
   // 0: direct stores, 1: shared-memory staging + bulk copies,
   // 2: CTA-pair kernel (256 x 128 tiles on two SMs, direct stores);
+  // 3: CTA-pair kernel with bulk-copy stores for interior tiles;
   // + kStoreFp6: operands as packed FP6 E3M2 planes (QC input, exact);
   // + kStoreS8 (pair only): signed 8-bit planes, integer MMAs (QC input, exact)
   int store_mode = 0;

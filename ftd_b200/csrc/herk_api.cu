@@ -122,7 +122,7 @@ ftdx_status get_fp4_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStrea
 ftdx_status launch_fp4(ftdx_handle h, const HerkCall& c, const Strategy& strat, cudaStream_t s) {
   const int64_t rows = int64_t(c.N) * c.batch;
   const int split = c.compute == FTDX_COMPUTE_FP4_SPLIT ? 1 : 0;
-  const int pair = ((strat.store_mode & 3) == 2 && nvfp4_pair_limit() >= 1) ? 1 : 0;
+  const int pair = ((strat.store_mode & 3) >= 2 && nvfp4_pair_limit() >= 1) ? 1 : 0;
   ftdx_status st = ensure_workspace(h, nvfp4_workspace_bytes(c.N, c.batch, c.K, split, pair), s);
   const Plan* plan = nullptr;
   if (st == FTDX_OK)
@@ -144,7 +144,7 @@ bool fp6_ok(const HerkCall& c) {
 }
 
 bool use_pair(ftdx_handle h, const Strategy& strat) {
-  return (strat.store_mode & 3) == 2 && pair_grid_limit(h) >= 2;
+  return (strat.store_mode & 3) >= 2 && pair_grid_limit(h) >= 2;
 }
 
 // Split-K count a call actually uses: none for Kahan, the XEngine formats and
@@ -237,7 +237,7 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   args.chans = plan->d_chans;
   args.num_tiles = plan->num_tiles;
   args.out_fp16 = (c.output == FTDX_OUT_FP16) ? 1 : 0;
-  args.bulk_store = (strat.store_mode & 3) == 1 ? 1 : 0;
+  args.bulk_store = (strat.store_mode & 1) ? 1 : 0;  // modes 1 and 3
   args.fp6 = fp6 ? 1 : 0;
   args.s8 = s8 ? 1 : 0;
   args.out_format = c.out_format;
@@ -310,8 +310,13 @@ ftdx_status run_tune(ftdx_handle h, const HerkCall& c, cudaStream_t s, TuneEntry
                 : default_candidates(h, c.output == FTDX_OUT_FP32, true);
   if (is_fp4(c) && nvfp4_pair_limit() >= 1) cands.push_back(Strategy{2, 0});
   // QC input: the pair kernel on signed 8-bit operands (kind::i8, exact)
-  if (fp6_ok(c) && c.compute == FTDX_COMPUTE_FP8 && !c.comp && pair_grid_limit(h) >= 2)
+  if (fp6_ok(c) && c.compute == FTDX_COMPUTE_FP8 && !c.comp && pair_grid_limit(h) >= 2) {
     cands.push_back(Strategy{2 | kStoreS8, pair_grid_limit(h)});
+    if (c.output == FTDX_OUT_FP32) {  // the pair with bulk-copy stores (complex64 rows)
+      cands.push_back(Strategy{3, pair_grid_limit(h)});
+      cands.push_back(Strategy{3 | kStoreS8, pair_grid_limit(h)});
+    }
+  }
   const int kblocks = int(round_up(c.K, kStageK) / kStageK);
   if (!is_fp4(c) && !c.comp && plan->num_tiles < h->sm_count)
     for (int sp : {2, 4, 8, 16, 32})
@@ -470,10 +475,10 @@ void release_graphs(ftdx_handle h) {
   h->graphs.clear();
 }
 
-// Store modes 0..2, each optionally + kStoreFp6, or 2 + kStoreS8.
+// Store modes 0..3, each optionally + kStoreFp6, or 2 / 3 + kStoreS8.
 static bool valid_store_mode(int m) {
-  if (m < 0 || (m & 3) > 2 || (m & ~(3 | kStoreFp6 | kStoreS8)) != 0) return false;
-  return !(m & kStoreS8) || m == (2 | kStoreS8);
+  if (m < 0 || (m & ~(3 | kStoreFp6 | kStoreS8)) != 0) return false;
+  return !(m & kStoreS8) || m == (2 | kStoreS8) || m == (3 | kStoreS8);
 }
 
 // Text cache, one entry per line:
@@ -785,7 +790,7 @@ ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid) {
   if (!valid_store_mode(store_mode) || grid < -1)
     return fail(h, FTDX_ERR_INVALID_ARG, "set_strategy: store_mode %d / grid %d", store_mode,
                 grid);
-  if ((store_mode & 3) == 2) {
+  if ((store_mode & 3) >= 2) {
     cudaSetDevice(h->device);
     if (pair_grid_limit(h) < 2)
       return fail(h, FTDX_ERR_UNSUPPORTED, "set_strategy: no CTA pair fits on this device");

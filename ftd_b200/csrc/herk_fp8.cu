@@ -730,7 +730,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
             // half-uniform: all 128 columns of these 32 rows below the diagonal and n
             if (sector_ok && j0 + kTile - 1 < i0 && i0 + 31 < n) {
               auto* sec = reinterpret_cast<float2(*)[3][4]>(
-                  stg_base + (2 * half + (sec_it & 1)) * kSecBufBytes);
+                  stg_base + kSecOffset(half, int(sec_it & 1)));
               ++sec_it;
               float2* t0 = reinterpret_cast<float2*>(outc) + (int64_t(i0) * (i0 + 1) / 2 + j0);
               if (sc == 1.f)
@@ -783,7 +783,9 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
 constexpr int kPairPlane = 128 * kStageK;  // 16 KB: 128 rows of 128 samples
 constexpr int kPairStageBytes = 4 * kPairPlane;
 constexpr int kPairStages = 3;
-constexpr size_t kPairSmem = 1024 + size_t(kPairStages) * kPairStageBytes + kSecBytes + 256;
+// the epilogue area: sector buffers and, for the bulk store mode, staging
+constexpr size_t kPairSmem = 1024 + size_t(kPairStages) * kPairStageBytes + kStgBytes + 256;
+static_assert(kPairSmem <= 232448, "shared memory per CTA");
 
 template <typename OutT>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
@@ -791,7 +793,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
   extern __shared__ uint8_t smem_dyn[];
   uint8_t* smem = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
   uint8_t* sec_base = smem + kPairStages * kPairStageBytes;  // epilogue shared sectors
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sec_base + kSecBytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sec_base + kStgBytes);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kPairStages + 5);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const uint32_t smem0 = smem_u32(smem);
@@ -962,8 +964,64 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
       Out2* outc = cd.out_ptr ? reinterpret_cast<Out2*>(cd.out_ptr) : out + cd.out0;
       const uint32_t tb = tmem_base + (uint32_t(q * 32) << 16) + uint32_t(acc * kAccCols);
       const float sc = args.alpha * (args.chan_scale ? args.chan_scale[td.ch] : 1.f);
+      const int jt0 = jw - q * 32;  // first of this CTA's 128 columns
+      bool bulk_tile = false;
+      if constexpr (sizeof(Out2) == 8) {
+        bulk_tile = args.bulk_store && args.alpha == 1.f && args.beta == 0.f && !args.kahan &&
+                    args.chan_scale == nullptr && jt0 + 127 < ib && ib + kTile <= n;
+      }
+      if (bulk_tile) {
+        // Interior tile, as the single-CTA kernel's bulk mode: 8 rows at a
+        // time staged in shared memory (keeping each row's 16-byte phase),
+        // one bulk copy per row; a row starting 8 mod 16 stores its first
+        // and last element directly.
+        const uint32_t stg = smem_u32(sec_base) + uint32_t(half * 2 * kStgRows * kStgRowBytes);
+        const bool issuer = (q == 0) && (lane < kStgRows);
 #pragma unroll 1
-      for (int cc = 0; cc < kChunks; ++cc) {
+        for (int sub = 0; sub < (kTile / 2) / kStgRows; ++sub) {
+          const int is = ib + half * (kTile / 2) + sub * kStgRows;
+          const uint32_t col = uint32_t(half * (kTile / 2) + sub * kStgRows);
+          uint32_t re[kStgRows], im[kStgRows];
+          __syncwarp();
+          tmem_ld_32x32b_x8(tb + col, re);
+          tmem_ld_32x32b_x8(tb + uint32_t(kTile) + col, im);
+          tmem_wait_ld();
+          if (args.s8) {  // exact S32 sums -> FP32
+#pragma unroll
+            for (int m = 0; m < kStgRows; ++m) {
+              re[m] = __float_as_uint(float(int32_t(re[m])));
+              im[m] = __float_as_uint(float(int32_t(im[m])));
+            }
+          }
+          const uint32_t buf = stg + uint32_t((sub & 1) * kStgRows * kStgRowBytes);
+#pragma unroll
+          for (int m = 0; m < kStgRows; ++m) {
+            const int i = is + m;
+            Out2* g = outc + int64_t(i) * (i + 1) / 2 + jt0;
+            const uint32_t ph = uint32_t(reinterpret_cast<uintptr_t>(g) & 8u);
+            st_shared_v2(buf + uint32_t(m * kStgRowBytes) + ph + 8u * uint32_t(q * 32 + lane),
+                         re[m], im[m]);
+            if (ph && ((q == 0 && lane == 0) || (q == 3 && lane == 31)))
+              put(outc + int64_t(i) * (i + 1) / 2 + j, __uint_as_float(re[m]),
+                  __uint_as_float(im[m]));
+          }
+          fence_proxy_async_smem();
+          named_bar_sync(bar_id, 128);
+          if (issuer) {
+            const int i = is + lane;
+            Out2* g = outc + int64_t(i) * (i + 1) / 2 + jt0;
+            const bool odd = (reinterpret_cast<uintptr_t>(g) & 8u) != 0;
+            const uint32_t src = buf + uint32_t(lane * kStgRowBytes) + (odd ? 16u : 0u);
+            bulk_store(odd ? static_cast<void*>(g + 1) : static_cast<void*>(g), src,
+                       odd ? uint32_t((kTile - 2) * 8) : uint32_t(kTile * 8));
+            bulk_commit();
+            bulk_wait_read<1>();  // the other buffer is free again
+          }
+          named_bar_sync(bar_id, 128);
+        }
+      }
+#pragma unroll 1
+      for (int cc = 0; cc < kChunks && !bulk_tile; ++cc) {
         const int c = half * kChunks + cc;
         const int i0 = ib + 32 * c;
         if (i0 + 31 < jw || i0 >= n) continue;  // warp-uniform: nothing to store
@@ -984,7 +1042,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
           const int jt0 = jw - q * 32;  // first column of this CTA's 128
           if (sector_ok && jt0 + 127 < i0 && i0 + 31 < n) {  // half-uniform
             auto* sec = reinterpret_cast<float2(*)[3][4]>(
-                sec_base + (2 * half + (sec_it & 1)) * kSecBufBytes);
+                sec_base + kSecOffset(half, int(sec_it & 1)));
             ++sec_it;
             float2* t0 = reinterpret_cast<float2*>(outc) + (int64_t(i0) * (i0 + 1) / 2 + jt0);
             if (sc == 1.f)
@@ -1005,6 +1063,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
         acc_phase ^= 1u;
       }
     }
+    if (q == 0 && lane < kStgRows) bulk_wait<0>();  // bulk stores complete before the CTA exits
   }
 
   tc_fence_before();

@@ -124,3 +124,22 @@ def test_s8_pair_all_codes_alpha_beta_fp16():
 def test_operand_forms_edge_sizes(N, K, B, store_mode):
     qc = oracle.gaussian_qc(800 + N + K, B, N, K, sigma=3.0)
     assert np.array_equal(run(qc, N, K, B, store_mode), oracle.herk_qc(qc, N, K, B).astype(np.float32))
+
+
+# ------------------------------------------------ CTA pair with bulk-copy stores
+@pytest.mark.parametrize("mode", [3, 3 + 8])
+@pytest.mark.parametrize("N,K,B", [(640, 192, 2), (1000, 130, 1), (300, 64, 3)])
+def test_pair_bulk_stores_bit_exact(mode, N, K, B):
+    # store mode 3: interior tiles (all 128 columns of a CTA below every row,
+    # rows inside n) leave through shared memory and one bulk copy per row;
+    # the others through the direct / sector path; 3 + 8 on int8 operands
+    qc = oracle.gaussian_qc(1000 + N + K + mode, B, N, K, sigma=3.0)
+    want = oracle.herk_qc(qc, N, K, B).astype(np.float32)
+    assert np.array_equal(run(qc, N, K, B, mode), want)
+
+
+def test_pair_bulk_stores_fall_back_for_alpha_fp16():
+    N, K, B = 640, 128, 2
+    qc = oracle.gaussian_qc(1100, B, N, K)
+    assert np.array_equal(run(qc, N, K, B, 2, alpha=0.5), run(qc, N, K, B, 3, alpha=0.5))
+    assert np.array_equal(run(qc, N, K, B, 2, output=OUT_FP16), run(qc, N, K, B, 3, output=OUT_FP16))
