@@ -143,3 +143,24 @@ def test_pair_bulk_stores_fall_back_for_alpha_fp16():
     qc = oracle.gaussian_qc(1100, B, N, K)
     assert np.array_equal(run(qc, N, K, B, 2, alpha=0.5), run(qc, N, K, B, 3, alpha=0.5))
     assert np.array_equal(run(qc, N, K, B, 2, output=OUT_FP16), run(qc, N, K, B, 3, output=OUT_FP16))
+
+
+@pytest.mark.parametrize("mode", [1, 3, 10, 11])
+def test_strategies_under_graph_replay(mode):
+    # the bench replays the tuned strategy as a captured CUDA graph: every
+    # store mode / operand form stays bit-exact across replays
+    N, K, B = 640, 256, 3
+    qc = oracle.gaussian_qc(1200 + mode, B, N, K)
+    want = oracle.herk_qc(qc, N, K, B).astype(np.float32)
+    d = torch.from_numpy(qc.reshape(-1)).to(DEV)
+    C = torch.empty(B, tri_size(N), 2, device=DEV)
+    with Correlator() as c:
+        c.set_strategy(mode, 0)
+        c.init_herk(N, K, B)
+        c.set_graph_mode(True)
+        for _ in range(3):
+            C.fill_(float("nan"))
+            c.herk(d, C, N, K, B, input=IN_INT4, output=OUT_FP32, tune=False)
+            torch.cuda.synchronize()
+            assert np.array_equal(C.cpu().numpy(), want)
+        assert c.graph_count() >= 1 and c.device_status() == 0
