@@ -164,3 +164,23 @@ def test_strategies_under_graph_replay(mode):
             torch.cuda.synchronize()
             assert np.array_equal(C.cpu().numpy(), want)
         assert c.graph_count() >= 1 and c.device_status() == 0
+
+
+@pytest.mark.parametrize("bad", [-1, 9, 12, 13, 14, 15, 16, 32, 2 + 8 + 4])
+def test_invalid_store_modes_refused(bad):
+    # 8 (int8 operands) only with the pair modes 2 / 3, never with 4 (FP6);
+    # no bits above 8
+    with Correlator() as c:
+        with pytest.raises(FtdxError):
+            c.set_strategy(bad, 0)
+
+
+def test_fp6_compute_with_kahan_refused():
+    N, K, B = 64, 32, 1
+    qc = oracle.gaussian_qc(1300, B, N, K)
+    d = torch.from_numpy(qc.reshape(-1)).to(DEV)
+    S = torch.zeros(B, tri_size(N), 2, device=DEV)
+    comp = torch.zeros_like(S)
+    with Correlator() as c:
+        with pytest.raises(FtdxError):
+            c.herk_kahan(d, S, comp, N, K, B, input=IN_INT4, compute=COMPUTE_FP6)
