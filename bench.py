@@ -387,10 +387,12 @@ def run_ours(args, rank, world, dist):
         e2e = run_e2e(torch, args, dev, qc, N, K, B, flops, world, dist)
 
     batched = precision = differentiation = raw_layout = imaging = xengine = splitk = None
+    imaging_visbf = None
     if not args.no_extra:
         batched = run_batched_leg(torch, dev)
         raw_layout = run_ftd_leg(torch, dev)
         imaging = run_imaging_leg(torch, dev)
+        imaging_visbf = run_imaging_visbf_leg(torch, dev)
         xengine = run_xengine_leg(torch, dev)
         splitk = run_splitk_leg(torch, dev)
         precision = run_precision_leg(torch, dev)
@@ -455,6 +457,7 @@ def run_ours(args, rank, world, dist):
         "batched_uneven_flagged": batched,
         "raw_layout_fused_corner_turn": raw_layout,
         "imaging_from_triangles": imaging,
+        "imaging_at_reference_visbf_sizes": imaging_visbf,
         "xengine_upper_triangle": xengine,
         "split_k_long_integration": splitk,
         "precision_modes": precision,
