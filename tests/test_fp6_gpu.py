@@ -29,8 +29,8 @@ def run(qc, N, K, B, store_mode, output=OUT_FP32, alpha=1.0, beta=0.0, C0=None):
     return C.cpu().numpy()
 
 
-@pytest.mark.parametrize("store_mode", [0, 1, 2])
-@pytest.mark.parametrize("N,K,B", [(160, 256, 3), (130, 100, 2), (300, 1000, 2)])
+@pytest.mark.parametrize("store_mode", [0, 1, 2, 3])
+@pytest.mark.parametrize("N,K,B", [(160, 256, 3), (130, 100, 2), (300, 1000, 2), (640, 96, 2)])
 def test_fp6_bit_exact(store_mode, N, K, B):
     qc = oracle.gaussian_qc(600 + N + K + store_mode, B, N, K, sigma=3.0)
     want = oracle.herk_qc(qc, N, K, B).astype(np.float32)
