@@ -394,3 +394,113 @@ def xengine(payload: np.ndarray, n_ant: int, K: int, batch: int, mat_format: int
         return C
     r, c = np.triu_indices(n_ant)
     return C[:, r, c]
+
+
+# ----------------------------------------------------------------- NVFP4
+# A restatement of the library's NVFP4 quantisation (its own format; the
+# reference has none) in IEEE float32 steps, so that the GPU result can be
+# checked against the same quantised operands to FP32 accumulation rounding.
+# Per input row an FP32 scale g = amax_row / (6 * 448) (1 for an empty row);
+# per block of 16 values (8 complex samples, Re/Im interleaved) a UE4M3 scale
+# b = the smallest E4M3 value >= amax_blk / (6 g) (at most 448); elements
+# E2M1(v * (1 / (g b))), round to nearest with ties to the even code,
+# saturating at 6.  Split mode: the residual x - code * (g b) (one rounding,
+# as a fused multiply-add) quantised again with its own block scale.
+E2M1_GRID = np.array([0.0, 0.5, 1.0, 1.5, 2.0, 3.0, 4.0, 6.0])
+
+
+def _e4m3_positive() -> np.ndarray:
+    vals = []
+    for e in range(16):
+        for m in range(8):
+            if e == 15 and m == 7:
+                continue  # NaN
+            vals.append(m / 8 * 2.0 ** -6 if e == 0 else (1 + m / 8) * 2.0 ** (e - 7))
+    return np.array(sorted(set(vals)))
+
+
+_E4M3 = _e4m3_positive()
+
+
+def ue4m3_ceil(v: np.ndarray) -> np.ndarray:
+    """Smallest E4M3 value >= v (float32 in), 448 at most, 0 for v <= 0."""
+    v = np.asarray(v, dtype=np.float64)
+    idx = np.searchsorted(_E4M3, v, side="left")
+    out = _E4M3[np.minimum(idx, len(_E4M3) - 1)]
+    return np.where(v > 0, out, 0.0).astype(np.float32)
+
+
+def e2m1_rne(x: np.ndarray) -> np.ndarray:
+    """E2M1 value of float32 x: nearest grid value, ties to the even code,
+    saturating at +-6."""
+    a = np.minimum(np.abs(np.asarray(x, dtype=np.float64)), 6.0)
+    d = np.abs(a[..., None] - E2M1_GRID)
+    best = d.min(axis=-1, keepdims=True)
+    cand = d == best
+    codes = np.arange(8)
+    # among equally near codes take the even one (ties), else the only one
+    score = np.where(cand, np.where(codes % 2 == 0, 0, 1), 9)
+    q = E2M1_GRID[np.argmin(score, axis=-1)]
+    return np.copysign(q, x).astype(np.float32)
+
+
+def _nvfp4_pass(x: np.ndarray, g: np.ndarray):
+    """Quantise float32 values x[..., nblk, 16] under row scales g[..., 1, 1]:
+    (dequantised values / g, block scales)."""
+    f32 = np.float32
+    amax = np.abs(x).max(axis=-1, keepdims=True).astype(f32)
+    b = ue4m3_ceil((amax / (f32(6.0) * g)).astype(f32))
+    with np.errstate(divide="ignore"):
+        inv = np.where(b > 0, f32(1.0) / (g * b).astype(f32), f32(0.0)).astype(f32)
+    codes = e2m1_rne((x * inv).astype(f32))
+    return codes.astype(np.float64) * b.astype(np.float64), b
+
+
+def nvfp4_quantize(v: np.ndarray, split: bool = False):
+    """Complex64 voltages [batch, N, K] -> (hi, lo or None, g): the dequantised
+    operands as complex128 without the row scale (the MMA operands code x
+    block scale), and the float32 row scales g [batch, N]."""
+    f32 = np.float32
+    B, N, K = v.shape
+    kp = (K + 7) // 8 * 8
+    x = np.zeros((B, N, kp, 2), dtype=f32)
+    x[:, :, :K, 0] = v.real
+    x[:, :, :K, 1] = v.imag
+    m = np.abs(x).reshape(B, N, -1).max(axis=-1).astype(f32)
+    g = np.where((m > 0) & (m < f32(3.0e38)), m / f32(6.0 * 448.0), f32(1.0)).astype(f32)
+    xb = x.reshape(B, N, kp // 8, 16)
+    gb = g[:, :, None, None]
+    hi, b = _nvfp4_pass(xb, gb)
+    lo = None
+    if split:
+        step = (gb.astype(f32) * b.astype(f32)).astype(f32).astype(np.float64)
+        codes = hi / np.where(b > 0, b, 1.0)
+        resid = (xb.astype(np.float64) - codes * step).astype(f32)
+        lo, _ = _nvfp4_pass(resid, gb)
+    def cplx(a):
+        a = a.reshape(B, N, kp, 2)[:, :, :K]
+        return a[..., 0] + 1j * a[..., 1]
+    return cplx(hi), (cplx(lo) if split else None), g
+
+
+def herk_nvfp4(v: np.ndarray, split: bool = False) -> np.ndarray:
+    """Packed lower triangles [batch, P, 2] (float64) of the NVFP4 product:
+    g_i g_j sum_t q_i q_j^* over the quantised operands (split: hi hi + hi lo
+    + lo hi), autocorrelations the exact sum |v|^2 rounded to float32."""
+    B, N, K = v.shape
+    hi, lo, g = nvfp4_quantize(v, split)
+    R = np.einsum("bik,bjk->bij", hi, hi.conj())
+    if split:
+        R += np.einsum("bik,bjk->bij", lo, hi.conj()) + np.einsum("bik,bjk->bij", hi, lo.conj())
+    gg = g.astype(np.float64)
+    R *= gg[:, :, None] * gg[:, None, :]
+    pw = (v.real.astype(np.float64) ** 2 + v.imag.astype(np.float64) ** 2).sum(axis=-1)
+    pw = pw.astype(np.float32)
+    i, j = np.tril_indices(N)
+    order = np.lexsort((j, i))
+    i, j = i[order], j[order]
+    out = np.stack([R[:, i, j].real, R[:, i, j].imag], axis=-1)
+    d = i == j
+    out[:, d, 0] = pw[:, i[d]]
+    out[:, d, 1] = 0.0
+    return out

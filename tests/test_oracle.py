@@ -225,3 +225,34 @@ def test_xengine_upper_packing_and_hermitian():
             assert k == r * n - r * (r - 1) // 2 + c - r
             assert tri[0, k] == full[0, r, c]
             k += 1
+
+
+def test_nvfp4_restatement_exact_on_representable_input():
+    # E2M1 values times per-block powers of two with a 6 in every block: the
+    # restated quantiser returns the input up to the rounding of the float32
+    # row scale g = amax / 2688 (codes x block scale exact), and the split
+    # residual is that rounding alone
+    rng = np.random.default_rng(5)
+    B, N, K = 2, 9, 32
+    e = rng.choice(oracle.E2M1_GRID, size=(B, N, K, 2)) * rng.choice([-1.0, 1.0], size=(B, N, K, 2))
+    blocks = e.reshape(B, N, K // 8, 16)
+    blocks[..., 0] = 6.0
+    blocks *= 2.0 ** rng.integers(-2, 1, size=(B, N, K // 8, 1))
+    v = blocks.reshape(B, N, K, 2)
+    vc = (v[..., 0] + 1j * v[..., 1]).astype(np.complex64)
+    hi, lo, g = oracle.nvfp4_quantize(vc, split=True)
+    deq = hi * g[..., None].astype(np.float64)
+    assert np.abs(deq - vc).max() <= 1e-6 * np.abs(vc).max()
+    assert np.abs(lo).max() <= 1e-5 * np.abs(hi).max()
+    got = oracle.herk_nvfp4(vc)
+    ref = oracle.herk_c128(vc.astype(np.complex128), N, K, B)
+    assert np.abs(got - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+def test_nvfp4_restatement_rounding_rules():
+    x = np.array([0.25, 0.75, 1.25, 1.75, 2.5, 3.5, 5.0, 7.0, -0.75, 0.2, 0.3], np.float32)
+    assert np.array_equal(oracle.e2m1_rne(x),
+                          np.array([0, 1, 1, 2, 2, 4, 4, 6, -1, 0, 0.5], np.float32))
+    v = np.array([0.0, 1.0, 1.01, 447.0, 500.0, 0.001], np.float32)
+    assert np.array_equal(oracle.ue4m3_ceil(v),
+                          np.array([0, 1, 1.125, 448, 448, 2.0 ** -9], np.float32))

@@ -230,3 +230,34 @@ def test_nvfp4_edge_sizes(N, K, B, store_mode):
         err = oracle.correlation_errors(got, ref, N)
         assert err["max_auto_rel"] < 1e-5
         assert err["max_offdiag_norm"] < bound, (compute, err)
+
+
+@pytest.mark.parametrize("store_mode", [0, 2])
+@pytest.mark.parametrize("kind", ["rfi", "gauss"])
+def test_nvfp4_matches_restated_quantiser(store_mode, kind):
+    # the GPU result against oracle.herk_nvfp4: the same quantised operands
+    # (row scale, rounded-up UE4M3 block scales, E2M1 round-to-nearest-even;
+    # split: the fused residual), products summed in FP64.  What is left is
+    # the FP32 accumulation of the MMAs and the FP32 epilogue scaling (measured
+    # 1e-8..6e-7 of the largest element): bound 1e-6 plain, 1e-5 split (room
+    # for a lo code flipped by the residual's last-bit rounding, one lo
+    # quantum).  Autocorrelations: float32 of FP64 sums.
+    from ftd_b200._lib import COMPUTE_FP4, COMPUTE_FP4_SPLIT
+    B, N, K = 2, 300, 256
+    if kind == "rfi":
+        v = oracle.workload4_voltages(410, B, N, K)
+    else:
+        rng = np.random.default_rng(411)
+        v = (rng.normal(size=(B, N, K)) + 1j * rng.normal(size=(B, N, K))).astype(np.complex64)
+    i, j = np.tril_indices(N)
+    order = np.lexsort((j, i))
+    diag = (i[order] == j[order])
+    for compute, split, tol in ((COMPUTE_FP4, False, 1e-6), (COMPUTE_FP4_SPLIT, True, 1e-5)):
+        got = run_float(v, compute, store_mode).astype(np.float64)
+        ref = oracle.herk_nvfp4(v, split)
+        scale = np.abs(ref).max()
+        err = np.abs(got - ref)
+        print(kind, store_mode, split, "max rel err vs restated quantiser",
+              err[:, ~diag].max() / scale)
+        assert err[:, ~diag].max() <= tol * scale
+        np.testing.assert_allclose(got[:, diag, 0], ref[:, diag, 0], rtol=1e-6)
