@@ -504,3 +504,64 @@ def herk_nvfp4(v: np.ndarray, split: bool = False) -> np.ndarray:
     out[:, d, 0] = pw[:, i[d]]
     out[:, d, 1] = 0.0
     return out
+
+
+# ----------------------------------------------------------------- FP8 (float input)
+# The per-channel-scaled E4M3 quantisation of float voltages (compute modes
+# FP8 and FP8 split): s = 448 / amax_channel (1 for an empty channel);
+# hi = E4M3(v s), round to nearest with ties to the even code, saturating at
+# 448 (subnormals down to 2^-9); split: lo = E4M3(v s - hi) in float32.
+# The result is scaled by 1 / (s s).
+def _e4m3_table():
+    vals, codes = [], []
+    for c in range(127):  # positive finite codes (0x7F is NaN)
+        e, m = c >> 3, c & 7
+        vals.append(m / 8 * 2.0 ** -6 if e == 0 else (1 + m / 8) * 2.0 ** (e - 7))
+        codes.append(c)
+    return np.array(vals), np.array(codes)
+
+
+_E4M3_VALS, _E4M3_CODES = _e4m3_table()
+
+
+def e4m3_rne(x: np.ndarray) -> np.ndarray:
+    """E4M3 value of float32 x: nearest, ties to the even code, saturating at
+    +-448."""
+    x = np.asarray(x, dtype=np.float64)
+    a = np.minimum(np.abs(x), 448.0)
+    idx = np.clip(np.searchsorted(_E4M3_VALS, a), 1, len(_E4M3_VALS) - 1)
+    lo, hi = _E4M3_VALS[idx - 1], _E4M3_VALS[idx]
+    dlo, dhi = a - lo, hi - a
+    pick_hi = (dhi < dlo) | ((dhi == dlo) & (_E4M3_CODES[idx] % 2 == 0))
+    q = np.where(pick_hi, hi, lo)
+    q = np.where(a == 0, 0.0, q)
+    return np.copysign(q, x).astype(np.float32)
+
+
+def herk_fp8_scaled(v: np.ndarray, split: bool = False) -> np.ndarray:
+    """Packed lower triangles [batch, P, 2] (float64) of the per-channel-scaled
+    E4M3 product of complex64 voltages [batch, N, K] (split: hi hi + lo hi +
+    hi lo), Im of the diagonal 0."""
+    f32 = np.float32
+    B, N, K = v.shape
+    re = v.real.astype(f32)
+    im = v.imag.astype(f32)
+    m = np.maximum(np.abs(re), np.abs(im)).reshape(B, -1).max(axis=-1).astype(f32)
+    s = np.where((m > 0) & (m < f32(3.0e38)), f32(448.0) / m, f32(1.0)).astype(f32)
+    out_scale = (f32(1.0) / (s * s).astype(f32)).astype(f32)
+    sb = s[:, None, None]
+    xr, xi = (re * sb).astype(f32), (im * sb).astype(f32)
+    hr, hi_ = e4m3_rne(xr), e4m3_rne(xi)
+    h = hr.astype(np.float64) + 1j * hi_.astype(np.float64)
+    R = np.einsum("bik,bjk->bij", h, h.conj())
+    if split:
+        lr, li = e4m3_rne((xr - hr).astype(f32)), e4m3_rne((xi - hi_).astype(f32))
+        lo = lr.astype(np.float64) + 1j * li.astype(np.float64)
+        R += np.einsum("bik,bjk->bij", lo, h.conj()) + np.einsum("bik,bjk->bij", h, lo.conj())
+    R *= out_scale.astype(np.float64)[:, None, None]
+    i, j = np.tril_indices(N)
+    order = np.lexsort((j, i))
+    i, j = i[order], j[order]
+    out = np.stack([R[:, i, j].real, R[:, i, j].imag], axis=-1)
+    out[:, i == j, 1] = 0.0
+    return out

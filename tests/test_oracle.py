@@ -256,3 +256,11 @@ def test_nvfp4_restatement_rounding_rules():
     v = np.array([0.0, 1.0, 1.01, 447.0, 500.0, 0.001], np.float32)
     assert np.array_equal(oracle.ue4m3_ceil(v),
                           np.array([0, 1, 1.125, 448, 448, 2.0 ** -9], np.float32))
+
+
+def test_e4m3_restatement_rounding_rules():
+    # ties to the even code, saturation at 448, subnormals (spacing 2^-9)
+    x = np.array([1.0625, 1.1875, 448.0, 480.0, 1000.0, 2.0 ** -10, 3 * 2.0 ** -10, -1.0625, 0.0],
+                 np.float32)
+    want = np.array([1.0, 1.25, 448.0, 448.0, 448.0, 0.0, 2.0 ** -8, -1.0, 0.0], np.float32)
+    assert np.array_equal(oracle.e4m3_rne(x), want)

@@ -261,3 +261,19 @@ def test_nvfp4_matches_restated_quantiser(store_mode, kind):
               err[:, ~diag].max() / scale)
         assert err[:, ~diag].max() <= tol * scale
         np.testing.assert_allclose(got[:, diag, 0], ref[:, diag, 0], rtol=1e-6)
+
+
+@pytest.mark.parametrize("store_mode", [0, 2])
+def test_fp8_float_modes_match_restated_quantiser(store_mode):
+    # per-channel-scaled E4M3 (and hi + lo split) of float voltages against
+    # oracle.herk_fp8_scaled: the same quantised operands summed in FP64; the
+    # rest is FP32 accumulation and the FP32 scale 1 / s^2 (bound 1e-6 of the
+    # largest element, 1e-5 split)
+    B, N, K = 2, 300, 256
+    v = oracle.workload4_voltages(412, B, N, K)
+    for compute, split, tol in ((COMPUTE_FP8, False, 1e-6), (COMPUTE_FP8_SPLIT, True, 1e-5)):
+        got = run_float(v, compute, store_mode).astype(np.float64)
+        ref = oracle.herk_fp8_scaled(v, split)
+        err = np.abs(got - ref).max() / np.abs(ref).max()
+        print("fp8", store_mode, split, "max rel err vs restated quantiser", err)
+        assert err <= tol
