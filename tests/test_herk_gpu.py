@@ -117,9 +117,13 @@ def test_fp16_input(corr):
     np.testing.assert_allclose(C.double().cpu().numpy(), ref, rtol=2e-3, atol=2e-2)
 
 
-def test_dsa2000_scale_spot_rows():
+# None: the autotuner's choice on this GPU; then every strategy it can pick
+# for QC input: 1 single CTA + bulk stores, 2 CTA pair, 3 pair + bulk stores,
+# 10 / 11 the pair on int8 operands
+@pytest.mark.parametrize("strategy", [None, 1, 2, 3, 10, 11])
+def test_dsa2000_scale_spot_rows(strategy):
     # 4096 inputs x 64 channels x K = 1024 (the DSA-2000 configuration): full
-    # output on the GPU, exact check of row blocks in two channels and of the
+    # output on the GPU, exact check of row blocks in three channels and of the
     # whole diagonal (sum |v|^2) of every channel.
     N, K, B = 4096, 1024, 64
     g = torch.Generator(device=DEV).manual_seed(3)
@@ -130,9 +134,13 @@ def test_dsa2000_scale_spot_rows():
         return torch.where(v < 0, 8 | (-v), v)
     qc = ((nib(re) << 4) | nib(im)).to(torch.uint8)
     C = torch.empty(B, tri_size(N), 2, device=DEV)
+    C.fill_(float("nan"))
     with Correlator() as c:
-        c.herk(qc, C, N, K, B, input=IN_INT4, output=OUT_FP32)
+        if strategy is not None:
+            c.set_strategy(strategy, 0)
+        c.herk(qc, C, N, K, B, input=IN_INT4, output=OUT_FP32, tune=strategy is None)
         assert c.device_status() == 0
+    assert not torch.isnan(C).any()
     diag_idx = torch.arange(N, device=DEV, dtype=torch.int64)
     diag_idx = diag_idx * (diag_idx + 1) // 2 + diag_idx
     power = (re * re + im * im).sum(-1)
