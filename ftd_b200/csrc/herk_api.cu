@@ -359,14 +359,17 @@ std::vector<Strategy> default_candidates(ftdx_handle h, bool fp32_out, bool pair
   return v;
 }
 
-// Candidates are interleaved: two warm-up rounds, then kTuneRounds timed
-// rounds in which every candidate runs once (each launch between its own pair
-// of events), and each candidate's median decides.  A part at its power limit
+// Candidates are interleaved: a pre-heat (kTunePreheat launches of the first
+// candidate, so that the sweep runs at the clock a sustained run settles to
+// under the power limit), two warm-up rounds, then kTuneRounds timed rounds in
+// which every candidate runs once (each launch between its own pair of
+// events), and each candidate's median decides.  A part at its power limit
 // slows as it heats; interleaving gives every candidate the same drift, where
 // timing them one after the other would favour the first ones.
 ftdx_status tune_sweep(ftdx_handle h, const LaunchFn& launch, const std::vector<Strategy>& cands,
                        cudaStream_t s, TuneEntry* best_out) {
   constexpr int kTuneRounds = 5;
+  constexpr int kTunePreheat = 50;
   const size_t nc = cands.size();
   std::vector<cudaEvent_t> ev(2 * nc, nullptr);
   ftdx_status st = FTDX_OK;
@@ -375,6 +378,7 @@ ftdx_status tune_sweep(ftdx_handle h, const LaunchFn& launch, const std::vector<
   const bool prof = h->profiling;
   h->profiling = false;
   std::vector<std::vector<float>> times(nc);
+  for (int w = 0; w < kTunePreheat && nc > 1 && st == FTDX_OK; ++w) st = launch(cands[0], s);
   for (int w = 0; w < 2 && st == FTDX_OK; ++w)
     for (size_t i = 0; i < nc && st == FTDX_OK; ++i) st = launch(cands[i], s);
   for (int r = 0; r < kTuneRounds && st == FTDX_OK; ++r) {
