@@ -234,7 +234,7 @@ struct Fp4Args {
   const uint8_t* sfa;      // scale atoms of the x rows (A)
   const uint8_t* sfb;      // scale atoms of the x/y rows (B)
   int gA, gB, nks;         // SfGeom: groups per channel, k-steps per row
-  // K segments (hi + lo split: hi.hi, hi.lo, lo.hi, lo.lo): segment s pairs
+  // K segments (hi + lo split: hi.hi, hi.lo, lo.hi; up to 4): segment s pairs
   // A k-blocks seg_a[s] + kk with B k-blocks seg_b[s] + kk; nseg = 1: plain
   int nseg;
   int seg_a[4], seg_b[4];
