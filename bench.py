@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--no-extra", action="store_true", help="skip the extra workload legs")
     p.add_argument("--leg", default=None,
                    choices=["nvfp4", "nvfp4split", "raw", "imaging", "xengine", "splitk",
-                            "precision", "imaging_visbf"],
+                            "precision", "imaging_visbf", "batched"],
                    help="run one extra workload alone and print its JSON (profiling cases); "
                         "nvfp4 and nvfp4split use --inputs/--channels/--k")
     p.add_argument("--strategy", default=None,
@@ -504,12 +504,26 @@ def run_batched_leg(torch, dev, seed=3, n_chans=96, inputs=4096):
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / reps
+        # each fixed strategy (untuned calls, graph replay): 0 direct, 1 bulk
+        # stores, 2 CTA pair, 3 CTA pair with bulk stores
+        by_mode = {}
+        for mode in (0, 1, 2, 3):
+            c.set_strategy(mode, 0)
+            for _ in range(3):
+                c.herk_batched_v(chans)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(reps):
+                c.herk_batched_v(chans)
+            e1.record()
+            torch.cuda.synchronize()
+            by_mode[str(mode)] = round(e0.elapsed_time(e1) / reps, 4)
         if c.device_status() != 0:
             raise RuntimeError("device wait timed out in the batched leg")
     return {"workload": f"{n_chans} channels, K in [128, 2048] step 64, {inputs} inputs with "
                         f"1536..{inputs} active after flagging, one call (tuned, graph replay)",
             "value": flops / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms,
-            "tflop_per_step": flops / 1e12}
+            "tflop_per_step": flops / 1e12, "ms_by_store_mode": by_mode}
 
 
 def run_ftd_leg(torch, dev, n_ant=2048, n_chan=64, n_pol=2, K=1024, seed=6):
@@ -827,6 +841,8 @@ def run_leg(args):
         out = run_precision_leg(torch, dev)
     elif args.leg == "imaging_visbf":
         out = run_imaging_visbf_leg(torch, dev)
+    elif args.leg == "batched":
+        out = run_batched_leg(torch, dev)
     else:
         out = run_xengine_leg(torch, dev)
     print(json.dumps(out), flush=True)

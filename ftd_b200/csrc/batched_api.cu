@@ -6,7 +6,9 @@
 // over channel groups (lib/visibility_pipeline.cu:268-277).  Here the
 // promotion pass gathers each channel's active rows into the FP8 planes and
 // the persistent correlator walks one tile list over all channels, longest
-// integration first so that the short channels fill the last wave.
+// integration first so that the short channels fill the last wave.  Store
+// modes 2 and 3 run the CTA-pair kernel on the same channel table, with its
+// own tile list (256 column x 128 row inputs) and the -Re plane.
 #include <algorithm>
 #include <cstring>
 #include <numeric>
@@ -20,8 +22,10 @@ namespace {
 struct VPlan {
   GatherDesc* d_gather = nullptr;
   TileDesc* d_tiles = nullptr;
+  TileDesc* d_tiles_pair = nullptr;
   ChanDesc* d_chans = nullptr;
   int num_tiles = 0;
+  int num_tiles_pair = 0;
   int num_chans = 0;
   int max_n = 0;
   int64_t rows = 0;
@@ -29,6 +33,7 @@ struct VPlan {
   ~VPlan() {
     if (d_gather) cudaFree(d_gather);
     if (d_tiles) cudaFree(d_tiles);
+    if (d_tiles_pair) cudaFree(d_tiles_pair);
     if (d_chans) cudaFree(d_chans);
   }
 };
@@ -51,7 +56,8 @@ uint64_t fingerprint(const ftdx_channel_desc* d, int n, int output) {
 }
 
 // Builds (or finds) the plan: gather table, channel table and the tile list,
-// channels ordered by descending K, each channel's tiles in triangle order.
+// channels ordered by descending K, each channel's tiles in triangle order;
+// the same for the pair kernel's tiles (tj over 256 column inputs).
 ftdx_status get_vplan(ftdx_handle h, const ftdx_channel_desc* d, int n, int output, uint64_t fp,
                       cudaStream_t s, const VPlan** out) {
   auto it = h->vplans.find(fp);
@@ -87,14 +93,18 @@ ftdx_status get_vplan(ftdx_handle h, const ftdx_channel_desc* d, int n, int outp
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(),
                    [&](int a, int b) { return ch[a].kblocks > ch[b].kblocks; });
-  std::vector<TileDesc> tiles;
+  std::vector<TileDesc> tiles, tiles_pair;
   for (int c : order) {
     const int nb = (ch[c].n + kTile - 1) / kTile;
-    for (int ti = 0; ti < nb; ++ti)
+    for (int ti = 0; ti < nb; ++ti) {
       for (int tj = 0; tj <= ti; ++tj) tiles.push_back(TileDesc{c, uint16_t(ti), uint16_t(tj)});
+      for (int tj = 0; tj <= ti / 2; ++tj)
+        tiles_pair.push_back(TileDesc{c, uint16_t(ti), uint16_t(tj)});
+    }
   }
   if (tiles.size() > size_t(1) << 30) return fail(h, FTDX_ERR_INVALID_ARG, "too many tiles");
   p->num_tiles = int(tiles.size());
+  p->num_tiles_pair = int(tiles_pair.size());
   p->num_chans = n;
   p->rows = rows;
   p->kp = kp;
@@ -102,11 +112,16 @@ ftdx_status get_vplan(ftdx_handle h, const ftdx_channel_desc* d, int n, int outp
   if (e == cudaSuccess) e = cudaMalloc(&p->d_chans, ch.size() * sizeof(ChanDesc));
   if (e == cudaSuccess) e = cudaMalloc(&p->d_tiles, tiles.size() * sizeof(TileDesc));
   if (e == cudaSuccess)
+    e = cudaMalloc(&p->d_tiles_pair, tiles_pair.size() * sizeof(TileDesc));
+  if (e == cudaSuccess)
     e = cudaMemcpy(p->d_gather, g.data(), g.size() * sizeof(GatherDesc), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(p->d_chans, ch.data(), ch.size() * sizeof(ChanDesc), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(p->d_tiles, tiles.data(), tiles.size() * sizeof(TileDesc),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(p->d_tiles_pair, tiles_pair.data(), tiles_pair.size() * sizeof(TileDesc),
                    cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(h, e, "batched plan upload");
   if (h->vplans.size() >= 8) h->vplans.erase(h->vplans.begin());
@@ -123,40 +138,58 @@ struct VCall {
   uint64_t fp;
 };
 
-ftdx_status prepare_v(ftdx_handle h, const VCall& c, cudaStream_t s, const VPlan** plan) {
+// The CTA-pair kernel (store modes 2 and 3) when a pair fits on the device.
+bool pair_strategy(ftdx_handle h, const Strategy& strat) {
+  return (strat.store_mode & 3) >= 2 && pair_grid_limit(h) >= 2;
+}
+
+// Plan and workspace (two planes, three for the pair kernel's -Re operand).
+ftdx_status prepare_v(ftdx_handle h, const VCall& c, cudaStream_t s, const VPlan** plan,
+                      bool pair) {
   ftdx_status st = get_vplan(h, c.d, c.n, int(c.output), c.fp, s, plan);
   if (st != FTDX_OK) return st;
-  return ensure_workspace(h, size_t(2) * size_t((*plan)->rows) * size_t((*plan)->kp), s);
+  return ensure_workspace(
+      h, size_t(pair ? 3 : 2) * size_t((*plan)->rows) * size_t((*plan)->kp), s);
 }
 
 ftdx_status launch_v(ftdx_handle h, const VCall& c, const Strategy& strat, cudaStream_t s) {
+  const bool pair = pair_strategy(h, strat);
   const VPlan* p = nullptr;
-  ftdx_status st = prepare_v(h, c, s, &p);
+  ftdx_status st = prepare_v(h, c, s, &p, pair);
   if (st != FTDX_OK) return st;
   cudaError_t e;
   {
     ScopedTimer tm(h, s, 1);
-    e = launch_gather_qc_to_planes(p->d_gather, p->num_chans, p->max_n, h->z, p->rows, p->kp, s);
+    e = launch_gather_qc_to_planes(p->d_gather, p->num_chans, p->max_n, h->z, p->rows, p->kp, s,
+                                   pair ? 1 : 0);
   }
   if (e != cudaSuccess) return cuda_fail(h, e, "gathered promotion launch");
   CUtensorMap tmZ;
-  st = encode_planes_map(h, h->z, p->rows, p->kp, &tmZ);
+  st = encode_planes_map(h, h->z, p->rows, p->kp, &tmZ, kTile, pair ? 3 : 2);
   if (st != FTDX_OK) return st;
   HerkArgs args = herk_args_default();
-  args.tiles = p->d_tiles;
+  args.tiles = pair ? p->d_tiles_pair : p->d_tiles;
   args.chans = p->d_chans;
-  args.num_tiles = p->num_tiles;
+  args.num_tiles = pair ? p->num_tiles_pair : p->num_tiles;
   args.out_fp16 = (c.output == FTDX_OUT_FP16) ? 1 : 0;
-  args.bulk_store = strat.store_mode == 1 ? 1 : 0;
+  args.bulk_store = (strat.store_mode & 1) ? 1 : 0;  // modes 1 and 3
   args.out_format = 0;
   args.out = nullptr;
   args.alpha = c.alpha;
   args.beta = c.beta;
   args.status = h->d_status;
-  int grid = strat.grid > 0 ? std::min(strat.grid, h->sm_count) : h->sm_count;
-  if (strat.grid < 0) grid = p->num_tiles;
-  grid = std::min(grid, p->num_tiles);
-  {
+  if (pair) {
+    // persistent pairs, at most as many as can be resident together
+    const int limit = pair_grid_limit(h);
+    int grid = strat.grid > 0 ? std::min(strat.grid, limit) : limit;
+    if (strat.grid < 0) grid = 2 * p->num_tiles_pair;
+    grid = std::min(grid, 2 * p->num_tiles_pair) & ~1;
+    ScopedTimer tm(h, s, 0);
+    e = launch_herk_fp8_pair(tmZ, args, grid, s);
+  } else {
+    int grid = strat.grid > 0 ? std::min(strat.grid, h->sm_count) : h->sm_count;
+    if (strat.grid < 0) grid = p->num_tiles;
+    grid = std::min(grid, p->num_tiles);
     ScopedTimer tm(h, s, 0);
     e = launch_herk_fp8(tmZ, args, grid, s);
   }
@@ -207,9 +240,12 @@ extern "C" ftdx_status ftdx_herk_batched_v(ftdx_handle h, const ftdx_channel_des
       strat = it->second.st;
     } else if (beta == 0.f && !capturing) {
       TuneEntry best;
+      std::vector<Strategy> cands = default_candidates(h, output == FTDX_OUT_FP32, true);
+      if (output == FTDX_OUT_FP32 && pair_grid_limit(h) >= 2)
+        cands.push_back(Strategy{3, pair_grid_limit(h)});  // pair with bulk-copy stores
       ftdx_status st = tune_sweep(
           h, [&](const Strategy& cand, cudaStream_t ss) { return launch_v(h, call, cand, ss); },
-          default_candidates(h, output == FTDX_OUT_FP32, false), s, &best);
+          cands, s, &best);
       if (st != FTDX_OK) return st;
       record_tuned(h, key, best);
       strat = best.st;
@@ -223,7 +259,8 @@ extern "C" ftdx_status ftdx_herk_batched_v(ftdx_handle h, const ftdx_channel_des
         h, gk,
         [&](cudaStream_t ss) {
           const VPlan* p = nullptr;
-          return ss == h->capture_stream ? launch_v(h, call, strat, ss) : prepare_v(h, call, ss, &p);
+          return ss == h->capture_stream ? launch_v(h, call, strat, ss)
+                                         : prepare_v(h, call, ss, &p, pair_strategy(h, strat));
         },
         s);
   }

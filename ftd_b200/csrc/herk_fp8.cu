@@ -233,11 +233,12 @@ __global__ void __launch_bounds__(256) fp16_to_planes_kernel(const __half2* __re
 
 // Batched promotion with row gathering (flagged inputs) and per-channel K.
 // Block (x, y): channel y, rows [x * rows_per_block, ...).  One thread
-// converts 16 samples of one row.
+// converts 16 samples of one row.  neg_plane: plane 2 receives -Re too.
 __global__ void __launch_bounds__(256) gather_qc_to_planes_kernel(const GatherDesc* __restrict__ gd,
                                                                   uint8_t* __restrict__ z,
                                                                   int64_t total_rows, int Kp,
-                                                                  int rows_per_block) {
+                                                                  int rows_per_block,
+                                                                  int neg_plane) {
   const GatherDesc g = gd[blockIdx.y];
   const int r0 = blockIdx.x * rows_per_block;
   if (r0 >= g.n) return;
@@ -275,6 +276,11 @@ __global__ void __launch_bounds__(256) gather_qc_to_planes_kernel(const GatherDe
     uint8_t* dst = z + (g.row0 + r) * int64_t(Kp) + t0;
     *reinterpret_cast<uint4*>(dst) = make_uint4(re[0], re[1], re[2], re[3]);
     *reinterpret_cast<uint4*>(dst + plane) = make_uint4(im[0], im[1], im[2], im[3]);
+    if (neg_plane) {
+      constexpr uint32_t kS = 0x80808080u;
+      *reinterpret_cast<uint4*>(dst + 2 * plane) =
+          make_uint4(re[0] ^ kS, re[1] ^ kS, re[2] ^ kS, re[3] ^ kS);
+    }
   }
 }
 
@@ -1127,10 +1133,10 @@ cudaError_t launch_fp16_to_planes(const void* a16, uint8_t* z, int64_t rows, int
 }
 
 cudaError_t launch_gather_qc_to_planes(const GatherDesc* g, int nch, int max_n, uint8_t* z,
-                                       int64_t total_rows, int Kp, cudaStream_t s) {
+                                       int64_t total_rows, int Kp, cudaStream_t s, int neg_plane) {
   const int rpb = rows_per_block(Kp >> 4);
   const dim3 grid(unsigned((max_n + rpb - 1) / rpb), unsigned(nch));
-  gather_qc_to_planes_kernel<<<grid, 256, 0, s>>>(g, z, total_rows, Kp, rpb);
+  gather_qc_to_planes_kernel<<<grid, 256, 0, s>>>(g, z, total_rows, Kp, rpb, neg_plane);
   return cudaGetLastError();
 }
 

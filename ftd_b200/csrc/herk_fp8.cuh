@@ -158,9 +158,11 @@ cudaError_t launch_fp16_to_planes(const void* a16, uint8_t* z, int64_t rows, int
                                   cudaStream_t s);
 // Gathered promotion for `nch` channels with a common plane pitch Kp
 // (>= every channel's K rounded up to 128); each channel's rows are
-// zero-padded from its K up to its own K rounded up to 128.
+// zero-padded from its K up to its own K rounded up to 128.  neg_plane: also
+// write plane 2 = -Re (CTA-pair kernel operand).
 cudaError_t launch_gather_qc_to_planes(const GatherDesc* g, int nch, int max_n, uint8_t* z,
-                                       int64_t total_rows, int Kp, cudaStream_t s);
+                                       int64_t total_rows, int Kp, cudaStream_t s,
+                                       int neg_plane = 0);
 cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s);
 // Split-K reduction: C[c] = alpha * cs_c * sum_s ws[c*splits + s] + beta * C[c].
 cudaError_t launch_split_reduce(const float2* ws, void* out, int out_fp16, int64_t P, int batch,

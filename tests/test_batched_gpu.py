@@ -87,6 +87,31 @@ def test_uneven_flagged_medium_tuned_and_graph():
         assert c.device_status() == 0
 
 
+@pytest.mark.parametrize("mode", [1, 2, 3])
+def test_uneven_flagged_store_modes(mode):
+    """Bulk stores and the CTA-pair kernel (with and without bulk stores) on
+    the gathered channels: bit-exact, including channels narrower than one
+    256-input pair tile and ones ending mid-tile."""
+    rng = np.random.default_rng(80 + mode)
+    specs = [(1, None, 1, 0), (200, 130, 64, 16), (300, 257, 200, 3), (64, None, 1000, 0),
+             (700, 600, 2048, 0), (129, 129, 65, 7), (500, 17, 130, 0), (1100, 1023, 384, 0)]
+    chans, host = make_channels(rng, specs)
+    with Correlator() as c:
+        c.set_strategy(mode, 0)
+        c.herk_batched_v(chans, output=OUT_FP32)
+        assert c.device_status() == 0
+        check(chans, host)
+        # a second call on the same plan after a single-CTA call
+        c.set_strategy(0, 0)
+        c.herk_batched_v(chans, output=OUT_FP32)
+        c.set_strategy(mode, 0)
+        for ch in chans:
+            ch["C"].fill_(float("nan"))
+        c.herk_batched_v(chans, output=OUT_FP32)
+        assert c.device_status() == 0
+    check(chans, host)
+
+
 def test_batched_fp16_out_and_beta():
     rng = np.random.default_rng(72)
     specs = [(150, 140, 96, 0), (90, None, 160, 0)]
@@ -159,3 +184,22 @@ def test_workload3_full_size_properties():
             ref = oracle.herk_qc_rows(qc, n, ch["K"], 0, i0, n).astype(np.float32)
             got = ch["C"][tri_size(i0):tri_size(n)].cpu().numpy()
             assert np.array_equal(got, ref), k
+
+
+def test_workload3_pair_modes_match_single():
+    """The full-size uneven workload through the CTA-pair kernel (store modes
+    2 and 3) equals the single-CTA result bit for bit."""
+    chans = make_workload3(2028, n_chans=24)
+    with Correlator() as c:
+        c.set_strategy(0, 0)
+        c.herk_batched_v(chans)
+        ref = [ch["C"].clone() for ch in chans]
+        for mode in (2, 3):
+            for ch in chans:
+                ch["C"].fill_(float("nan"))
+            c.set_strategy(mode, 0)
+            c.herk_batched_v(chans)
+            assert c.device_status() == 0
+            torch.cuda.synchronize()
+            for k, ch in enumerate(chans):
+                assert torch.equal(ch["C"], ref[k]), (mode, k)
