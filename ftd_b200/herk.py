@@ -104,7 +104,9 @@ class Correlator:
     def herk_batched_v(self, channels, output: int = OUT_FP32, alpha: float = 1.0,
                        beta: float = 0.0, stream=None, tune: bool = False) -> None:
         """Uneven / flagged channels in one launch.  `channels` is a list of dicts
-        with keys A, C, n_inputs, K and optionally lda, active (device buffers)."""
+        with keys A, C, n_inputs, K and optionally lda, active (device buffers).
+        Untuned calls follow set_strategy (store modes 0-3; 2 and 3 run the
+        CTA-pair kernel); tune=True times modes 0-3 once per descriptor set."""
         arr = (_lib.ChannelDesc * len(channels))()
         for k, ch in enumerate(channels):
             arr[k].A = _ptr(ch["A"])

@@ -115,7 +115,8 @@ FTDX_API ftdx_status ftdx_herk(ftdx_handle h, const void* A, void* C, int N, int
  * in the order of `active`) is
  *   C_c = alpha * A_c A_c^H + beta * C_c,  A_c = rows active[0..n_inputs) of
  *   the [rows][lda] QC block at A (rows 0..n_inputs-1 when active == NULL).
- * All channels run in one persistent correlator launch (longest K first).
+ * All channels run in one persistent correlator launch (longest K first),
+ * on the single-CTA or the CTA-pair kernel (ftdx_set_strategy / tune).
  * A plan is built on the first call with a given descriptor set (pointers
  * and sizes; the contents of `active` are read on every call) and cached. */
 typedef struct ftdx_channel_desc {
@@ -315,18 +316,20 @@ FTDX_API int ftdx_graph_count(ftdx_handle h);
 /* Strategy for calls that are not tuned (tune = 0, or no cache entry):
  * store_mode 0 = direct stores, 1 = shared-memory staging + bulk copies,
  * 2 = CTA-pair kernel (one tcgen05 cta_group::2 MMA over two SMs per
- * 256 x 128 tile; uniform ftdx_herk calls only, others use 0);
+ * 256 x 128 tile; uniform ftdx_herk calls and ftdx_herk_batched_v, others
+ * use 0);
  * 3 = CTA-pair kernel with bulk-copy stores for interior tiles (FP32 output,
  * alpha = 1, beta = 0; other tiles and calls as 2);
  * + 4 = operands as packed FP6 E3M2 planes (INT4 input; exact);
  * 2 + 8, 3 + 8 = CTA-pair kernel on signed 8-bit operands (kind::i8, S32
- * accumulation; INT4 input; exact).  For NVFP4 compute, store_mode 2 selects
+ * accumulation; uniform INT4 input; exact; ftdx_herk_batched_v runs these
+ * as 2 and 3 on E4M3 operands).  For NVFP4 compute, store_mode 2 selects
  * the NVFP4 CTA-pair kernel and 0 / 1 the single-CTA one.
  * grid > 0 = that many persistent CTAs (capped at one per SM; even and capped
  * at the co-resident pairs for store_mode 2), 0 = one per SM, -1 = one CTA
  * (pair) per tile (a plain, non-persistent launch).  The tuner also times
- * store_mode 2, 3, 2 + 8 and 3 + 8 for uniform INT4 calls, and both NVFP4
- * kernels. */
+ * store_mode 2, 3, 2 + 8 and 3 + 8 for uniform INT4 calls, 2 and 3 for
+ * ftdx_herk_batched_v, and both NVFP4 kernels. */
 FTDX_API ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid);
 
 /* Split-K for untuned calls: K is cut into `splits` (1..32) ranges of
