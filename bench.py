@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--no-extra", action="store_true", help="skip the extra workload legs")
     p.add_argument("--leg", default=None,
                    choices=["nvfp4", "nvfp4split", "raw", "imaging", "xengine", "splitk",
-                            "precision", "imaging_visbf", "batched"],
+                            "precision", "imaging_visbf", "batched", "xengine"],
                    help="run one extra workload alone and print its JSON (profiling cases); "
                         "nvfp4 and nvfp4split use --inputs/--channels/--k")
     p.add_argument("--strategy", default=None,
@@ -617,13 +617,28 @@ def run_xengine_leg(torch, dev, n_ant=2048, K=1024, batch=128, seed=9):
     p = torch.randint(0, 256, (batch * K * n_ant,), device=dev, dtype=torch.uint8, generator=g)
     C = torch.empty(batch, tri_size(n_ant), 2, device=dev)
     with Correlator(device=dev.index) as c:
-        ms = _timed(torch, lambda: c.xengine(p, C, n_ant, K, batch, mat_format=1), reps=10)
+        by_mode = {}
+        for mode in (2, 0):  # CTA pair, single-CTA kernel
+            c.set_strategy(mode, 0)
+            ms = _timed(torch, lambda: c.xengine(p, C, n_ant, K, batch, mat_format=1), reps=10)
+            # per-kernel CUDA-event times of 5 more calls: corner turn + promotion, correlator
+            c.set_profiling(True)
+            for _ in range(5):
+                c.xengine(p, C, n_ant, K, batch, mat_format=1)
+            torch.cuda.synchronize()
+            prof = c.profile_read()
+            c.set_profiling(False)
+            by_mode[str(mode)] = {
+                "ms_per_step": ms,
+                "corner_turn_promotion_ms": prof["prep_ms"] / max(prof["prep_launches"], 1),
+                "correlator_ms": prof["herk_ms"] / max(prof["herk_launches"], 1)}
         if c.device_status() != 0:
             raise RuntimeError("device status after the XEngine leg")
+    ms = by_mode["0"]["ms_per_step"]  # the default strategy: single-CTA kernel
     return {"workload": f"XEngine: {batch} blocks of [K={K}][{n_ant}] two's-complement (4,4)b "
-                        f"-> packed upper triangles (FP32)",
+                        f"-> packed upper triangles (FP32), single-CTA kernel",
             "value": herk_flops(n_ant, K, batch) / (ms * 1e-3) / 1e12, "unit": UNIT,
-            "ms_per_step": ms}
+            "ms_per_step": ms, "by_store_mode": by_mode}
 
 
 def run_splitk_leg(torch, dev, N=256, K=65536, B=4, seed=10):

@@ -129,9 +129,11 @@ ftdx_status cuda_fail(ftdx_handle h, cudaError_t e, const char* what);
 bool stream_capturing(cudaStream_t s);
 ftdx_status ensure_workspace(ftdx_handle h, size_t bytes, cudaStream_t s);
 ftdx_status ensure_aux(ftdx_handle h, size_t bytes, cudaStream_t s);
-// pair: tiles of the CTA-pair kernel (tj over 256 inputs, ti over 128)
+// pair: tiles of the CTA-pair kernel (tj over 256 inputs, ti over 128);
+// upper (pair only): the packed-upper XEngine format's tiles, tj over 256
+// column inputs c and ti over 128 row inputs r <= c
 ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
-                     const Plan** out, bool pair = false, int splits = 1);
+                     const Plan** out, bool pair = false, int splits = 1, bool upper = false);
 ftdx_status ensure_split_ws(ftdx_handle h, size_t bytes, cudaStream_t s);
 // fp6: planes of packed E3M2 codes (the kernels' fp6 operand form)
 ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t Kp,

@@ -21,7 +21,7 @@
 namespace ftdx {
 namespace {
 
-constexpr int kTK = 64;          // time samples per tile
+constexpr int kTK = 128;         // time samples per tile
 constexpr int kTS = 128;         // source bytes (ant, chan, pol) per tile
 constexpr int kTPitch = kTK + 4; // transposed tile row pitch (bytes)
 
@@ -34,16 +34,18 @@ __device__ __forceinline__ void put32(uint8_t* dst, const uint32_t (&w)[8], int 
 #pragma unroll
     for (int x = 0; x < 8; ++x) reinterpret_cast<uint32_t*>(dst)[x] = w[x];
   } else {
-    for (int b = 0; b < nbytes; ++b) dst[b] = uint8_t(w[b >> 2] >> (8 * (b & 3)));
+#pragma unroll
+    for (int b = 0; b < 32; ++b)  // unrolled: w stays in registers
+      if (b < nbytes) dst[b] = uint8_t(w[b >> 2] >> (8 * (b & 3)));
   }
 }
 
 // [t][ant][chan][pol] source.  Block (x, y, z): source bytes [128 x, +128) of
-// a time slice (S = n_ant*n_chan*n_pol bytes each), samples k in [64 y, +64),
-// time_inner z.  The 64 x 128 byte tile is read with coalesced 4-byte loads
+// a time slice (S = n_ant*n_chan*n_pol bytes each), samples k in [128 y, +128),
+// time_inner z.  The 128 x 128 byte tile is read with coalesced 4-byte loads
 // along the slice, transposed 4 x 4 in registers into shared memory as
 // [source byte][k], then every (source byte, 32 samples) run is converted and
-// written as 32 contiguous bytes per plane.
+// written as 32 contiguous bytes per plane (four threads: one 128-byte line).
 __global__ void __launch_bounds__(256) ftd_tacp_to_planes_kernel(const uint8_t* __restrict__ raw,
                                                                  uint8_t* __restrict__ z,
                                                                  FtdGeom g) {
@@ -54,9 +56,9 @@ __global__ void __launch_bounds__(256) ftd_tacp_to_planes_kernel(const uint8_t* 
   const int ti = blockIdx.z;
   const int t = threadIdx.x;
   const bool wide = (S & 3) == 0 && (reinterpret_cast<uintptr_t>(raw) & 3) == 0;
-  // phase 1: 16 k-groups x 32 s-groups of 4 x 4 bytes, two per thread
+  // phase 1: kTK / 4 k-groups x 32 s-groups of 4 x 4 bytes, kTK / 32 per thread
 #pragma unroll
-  for (int rep = 0; rep < 2; ++rep) {
+  for (int rep = 0; rep < kTK / 32; ++rep) {
     const int blk = t + 256 * rep;
     const int sg = blk & 31, kg = blk >> 5;  // lanes of a warp: consecutive source words
     uint32_t w[4];
@@ -89,48 +91,51 @@ __global__ void __launch_bounds__(256) ftd_tacp_to_planes_kernel(const uint8_t* 
     *reinterpret_cast<uint32_t*>(d + 3 * kTPitch) = o3;
   }
   __syncthreads();
-  // phase 2: thread -> (source byte sl, 32 samples)
-  const int sl = t >> 1, h = t & 1;
-  const int64_t s = s0 + sl;
-  if (s >= S) return;
-  const int pol = int(s % g.n_pol);
-  const int64_t ac = s / g.n_pol;
-  const int chan = int(ac % g.n_chan);
-  const int ant = int(ac / g.n_chan);
-  int64_t row;
-  int col0, kend;
-  if (g.pol_sum) {
-    row = (int64_t(chan) * g.n_ti + ti) * g.n_ant + ant;
-    col0 = pol * g.K;
-    kend = (pol == g.n_pol - 1) ? g.Kp - (g.n_pol - 1) * g.K : g.K;  // last pol owns the padding
-  } else {
-    row = ((int64_t(chan) * g.n_pol + pol) * g.n_ti + ti) * g.n_ant + ant;
-    col0 = 0;
-    kend = g.Kp;
-  }
-  const int kb = k0 + 32 * h;
-  if (kb >= kend) return;
-  const int nbytes = kend - kb < 32 ? kend - kb : 32;
-  uint32_t q[8];
-  const uint8_t* src = tileT + sl * kTPitch + 32 * h;
+  // phase 2: task -> (source byte sl, samples [32 h, +32)), kTK / 64 per thread
+#pragma unroll 1
+  for (int task = t; task < kTS * (kTK / 32); task += 256) {
+    const int sl = task / (kTK / 32), h = task % (kTK / 32);
+    const int64_t s = s0 + sl;
+    if (s >= S) break;
+    const int pol = int(s % g.n_pol);
+    const int64_t ac = s / g.n_pol;
+    const int chan = int(ac % g.n_chan);
+    const int ant = int(ac / g.n_chan);
+    int64_t row;
+    int col0, kend;
+    if (g.pol_sum) {
+      row = (int64_t(chan) * g.n_ti + ti) * g.n_ant + ant;
+      col0 = pol * g.K;
+      kend = (pol == g.n_pol - 1) ? g.Kp - (g.n_pol - 1) * g.K : g.K;  // last pol owns the padding
+    } else {
+      row = ((int64_t(chan) * g.n_pol + pol) * g.n_ti + ti) * g.n_ant + ant;
+      col0 = 0;
+      kend = g.Kp;
+    }
+    const int kb = k0 + 32 * h;
+    if (kb >= kend) continue;
+    const int nbytes = kend - kb < 32 ? kend - kb : 32;
+    uint32_t q[8];
+    const uint8_t* src = tileT + sl * kTPitch + 32 * h;
 #pragma unroll
-  for (int x = 0; x < 8; ++x) q[x] = *reinterpret_cast<const uint32_t*>(src + 4 * x);
-  uint32_t re[8], im[8];
-  if (g.twos) {
+    for (int x = 0; x < 8; ++x) q[x] = *reinterpret_cast<const uint32_t*>(src + 4 * x);
+    uint32_t re[8], im[8];
+    if (g.twos) {
 #pragma unroll
-    for (int x = 0; x < 8; ++x) tc4_to_e4m3(q[x], re[x], im[x]);
-  } else {
+      for (int x = 0; x < 8; ++x) tc4_to_e4m3(q[x], re[x], im[x]);
+    } else {
 #pragma unroll
-    for (int x = 0; x < 8; ++x) qc4_to_e4m3(q[x], re[x], im[x]);
-  }
-  const int64_t plane = g.rows * int64_t(g.Kp);
-  uint8_t* dst = z + row * g.Kp + col0 + kb;
-  put32(dst, re, nbytes);
-  put32(dst + plane, im, nbytes);
-  if (g.neg_plane) {
+      for (int x = 0; x < 8; ++x) qc4_to_e4m3(q[x], re[x], im[x]);
+    }
+    const int64_t plane = g.rows * int64_t(g.Kp);
+    uint8_t* dst = z + row * g.Kp + col0 + kb;
+    put32(dst, re, nbytes);
+    put32(dst + plane, im, nbytes);
+    if (g.neg_plane) {
 #pragma unroll
-    for (int x = 0; x < 8; ++x) re[x] ^= 0x80808080u;
-    put32(dst + 2 * plane, re, nbytes);
+      for (int x = 0; x < 8; ++x) re[x] ^= 0x80808080u;
+      put32(dst + 2 * plane, re, nbytes);
+    }
   }
 }
 

@@ -131,10 +131,13 @@ ftdx_status ensure_aux(ftdx_handle h, size_t bytes, cudaStream_t s) {
 // Lower-triangle tile list for `batch` channels of N inputs, channel-major so
 // that concurrently running CTAs share a channel's operand in L2.
 ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t s,
-                     const Plan** out, bool pair, int splits) {
-  // kblocks < 2^23 (K <= 2^30) and splits <= 32, so pair and split-K plans
-  // never share a key with others
-  auto key = std::make_tuple(N, kblocks + (pair ? (1 << 24) : 0) + ((splits - 1) << 25), batch);
+                     const Plan** out, bool pair, int splits, bool upper) {
+  upper = upper && pair;
+  // kblocks < 2^23 (K <= 2^30) and splits <= 32, so pair, split-K and
+  // upper-format pair plans never share a key with others
+  auto key = std::make_tuple(N, kblocks + (pair ? (1 << 24) : 0) + ((splits - 1) << 25) +
+                                    (upper ? (1 << 30) : 0),
+                             batch);
   auto it = h->plans.find(key);
   if (it != h->plans.end()) {
     *out = it->second.get();
@@ -161,6 +164,14 @@ ftdx_status get_plan(ftdx_handle h, int N, int kblocks, int batch, cudaStream_t 
       chans[vc].row0 = int64_t(c) * N;
       chans[vc].out0 = int64_t(vc) * (int64_t(N) * (N + 1) / 2);
       chans[vc].out_ptr = 0;
+      if (upper) {
+        // packed-upper pair tiles: tj over 256 column inputs c (the TMEM
+        // lanes), ti over 128 row inputs r <= c (the TMEM columns)
+        for (int tj = 0; tj < (N + 255) / 256; ++tj)
+          for (int ti = 0; ti < nb && ti <= 2 * tj + 1; ++ti)
+            tiles.push_back(TileDesc{vc, uint16_t(ti), uint16_t(tj)});
+        continue;
+      }
       for (int ti = 0; ti < nb; ++ti)
         for (int tj = 0; tj <= (pair ? ti / 2 : ti); ++tj)
           tiles.push_back(TileDesc{vc, uint16_t(ti), uint16_t(tj)});

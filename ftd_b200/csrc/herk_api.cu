@@ -173,7 +173,7 @@ ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan
                                 size_t(int64_t(c.N) * (c.N + 1) / 2) * sizeof(float2), s);
     if (st != FTDX_OK) return st;
   }
-  return get_plan(h, c.N, int(Kp / kStageK), c.batch, s, plan, pair, splits);
+  return get_plan(h, c.N, int(Kp / kStageK), c.batch, s, plan, pair, splits, c.out_format == 1);
 }
 
 // Promotion kernel + correlator kernel on stream s.
@@ -746,9 +746,10 @@ ftdx_status ftdx_xengine(ftdx_handle h, const void* payload, void* out, int n_an
     return fail(h, FTDX_ERR_INVALID_ARG, "xengine: K too large");
   cudaError_t e = cudaSetDevice(h->device);
   if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
-  // the XEngine formats are written by the single-CTA kernel's direct stores
+  // the XEngine formats are written with direct stores, by the single-CTA
+  // kernel or (store modes 2 and 3) the CTA pair
   Strategy strat = h->default_strategy;
-  strat.store_mode = 0;
+  strat.store_mode = (strat.store_mode & 3) >= 2 ? 2 : 0;
   return launch_all(h, c, strat, static_cast<cudaStream_t>(stream));
 }
 

@@ -234,7 +234,7 @@ struct Fp4Args {
   const uint8_t* sfa;      // scale atoms of the x rows (A)
   const uint8_t* sfb;      // scale atoms of the x/y rows (B)
   int gA, gB, nks;         // SfGeom: groups per channel, k-steps per row
-  // K segments (hi + lo split: hi.hi, hi.lo, lo.hi; up to 4): segment s pairs
+  // K segments (hi + lo split: hi.hi, hi.lo, lo.hi; at most 3): segment s pairs
   // A k-blocks seg_a[s] + kk with B k-blocks seg_b[s] + kk; nseg = 1: plain
   int nseg;
   int seg_a[4], seg_b[4];
@@ -348,7 +348,11 @@ __global__ void __launch_bounds__(k4Threads, 1)
             break;
           }
           const int seg = kb / cd.kblocks, kk = kb - seg * cd.kblocks;
-          const int ka = args.seg_a[seg] + kk, kbb = args.seg_b[seg] + kk;
+          // selects, not an indexed load: a dynamic index into the kernel
+          // parameters would copy them to local memory
+          const int sa = seg == 0 ? args.seg_a[0] : (seg == 1 ? args.seg_a[1] : args.seg_a[2]);
+          const int sb = seg == 0 ? args.seg_b[0] : (seg == 1 ? args.seg_b[1] : args.seg_b[2]);
+          const int ka = sa + kk, kbb = sb + kk;
           mbar_arrive_expect_tx(full_bar(stage), k4StageBytes);
           tma_load_2d(a_addr(stage), &tmA, ka * k4KB, rowA, full_bar(stage));
           tma_load_2d(b_addr(stage), &tmB, kbb * k4KB, rowB, full_bar(stage));
@@ -583,7 +587,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(k4pThreads, 1)
             break;
           }
           const int seg = kb / cd.kblocks, kk = kb - seg * cd.kblocks;
-          const int ka = args.seg_a[seg] + kk, kbb = args.seg_b[seg] + kk;
+          // selects, not an indexed load: a dynamic index into the kernel
+          // parameters would copy them to local memory
+          const int sa = seg == 0 ? args.seg_a[0] : (seg == 1 ? args.seg_a[1] : args.seg_a[2]);
+          const int sb = seg == 0 ? args.seg_b[0] : (seg == 1 ? args.seg_b[1] : args.seg_b[2]);
+          const int ka = sa + kk, kbb = sb + kk;
           if (leader) mbar_arrive_expect_tx(full_bar(stage), 2 * k4pStageBytes);
           const uint32_t fb = map_shared(full_bar(stage), 0);
           tma_load_2d_pair(a_addr(stage), &tmA, ka * k4KB, rowA, fb);

@@ -313,7 +313,7 @@ template <typename Out2>
 __device__ __forceinline__ void store_chunk_xengine(Out2* ob, int i0, int j, int n, float sc,
                                                     int format, const uint32_t (&re)[32],
                                                     const uint32_t (&im)[32]) {
-#pragma unroll 4
+#pragma unroll
   for (int m = 0; m < 32; ++m) {
     const int i = i0 + m;
     if (i < n && j <= i) {
@@ -703,7 +703,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
             }
             continue;
           }
-#pragma unroll 4
+#pragma unroll
           for (int m = 0; m < 32; ++m) {
             const int r = r0 + m;
             if (c < n && r <= c) {
@@ -973,8 +973,55 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
       const int jt0 = jw - q * 32;  // first of this CTA's 128 columns
       bool bulk_tile = false;
       if constexpr (sizeof(Out2) == 8) {
-        bulk_tile = args.bulk_store && args.alpha == 1.f && args.beta == 0.f && !args.kahan &&
-                    args.chan_scale == nullptr && jt0 + 127 < ib && ib + kTile <= n;
+        bulk_tile = args.bulk_store && args.out_format == 0 && args.alpha == 1.f &&
+                    args.beta == 0.f && !args.kahan && args.chan_scale == nullptr &&
+                    jt0 + 127 < ib && ib + kTile <= n;
+      }
+      if (args.out_format == 1) {
+        // Packed upper triangle, row-major (the XEngine's format): the plan's
+        // tiles put column inputs c on the TMEM lanes (tj over 256) and row
+        // inputs r on the TMEM columns (ti over 128), so the accumulator
+        // holds sum_t v_r conj(v_c) = conj(C(r, c)).  A warp stores 32
+        // consecutive c of one row r.
+        const int c = j;
+#pragma unroll 1
+        for (int cc = 0; cc < kChunks; ++cc) {
+          const int k = half * kChunks + cc;
+          const int r0 = ib + 32 * k;
+          if (r0 > jw + 31 || jw >= n) continue;  // warp-uniform: nothing to store
+          uint32_t re[32], im[32];
+          __syncwarp();
+          tmem_ld_32x32b_x32(tb + 32u * k, re);
+          tmem_ld_32x32b_x32(tb + uint32_t(kTile) + 32u * k, im);
+          tmem_wait_ld();
+          if (args.s8) {  // exact S32 sums -> FP32
+#pragma unroll
+            for (int m = 0; m < 32; ++m) {
+              re[m] = __float_as_uint(float(int32_t(re[m])));
+              im[m] = __float_as_uint(float(int32_t(im[m])));
+            }
+          }
+          if (r0 + 31 < jw && jw + 31 < n) {
+            // every element strictly above the diagonal and inside n: row
+            // r + 1 starts n - r - 1 elements after element (r, c)'s row start
+            Out2* p = outc + (int64_t(r0) * n - int64_t(r0) * (r0 - 1) / 2 + (c - r0));
+#pragma unroll
+            for (int m = 0; m < 32; ++m) {
+              put(p, __uint_as_float(re[m]) * sc, -__uint_as_float(im[m]) * sc);
+              p += n - (r0 + m) - 1;
+            }
+            continue;
+          }
+#pragma unroll
+          for (int m = 0; m < 32; ++m) {
+            const int r = r0 + m;
+            if (c < n && r <= c) {
+              const float vr = __uint_as_float(re[m]) * sc;
+              const float vi = (r == c) ? 0.f : -__uint_as_float(im[m]) * sc;
+              put(outc + (int64_t(r) * n - int64_t(r) * (r - 1) / 2 + (c - r)), vr, vi);
+            }
+          }
+        }
       }
       if (bulk_tile) {
         // Interior tile, as the single-CTA kernel's bulk mode: 8 rows at a
@@ -1027,7 +1074,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
         }
       }
 #pragma unroll 1
-      for (int cc = 0; cc < kChunks && !bulk_tile; ++cc) {
+      for (int cc = 0; cc < kChunks && !bulk_tile && args.out_format != 1; ++cc) {
         const int c = half * kChunks + cc;
         const int i0 = ib + 32 * c;
         if (i0 + 31 < jw || i0 >= n) continue;  // warp-uniform: nothing to store
@@ -1042,6 +1089,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
             re[m] = __float_as_uint(float(int32_t(re[m])));
             im[m] = __float_as_uint(float(int32_t(im[m])));
           }
+        }
+        if (args.out_format == 2) {  // the XEngine's full Hermitian matrix
+          store_chunk_xengine(out + int64_t(td.ch) * n * n, i0, j, n, sc, 2, re, im);
+          continue;
         }
         const int64_t e0 = int64_t(i0) * (i0 + 1) / 2 + j;
         if constexpr (sizeof(Out2) == 8) {

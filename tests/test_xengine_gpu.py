@@ -14,12 +14,14 @@ pytestmark = pytest.mark.gpu
 DEV = "cuda:0"
 
 
-def run(n, K, B, fmt, out=OUT_FP32, seed=0):
+def run(n, K, B, fmt, out=OUT_FP32, seed=0, mode=0):
+    """mode: the strategy (0 single-CTA kernel, 2 CTA pair)."""
     p = np.random.default_rng(seed).integers(0, 256, size=B * K * n, dtype=np.uint8)
     size = n * n if fmt == 0 else n * (n + 1) // 2
     dt = torch.float32 if out == OUT_FP32 else torch.float16
     C = torch.full((B, size, 2), float("nan"), dtype=dt, device=DEV)
     with Correlator() as c:
+        c.set_strategy(mode, 0)
         c.xengine(torch.from_numpy(p).to(DEV), C, n, K, B, mat_format=fmt, output=out)
         assert c.device_status() == 0
     torch.cuda.synchronize()
@@ -28,17 +30,20 @@ def run(n, K, B, fmt, out=OUT_FP32, seed=0):
     return got[..., 0] + 1j * got[..., 1], ref
 
 
+@pytest.mark.parametrize("mode", [0, 2])
 @pytest.mark.parametrize("fmt", [0, 1])
-# 640: interior tiles, which the packed-upper FP32 format writes with bulk copies
+# 640 and 1000: interior tiles (the unmasked store paths); 257, 1000: a last
+# 256-input block of the pair kernel that is partly or mostly empty
 @pytest.mark.parametrize("n,K,B", [(64, 128, 3), (130, 100, 2), (257, 64, 1), (5, 3, 4),
-                                   (640, 96, 2)])
-def test_formats_exact(fmt, n, K, B):
-    got, ref = run(n, K, B, fmt, seed=n + K + fmt)
+                                   (640, 96, 2), (1000, 160, 1)])
+def test_formats_exact(mode, fmt, n, K, B):
+    got, ref = run(n, K, B, fmt, seed=n + K + fmt, mode=mode)
     assert np.array_equal(got, ref)
 
 
-def test_fp16_output():
-    got, ref = run(96, 64, 2, 1, out=OUT_FP16, seed=9)
+@pytest.mark.parametrize("mode", [0, 2])
+def test_fp16_output(mode):
+    got, ref = run(96, 64, 2, 1, out=OUT_FP16, seed=9, mode=mode)
     assert np.array_equal(got, ref.real.astype(np.float16) + 1j * ref.imag.astype(np.float16))
 
 
