@@ -316,8 +316,8 @@ FTDX_API int ftdx_graph_count(ftdx_handle h);
 /* Strategy for calls that are not tuned (tune = 0, or no cache entry):
  * store_mode 0 = direct stores, 1 = shared-memory staging + bulk copies,
  * 2 = CTA-pair kernel (one tcgen05 cta_group::2 MMA over two SMs per
- * 256 x 128 tile; uniform ftdx_herk calls and ftdx_herk_batched_v, others
- * use 0);
+ * 256 x 128 tile; uniform ftdx_herk calls, ftdx_herk_batched_v and
+ * ftdx_xengine (which takes 3 as 2 and 1 as 0: direct stores), others use 0);
  * 3 = CTA-pair kernel with bulk-copy stores for interior tiles (FP32 output,
  * alpha = 1, beta = 0; other tiles and calls as 2);
  * + 4 = operands as packed FP6 E3M2 planes (INT4 input; exact);
