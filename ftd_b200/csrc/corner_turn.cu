@@ -97,10 +97,13 @@ __global__ void __launch_bounds__(256) ftd_tacp_to_planes_kernel(const uint8_t* 
     const int sl = task / (kTK / 32), h = task % (kTK / 32);
     const int64_t s = s0 + sl;
     if (s >= S) break;
-    const int pol = int(s % g.n_pol);
-    const int64_t ac = s / g.n_pol;
-    const int chan = int(ac % g.n_chan);
-    const int ant = int(ac / g.n_chan);
+    // 32-bit divisions (S < 2^31, checked at launch): the 64-bit ones are
+    // emulated in dozens of instructions each
+    const uint32_t s32 = uint32_t(s);
+    const int pol = int(s32 % uint32_t(g.n_pol));
+    const uint32_t ac = s32 / uint32_t(g.n_pol);
+    const int chan = int(ac % uint32_t(g.n_chan));
+    const int ant = int(ac / uint32_t(g.n_chan));
     int64_t row;
     int col0, kend;
     if (g.pol_sum) {
@@ -202,7 +205,7 @@ cudaError_t launch_ftd_to_planes(const uint8_t* raw, uint8_t* z, const FtdGeom& 
     const int kmax = g.pol_sum ? g.Kp - (g.n_pol - 1) * g.K : g.Kp;
     const dim3 grid(unsigned((S + kTS - 1) / kTS), unsigned((kmax + kTK - 1) / kTK),
                     unsigned(g.n_ti));
-    if (grid.y > 65535u || grid.z > 65535u || grid.x > 0x7fffffffu)
+    if (grid.y > 65535u || grid.z > 65535u || S >= (int64_t(1) << 31))
       return cudaErrorInvalidConfiguration;
     ftd_tacp_to_planes_kernel<<<grid, 256, 0, s>>>(raw, z, g);
   } else {
