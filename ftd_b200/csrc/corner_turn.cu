@@ -46,7 +46,9 @@ __device__ __forceinline__ void put32(uint8_t* dst, const uint32_t (&w)[8], int 
 // along the slice, transposed 4 x 4 in registers into shared memory as
 // [source byte][k], then every (source byte, 32 samples) run is converted and
 // written as 32 contiguous bytes per plane (four threads: one 128-byte line).
-__global__ void __launch_bounds__(256) ftd_tacp_to_planes_kernel(const uint8_t* __restrict__ raw,
+// Eight blocks per SM (32 registers, a few bytes spilled) beat six (40
+// registers, no spill): the kernel is latency- and issue-bound.
+__global__ void __launch_bounds__(256, 8) ftd_tacp_to_planes_kernel(const uint8_t* __restrict__ raw,
                                                                  uint8_t* __restrict__ z,
                                                                  FtdGeom g) {
   __shared__ __align__(16) uint8_t tileT[kTS * kTPitch];
