@@ -112,15 +112,18 @@ def test_uneven_flagged_store_modes(mode):
     check(chans, host)
 
 
-def test_batched_fp16_out_and_beta():
+@pytest.mark.parametrize("mode", [0, 2])
+def test_batched_fp16_out_and_beta(mode):
+    """alpha / beta and FP16 output on the single-CTA kernel and the CTA pair."""
     rng = np.random.default_rng(72)
-    specs = [(150, 140, 96, 0), (90, None, 160, 0)]
+    specs = [(150, 140, 96, 0), (90, None, 160, 0), (600, 530, 256, 0)]
     chans, host = make_channels(rng, specs)
     olds = []
     for ch in chans:
         ch["C"] = torch.randn(tri_size(ch["n_inputs"]), 2, device=DEV)
         olds.append(ch["C"].clone())
     with Correlator() as c:
+        c.set_strategy(mode, 0)
         c.herk_batched_v(chans, output=OUT_FP32, alpha=2.0, beta=0.5)
     torch.cuda.synchronize()
     for ch, hb, old in zip(chans, host, olds):
@@ -130,6 +133,7 @@ def test_batched_fp16_out_and_beta():
     for ch in chans16:
         ch["C"] = torch.empty(tri_size(ch["n_inputs"]), 2, dtype=torch.float16, device=DEV)
     with Correlator() as c:
+        c.set_strategy(mode, 0)
         c.herk_batched_v(chans16, output=OUT_FP16)
     torch.cuda.synchronize()
     for ch, hb in zip(chans16, host16):
