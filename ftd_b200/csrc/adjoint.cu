@@ -353,13 +353,8 @@ cudaError_t launch_adjoint(const void* G, const uint8_t* V, void* dV, int n, int
   a.num_tiles = batch * a.tiles_t * a.tiles_a;
   a.out = static_cast<float2*>(dV);
   a.status = status;
-  static bool attr = false;
-  if (!attr) {
-    e = cudaFuncSetAttribute(adjoint_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(kASmem));
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  e = ensure_smem_limit(reinterpret_cast<const void*>(adjoint_tc_kernel), kASmem);
+  if (e != cudaSuccess) return e;
   const int grid = a.num_tiles < sm_count ? a.num_tiles : sm_count;
   adjoint_tc_kernel<<<grid, kAThreads, kASmem, s>>>(tmV, tmS, a);
   return cudaGetLastError();

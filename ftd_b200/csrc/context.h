@@ -143,6 +143,8 @@ ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t K
 int pair_grid_limit(ftdx_handle h);
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 void* tensor_map_encoder();  // cuTensorMapEncodeTiled through the runtime
+// Text set by set_thread_error on the calling thread (empty: none).
+const std::string& thread_error();
 
 // Event pair around one kernel launch when profiling is on (never during capture).
 struct ScopedTimer {

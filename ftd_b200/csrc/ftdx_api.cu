@@ -9,6 +9,9 @@
 #include <cstring>
 
 #include <algorithm>
+#include <mutex>
+#include <set>
+#include <utility>
 
 #include "context.h"
 
@@ -21,17 +24,44 @@ Plan::~Plan() {
 
 static PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
+  static std::once_flag once;
+  std::call_once(once, [] {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
             cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
       fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }
+  });
   return fn;
+}
+
+static std::string& thread_error_text() {
+  thread_local std::string t;  // last failure of a handle-less call on this thread
+  return t;
+}
+const std::string& thread_error() { return thread_error_text(); }
+
+void set_thread_error(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  thread_error_text() = buf;
+}
+
+cudaError_t ensure_smem_limit(const void* kernel, size_t bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({dev, kernel})) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+  if (e == cudaSuccess) done.insert({dev, kernel});
+  return e;
 }
 
 void* tensor_map_encoder() { return reinterpret_cast<void*>(get_encode_fn()); }
@@ -338,7 +368,11 @@ ftdx_status ftdx_destroy(ftdx_handle h) {
   return FTDX_OK;
 }
 
-const char* ftdx_last_error(ftdx_handle h) { return h ? h->last_error.c_str() : "null handle"; }
+const char* ftdx_last_error(ftdx_handle h) {
+  if (h) return h->last_error.c_str();
+  const std::string& t = ftdx::thread_error();
+  return t.empty() ? "null handle" : t.c_str();
+}
 
 ftdx_status ftdx_device_status(ftdx_handle h, void* stream, uint32_t* bits) {
   if (!h) return FTDX_ERR_INVALID_ARG;

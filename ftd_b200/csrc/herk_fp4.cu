@@ -25,6 +25,9 @@
 #include <cudaTypedefs.h>
 #include <cuda_fp8.h>
 
+#include <map>
+#include <mutex>
+
 #include "herk_fp8.cuh"
 #include "sm100.cuh"
 
@@ -757,22 +760,28 @@ size_t nvfp4_workspace_bytes(int n, int batch, int K, int split, int pair) {
   return size_t(fp4_ws(n, batch, K, split, pair).total);
 }
 
-// Pairs of the NVFP4 pair kernel that can be resident at once (0: none).
+// Pairs of the NVFP4 pair kernel that can be resident at once on the current
+// device (0: none), queried once per device.
 int nvfp4_pair_limit() {
-  static int limit = -1;
-  if (limit < 0) {
-    limit = 0;
-    if (cudaFuncSetAttribute(herk_fp4_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(k4pSmem)) == cudaSuccess) {
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(2, 1, 1);
-      cfg.blockDim = dim3(k4pThreads, 1, 1);
-      cfg.dynamicSmemBytes = k4pSmem;
-      int n = 0;
-      if (cudaOccupancyMaxActiveClusters(&n, herk_fp4_pair_kernel, &cfg) == cudaSuccess) limit = n;
-    }
-    cudaGetLastError();
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  static std::mutex mu;
+  static std::map<int, int> limits;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = limits.find(dev);
+  if (it != limits.end()) return it->second;
+  int limit = 0;
+  if (ensure_smem_limit(reinterpret_cast<const void*>(herk_fp4_pair_kernel), k4pSmem) ==
+      cudaSuccess) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2, 1, 1);
+    cfg.blockDim = dim3(k4pThreads, 1, 1);
+    cfg.dynamicSmemBytes = k4pSmem;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, herk_fp4_pair_kernel, &cfg) == cudaSuccess) limit = n;
   }
+  cudaGetLastError();
+  limits[dev] = limit;
   return limit;
 }
 
@@ -858,13 +867,8 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
     herk_fp4_pair_kernel<<<2 * pairs, k4pThreads, k4pSmem, s>>>(tmA, tmB, tmSa, tmSb, args);
     return cudaGetLastError();
   }
-  static bool attr = false;
-  if (!attr) {
-    e = cudaFuncSetAttribute(herk_fp4_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(k4Smem));
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  e = ensure_smem_limit(reinterpret_cast<const void*>(herk_fp4_tc_kernel), k4Smem);
+  if (e != cudaSuccess) return e;
   const int grid = num_tiles < sm_count ? num_tiles : sm_count;
   herk_fp4_tc_kernel<<<grid, k4Threads, k4Smem, s>>>(tmA, tmB, args);
   return cudaGetLastError();

@@ -1194,26 +1194,16 @@ cudaError_t launch_gather_qc_to_planes(const GatherDesc* g, int nch, int max_n, 
 template <typename OutT>
 static cudaError_t launch_herk_t(const CUtensorMap& tmZ, const HerkArgs& a, int grid,
                                  cudaStream_t s) {
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaError_t e = cudaFuncSetAttribute(herk_fp8_tc_kernel<OutT>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(kHerkSmem));
-    if (e != cudaSuccess) return e;
-    attr_done = true;
-  }
+  cudaError_t e =
+      ensure_smem_limit(reinterpret_cast<const void*>(herk_fp8_tc_kernel<OutT>), kHerkSmem);
+  if (e != cudaSuccess) return e;
   herk_fp8_tc_kernel<OutT><<<grid, kHerkThreads, kHerkSmem, s>>>(tmZ, a);
   return cudaGetLastError();
 }
 
 template <typename OutT>
 static cudaError_t pair_attributes() {
-  static bool done = false;
-  if (done) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(herk_fp8_pair_kernel<OutT>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPairSmem));
-  if (e == cudaSuccess) done = true;
-  return e;
+  return ensure_smem_limit(reinterpret_cast<const void*>(herk_fp8_pair_kernel<OutT>), kPairSmem);
 }
 
 template <typename OutT>

@@ -125,6 +125,14 @@ inline HerkArgs herk_args_default() {
   return a;
 }
 
+// Raises `kernel`'s dynamic shared-memory limit to `bytes` on the current
+// device, once per (device, kernel): CUDA keeps this attribute per device, so
+// a process driving several GPUs sets it on each.  Thread-safe (ftdx_api.cu).
+cudaError_t ensure_smem_limit(const void* kernel, size_t bytes);
+// Records the text of a failure of an entry point that takes no handle, for
+// the calling thread; ftdx_last_error(NULL) returns it (ftdx_api.cu).
+void set_thread_error(const char* fmt, ...);
+
 // Host-side launchers (herk_fp8.cu).
 // neg_plane: also write plane 2 = -Re (CTA-pair kernel operand)
 cudaError_t launch_qc_to_planes(const uint8_t* qc, uint8_t* z, int64_t rows, int K, int Kp,

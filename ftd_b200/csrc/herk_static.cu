@@ -14,7 +14,6 @@
 // voltages and the output triangles.
 #include <algorithm>
 #include <cmath>
-#include <cstdio>
 #include <mutex>
 
 #include <cudaTypedefs.h>
@@ -93,36 +92,65 @@ using namespace ftdx;
 
 extern "C" ftdx_status ftdx_herk_static(const void* A, void* C, int N, int K, int batch,
                                         void* stream, uint32_t* status_out, size_t* scratch_used) {
-  if (!A || !C || N < 1 || K < 1 || batch < 1) return FTDX_ERR_INVALID_ARG;
-  if ((reinterpret_cast<uintptr_t>(C) & 7) != 0) return FTDX_ERR_INVALID_ARG;
-  if (N > 65535 * kTile || int64_t(K) > (int64_t(1) << 30)) return FTDX_ERR_INVALID_ARG;
-  // Scratch layout: status | channel table + tile list | FP8 planes (1 KiB aligned).
+  if (!A || !C || N < 1 || K < 1 || batch < 1) {
+    set_thread_error("ftdx_herk_static: null pointer or size < 1");
+    return FTDX_ERR_INVALID_ARG;
+  }
+  if ((reinterpret_cast<uintptr_t>(C) & 7) != 0) {
+    set_thread_error("ftdx_herk_static: C is not 8-byte aligned");
+    return FTDX_ERR_INVALID_ARG;
+  }
+  if (N > 65535 * kTile || int64_t(K) > (int64_t(1) << 30)) {
+    set_thread_error("ftdx_herk_static: N=%d or K=%d out of range", N, K);
+    return FTDX_ERR_INVALID_ARG;
+  }
+  // Scratch layout: status | channel table + tile list | FP8 planes (1 KiB
+  // aligned).  All sizes in 64 bits: the tile count of a large N overflows int.
   const int64_t Kp = (int64_t(K) + kStageK - 1) / kStageK * kStageK;
   const int64_t rows = int64_t(N) * batch;
-  const int nb = (N + kTile - 1) / kTile;
-  const int per_chan = nb * (nb + 1) / 2;
+  const int64_t nb = (int64_t(N) + kTile - 1) / kTile;
+  const int64_t per_chan = nb * (nb + 1) / 2;
   const int64_t ntiles = int64_t(batch) * per_chan;
-  const size_t plan_bytes = size_t(batch) * sizeof(ChanDesc) + size_t(ntiles) * sizeof(TileDesc);
-  const size_t z_off = (kPlanOffset + plan_bytes + 1023) / 1024 * 1024;
-  const size_t need = z_off + size_t(2) * size_t(rows) * size_t(Kp);
-  if (scratch_used) *scratch_used = need;
-  if (need > kStaticBytes || ntiles > (int64_t(1) << 30)) {
-    fprintf(stderr,
-            "ftdx_herk_static: N=%d K=%d batch=%d needs %zu bytes of scratch; the static "
-            "scratch holds %zu (FTDX_STATIC_SCRATCH_BYTES)\n",
-            N, K, batch, need, kStaticBytes);
+  const uint64_t plan_bytes =
+      uint64_t(batch) * sizeof(ChanDesc) + uint64_t(ntiles) * sizeof(TileDesc);
+  const uint64_t z_off = (kPlanOffset + plan_bytes + 1023) / 1024 * 1024;
+  const uint64_t need = z_off + uint64_t(2) * uint64_t(rows) * uint64_t(Kp);
+  if (scratch_used) *scratch_used = size_t(need);
+  if (need > kStaticBytes) {
+    set_thread_error(
+        "ftdx_herk_static: N=%d K=%d batch=%d needs %llu bytes of scratch; the static scratch "
+        "holds %zu (FTDX_STATIC_SCRATCH_BYTES)",
+        N, K, batch, static_cast<unsigned long long>(need), kStaticBytes);
     return FTDX_ERR_CAPACITY;
   }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (status_out) {
+    // reading the status synchronises the stream, which a capture forbids
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+      set_thread_error("ftdx_herk_static: status_out must be NULL while the stream is captured");
+      return FTDX_ERR_INVALID_ARG;
+    }
+  }
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return FTDX_ERR_NO_DEVICE;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    set_thread_error("ftdx_herk_static: no current CUDA device");
+    return FTDX_ERR_NO_DEVICE;
+  }
   int major = 0, sms = 0;
   cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (major != 10) return FTDX_ERR_NO_DEVICE;
+  if (major != 10) {
+    set_thread_error("ftdx_herk_static: device %d is not an sm_100 GPU", dev);
+    return FTDX_ERR_NO_DEVICE;
+  }
   uint8_t* base = nullptr;
-  if (scratch_for_device(dev, &base) != cudaSuccess) return FTDX_ERR_CUDA;
+  const cudaError_t se = scratch_for_device(dev, &base);
+  if (se != cudaSuccess) {
+    set_thread_error("ftdx_herk_static: cudaGetSymbolAddress: %s", cudaGetErrorString(se));
+    return FTDX_ERR_CUDA;
+  }
 
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   uint32_t* status = reinterpret_cast<uint32_t*>(base + kStatusOffset);
   ChanDesc* chans = reinterpret_cast<ChanDesc*>(base + kPlanOffset);
   TileDesc* tiles = reinterpret_cast<TileDesc*>(base + kPlanOffset + size_t(batch) * sizeof(ChanDesc));
@@ -130,13 +158,20 @@ extern "C" ftdx_status ftdx_herk_static(const void* A, void* C, int N, int K, in
 
   const int pblocks = int(std::min<int64_t>((ntiles + 255) / 256, int64_t(sms) * 4));
   static_plan_kernel<<<pblocks, 256, 0, s>>>(chans, tiles, status, N, int(Kp / kStageK), batch,
-                                             per_chan);
-  if (cudaGetLastError() != cudaSuccess) return FTDX_ERR_CUDA;
-  if (launch_qc_to_planes(static_cast<const uint8_t*>(A), z, rows, K, int(Kp), s) != cudaSuccess)
+                                             int(per_chan));
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = launch_qc_to_planes(static_cast<const uint8_t*>(A), z, rows, K, int(Kp), s);
+  if (e != cudaSuccess) {
+    set_thread_error("ftdx_herk_static: launch failed: %s", cudaGetErrorString(e));
     return FTDX_ERR_CUDA;
+  }
 
   auto enc = encode_fn();
-  if (!enc) return FTDX_ERR_CUDA;
+  if (!enc) {
+    set_thread_error("ftdx_herk_static: cuTensorMapEncodeTiled unavailable");
+    return FTDX_ERR_CUDA;
+  }
   CUtensorMap tm;
   const cuuint32_t estr[3] = {1, 1, 1};
   const cuuint64_t dims[3] = {cuuint64_t(Kp), cuuint64_t(rows), 2};
@@ -144,8 +179,10 @@ extern "C" ftdx_status ftdx_herk_static(const void* A, void* C, int N, int K, in
   const cuuint32_t box[3] = {cuuint32_t(kStageK), cuuint32_t(kTile), 1};
   if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, z, dims, strides, box, estr,
           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+    set_thread_error("ftdx_herk_static: tensor map encode failed");
     return FTDX_ERR_CUDA;
+  }
 
   HerkArgs args = herk_args_default();
   args.tiles = tiles;
@@ -159,15 +196,26 @@ extern "C" ftdx_status ftdx_herk_static(const void* A, void* C, int N, int K, in
   args.beta = 0.f;
   args.status = status;
   const int grid = int(std::min<int64_t>(ntiles, sms));
-  if (launch_herk_fp8(tm, args, grid, s) != cudaSuccess) return FTDX_ERR_CUDA;
+  e = launch_herk_fp8(tm, args, grid, s);
+  if (e != cudaSuccess) {
+    set_thread_error("ftdx_herk_static: correlator launch failed: %s", cudaGetErrorString(e));
+    return FTDX_ERR_CUDA;
+  }
 
   if (status_out) {
+    // an ordered copy on the caller's stream, so no other stream is waited on
     uint32_t v = 0;
-    if (cudaStreamSynchronize(s) != cudaSuccess ||
-        cudaMemcpy(&v, status, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess)
+    e = cudaMemcpyAsync(&v, status, sizeof(v), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      set_thread_error("ftdx_herk_static: status read failed: %s", cudaGetErrorString(e));
       return FTDX_ERR_CUDA;
+    }
     *status_out = v;
-    if (v) return FTDX_ERR_TIMEOUT;
+    if (v) {
+      set_thread_error("ftdx_herk_static: device status bits 0x%x (a bounded wait ran out)", v);
+      return FTDX_ERR_TIMEOUT;
+    }
   }
   return FTDX_OK;
 }

@@ -91,7 +91,9 @@ FTDX_API const char* ftdx_status_string(ftdx_status s);
 FTDX_API ftdx_status ftdx_create(ftdx_handle* h, const ftdx_config* cfg);
 FTDX_API ftdx_status ftdx_destroy(ftdx_handle h);
 
-/* Text of the last error raised on this handle (static until the next call). */
+/* Text of the last error raised on this handle (static until the next call).
+ * With h = NULL: the text of the last failure of a handle-less entry point
+ * (ftdx_herk_static) on the calling thread, or "null handle" if none. */
 FTDX_API const char* ftdx_last_error(ftdx_handle h);
 
 /* Batched HERK.  Replaces CutlassComplexGemm::herk (cutlass_gemm_api.h:750-760,
@@ -355,17 +357,21 @@ FTDX_API int ftdx_tuned_split_k(ftdx_handle h, int N, int K, int batch, ftdx_inp
  * (QC int4 in, complex64 packed lower triangles out), but no handle and no
  * workspace: all scratch lives in one static device array of
  * FTDX_STATIC_SCRATCH_BYTES that every GPU loading this library holds until
- * the process exits.  Needed: 1 KiB + 2*N*batch*Kp bytes (Kp = K rounded up
- * to 128) + 8 bytes per lower-triangle tile of 128 x 128 inputs; larger
- * problems return FTDX_ERR_CAPACITY (and print the sizes to stderr), e.g.
- * N = 1024 inputs, K = 1024 samples fits 15 channels per call.  The first
- * call on a device looks up the array's device address (a one-time set-up);
- * make that first call before any stream capture.  All calls share the one
- * array: calls that overlap on the GPU (other streams, other threads) race
- * and corrupt each other's results; serialise them.  If status_out is not
- * NULL the call synchronises `stream` and stores the device status bits
- * there (FTDX_ERR_TIMEOUT if any is set).  scratch_used (may be NULL)
- * receives the bytes this problem needs. */
+ * the process exits.  Bytes needed, exactly:
+ *   round_up(256 + 40*batch + 8*tiles, 1024) + 2*N*batch*Kp
+ * with Kp = K rounded up to 128 and tiles = batch*nb*(nb+1)/2, nb = ceil(N/128)
+ * (a 40-byte table entry per channel, 8 bytes per lower-triangle tile of
+ * 128 x 128 inputs); scratch_used (may be NULL) receives it, also on refusal.
+ * Larger problems return FTDX_ERR_CAPACITY before any GPU work, with the
+ * sizes in ftdx_last_error(NULL); e.g. N = 1024 inputs, K = 1024 samples fits
+ * 15 channels per call.  The first call on a device looks up the array's
+ * device address (a one-time set-up); make that first call before any stream
+ * capture.  All calls share the one array: calls that overlap on the GPU
+ * (other streams, other threads) race and corrupt each other's results;
+ * serialise them.  If status_out is not NULL the call synchronises `stream`
+ * (an ordered copy on that stream, no device-wide wait) and stores the
+ * device status bits there (FTDX_ERR_TIMEOUT if any is set); status_out must
+ * be NULL while `stream` is being captured (FTDX_ERR_INVALID_ARG otherwise). */
 #define FTDX_STATIC_SCRATCH_BYTES (32u << 20)
 FTDX_API ftdx_status ftdx_herk_static(const void* A, void* C, int N, int K, int batch,
                                       void* stream, uint32_t* status_out, size_t* scratch_used);

@@ -1,11 +1,12 @@
 #!/usr/bin/env bash
 # Builds oracle/_ref/libref_herk.so from the reference's own host correlator
-# code.  Reads the reference tree (default /root/reference, or $FTD_REFERENCE)
-# and writes only into oracle/_ref/ (git-ignored).  The extracted text is
-# never committed; ref_harness.cpp (ours) includes it.
+# code.  Reads the reference tree ($FTD_REFERENCE, else a checkout named
+# "reference" beside this repository) and writes only into oracle/_ref/
+# (git-ignored).  The extracted text is never committed; ref_harness.cpp
+# (ours) includes it.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${FTD_REFERENCE:-/root/reference}"
+REF="${FTD_REFERENCE:-$(cd "$HERE/../.." && pwd)/reference}"
 OUT="$HERE/_ref"
 T1="$REF/cutlass_interface/test_herk_int4.cu"
 T2="$REF/tests/visibility_pipeline_test.cpp"

@@ -33,7 +33,14 @@ def test_static_rejects_oversize_without_gpu_work():
                             ctypes.byref(used))
     assert st == 6  # FTDX_ERR_CAPACITY
     assert used.value == _sizes(N, K, B) > STATIC_BYTES
+    # the sizes are reported through the calling thread's error text, not stderr
+    msg = L.ftdx_last_error(None).decode()
+    assert f"needs {used.value} bytes" in msg and str(STATIC_BYTES) in msg
     assert L.ftdx_herk_static(None, None, 1, 1, 1, None, None, None) == 1
+    # a tile count that overflows 32-bit arithmetic is refused as too large
+    st = L.ftdx_herk_static(ctypes.c_void_p(16), ctypes.c_void_p(16), 6_000_000, 1, 1, None,
+                            None, ctypes.byref(used))
+    assert st == 6 and used.value == _sizes(6_000_000, 1, 1)
 
 
 @pytest.mark.gpu
