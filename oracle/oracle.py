@@ -89,8 +89,65 @@ def ref_lib():
             L.ref_cpu_herk_ftd.argtypes = [_u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p]
         L.ref_num_threads.restype = ctypes.c_int
+        if hasattr(L, "ref_data_promote"):
+            L.ref_data_promote.argtypes = [_u8p, ctypes.c_int64, _f64p]
+            L.ref_promote_to_float.argtypes = [_u8p, ctypes.c_int64, _f64p]
+            L.ref_herm_to_tri.argtypes = [_f64p, ctypes.c_int, ctypes.c_int, _f64p]
+            L.ref_tri_decode.argtypes = [ctypes.c_int64, _i32p, _i32p]
+            L.ref_uv_cell.argtypes = [_f32p, _f32p, ctypes.c_int64, ctypes.c_double,
+                                      ctypes.c_float, ctypes.c_float, _f32p, _f32p, _i32p, _i32p]
         _ref = L
     return _ref
+
+
+def ref_kernels():
+    """The reference's XEngine / imaging helpers compiled for the host (None
+    when oracle/_ref was built without them)."""
+    L = ref_lib()
+    return L if L is not None and hasattr(L, "ref_data_promote") else None
+
+
+def ref_data_promote(b: np.ndarray, host_test: bool = False):
+    """(re, im) float64 of QC bytes through the reference's DataPromote functor
+    (or, host_test, the XEngine test's promote_to_float)."""
+    b = np.ascontiguousarray(b, dtype=np.uint8).reshape(-1)
+    out = np.empty(2 * b.size, dtype=np.float64)
+    f = ref_kernels().ref_promote_to_float if host_test else ref_kernels().ref_data_promote
+    f(_p(b, _u8p), b.size, _p(out, _f64p))
+    return out[0::2], out[1::2]
+
+
+def ref_herm_to_tri(full: np.ndarray) -> np.ndarray:
+    """Packed upper triangles [batch, n(n+1)/2] (complex128) of full
+    [batch, n, n] matrices through the reference's HermToTri functor."""
+    full = np.ascontiguousarray(full, dtype=np.complex128)
+    b, n = full.shape[0], full.shape[1]
+    out = np.zeros((b, n * (n + 1) // 2), dtype=np.complex128)
+    ref_kernels().ref_herm_to_tri(_p(full.view(np.float64), _f64p), n, b,
+                                  _p(out.view(np.float64), _f64p))
+    return out
+
+
+def ref_tri_decode(count: int):
+    """(row, col) of packed lower indices 0..count-1 by the reference's tri_decode."""
+    r = np.empty(count, dtype=np.int32)
+    c = np.empty(count, dtype=np.int32)
+    ref_kernels().ref_tri_decode(count, _p(r, _i32p), _p(c, _i32p))
+    return r, c
+
+
+def ref_uv_cell(uv_m: np.ndarray, freq_hz: float, cell: float, ng: int):
+    """(iu, iv, u_lam, v_lam) of baselines uv_m [n, 2] (metres) by the
+    reference's uv_cell."""
+    u = np.ascontiguousarray(uv_m[:, 0], dtype=np.float32)
+    v = np.ascontiguousarray(uv_m[:, 1], dtype=np.float32)
+    n = u.size
+    ul, vl = np.empty(n, np.float32), np.empty(n, np.float32)
+    iu, iv = np.empty(n, np.int32), np.empty(n, np.int32)
+    ref_kernels().ref_uv_cell(_p(u, _f32p), _p(v, _f32p), n, float(freq_hz), float(cell),
+                              float(0.5 * ng), _p(ul, _f32p), _p(vl, _f32p), _p(iu, _i32p),
+                              _p(iv, _i32p))
+    return iu, iv, ul, vl
 
 
 # ----------------------------------------------------------------- codecs

@@ -123,8 +123,8 @@ def test_fp16_input(corr):
 @pytest.mark.parametrize("strategy", [None, 1, 2, 3, 10, 11])
 def test_dsa2000_scale_spot_rows(strategy):
     # 4096 inputs x 64 channels x K = 1024 (the DSA-2000 configuration): full
-    # output on the GPU, exact check of row blocks in three channels and of the
-    # whole diagonal (sum |v|^2) of every channel.
+    # output on the GPU, exact check of two whole channels, of row blocks in
+    # three more and of the whole diagonal (sum |v|^2) of every channel.
     N, K, B = 4096, 1024, 64
     g = torch.Generator(device=DEV).manual_seed(3)
     re = torch.clamp(torch.round(torch.randn(B, N, K, device=DEV, generator=g) * 2.5), -7, 7)
@@ -151,6 +151,10 @@ def test_dsa2000_scale_spot_rows(strategy):
         ref = oracle.herk_qc_rows(qc_h, N, K, b, i0, i1).astype(np.float32)
         got = C[b, tri_size(i0):tri_size(i1)].cpu().numpy()
         assert np.array_equal(got, ref), (b, i0, i1)
+    # two whole channels, all 8,390,656 elements of each, against the int64 oracle
+    for b in (5, 40):
+        ref = oracle.herk_qc(np.ascontiguousarray(qc_h[b:b + 1]), N, K, 1)[0].astype(np.float32)
+        assert np.array_equal(C[b].cpu().numpy(), ref), b
 
 
 def test_ggp_entry_point(corr):

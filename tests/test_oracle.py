@@ -264,3 +264,82 @@ def test_e4m3_restatement_rounding_rules():
                  np.float32)
     want = np.array([1.0, 1.25, 448.0, 448.0, 448.0, 0.0, 2.0 ** -8, -1.0, 0.0], np.float32)
     assert np.array_equal(oracle.e4m3_rne(x), want)
+
+
+# ------------------------------------------------ pinned to the reference's own helpers
+# DataPromote, HermToTri, tri_decode and uv_cell are device code of the
+# reference; oracle/build_ref.sh extracts them and ref_harness.cpp compiles
+# them for the host, so the restatements below are checked against the
+# reference's own arithmetic, not against a reading of it.
+needs_ref_kernels = pytest.mark.skipif(oracle.ref_kernels() is None,
+                                       reason="reference helpers not built here")
+
+
+@needs_ref_kernels
+def test_decode_twos_pinned_to_data_promote_all_bytes():
+    b = np.arange(256, dtype=np.uint8)
+    re, im = oracle.decode_twos(b)
+    for host_test in (False, True):  # the kernel functor and the test's host decode
+        rr, ri = oracle.ref_data_promote(b, host_test=host_test)
+        assert np.array_equal(re.astype(np.float64), rr)
+        assert np.array_equal(im.astype(np.float64), ri)
+
+
+@needs_ref_kernels
+def test_xengine_oracle_pinned_to_promote_and_herm_to_tri():
+    # the reference XEngine chain: promoteData (DataPromote) -> C = M^H M per
+    # block -> triangulateFromHerm (HermToTri, packed upper, row-major)
+    rng = np.random.default_rng(31)
+    for (n, K, B) in [(1, 1, 1), (5, 7, 2), (33, 20, 3), (64, 9, 2)]:
+        p = rng.integers(0, 256, size=B * K * n, dtype=np.uint8)
+        re, im = oracle.ref_data_promote(p)
+        M = (re + 1j * im).reshape(B, K, n)
+        full = np.einsum("btr,btc->brc", np.conj(M), M)
+        tri = oracle.ref_herm_to_tri(full)
+        assert np.array_equal(oracle.xengine(p, n, K, B, 1), tri)
+        assert np.array_equal(oracle.xengine(p, n, K, B, 0), full)
+
+
+@needs_ref_kernels
+def test_tri_rows_cols_pinned_to_tri_decode():
+    # every packed index of a 2048-input triangle (2,098,176 entries): the
+    # reference's float decode and the oracle's exact one agree there
+    n = 2048
+    r, c = oracle.ref_tri_decode(n * (n + 1) // 2)
+    i, j = oracle.tri_rows_cols(n)
+    assert np.array_equal(r, i) and np.array_equal(c, j)
+
+
+@needs_ref_kernels
+def test_uv_cells_pinned_to_uv_cell():
+    # random baselines over and beyond a 4096 grid, and baselines placed within
+    # float resolution of a cell boundary (u / cell + Ng/2 = k + 1/2)
+    rng = np.random.default_rng(5)
+    ng, f, cell = 4096, 1.4e9, 1.0 / 3000.0
+    lam = oracle.C_LIGHT / f
+    uv = rng.uniform(-1.2, 1.2, size=(20000, 2)) * (ng / 2) * cell * lam
+    k = rng.integers(-ng // 2, ng // 2, size=(4000, 2)) + 0.5
+    edge = (k * cell * lam).astype(np.float32)
+    nudged = np.concatenate([edge, np.nextafter(edge, np.float32(np.inf)),
+                             np.nextafter(edge, np.float32(-np.inf))])
+    uv = np.concatenate([uv.astype(np.float32), nudged, np.zeros((1, 2), np.float32)])
+    iu, iv, iuc, ivc = oracle.uv_cells(uv, f, cell, ng)
+    riu, riv, ul, vl = oracle.ref_uv_cell(uv, f, cell, ng)
+    assert np.array_equal(iu, riu) and np.array_equal(iv, riv)
+    # the mirror cell, as the scatter kernel forms it from uv_cell's u_lam
+    c, h = np.float32(cell), np.float32(0.5 * ng)
+    assert np.array_equal(iuc, oracle._roundf((-ul / c).astype(np.float32) + h))
+    assert np.array_equal(ivc, oracle._roundf((-vl / c).astype(np.float32) + h))
+
+
+@needs_ref_kernels
+def test_reference_tri_decode_misassigns_large_indices():
+    # beyond ~10.6 M entries (inputs > 4607) the reference's float decode puts
+    # some diagonal entries on the next row with column -1; the library's
+    # gridding decodes exactly, so its cells follow tri_rows_cols there
+    n = 4700
+    r, c = oracle.ref_tri_decode(n * (n + 1) // 2)
+    i, j = oracle.tri_rows_cols(n)
+    bad = np.nonzero((r != i) | (c != j))[0]
+    assert bad.size > 0 and bad[0] == 10619135
+    assert (r[bad[0]], c[bad[0]]) == (4608, -1) and (i[bad[0]], j[bad[0]]) == (4607, 4607)
