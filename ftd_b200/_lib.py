@@ -83,6 +83,7 @@ PROTOTYPES = {
     "ftdx_herk_ftd": (_i, [_vp, _vp, _vp, ctypes.POINTER(FtdDesc), _i, _f, _f, _vp]),
     "ftdx_strided_batch_gemm": (ctypes.c_longlong, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _i,
                                                     _i, _vp]),
+    "ftdx_set_strided_mode": (_i, [_vp, _i]),
     "ftdx_wait_selftest": (_i, [_vp, _i, _vp]),
     "ftdx_xengine": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
     "ftdx_image_beams": (_i, [_vp, ctypes.POINTER(ImagingConfig), _vp, _vp, _vp, _vp]),

@@ -96,6 +96,10 @@ struct ftdx_context {
   // split-K partial triangles (grown on demand)
   uint8_t* split_ws = nullptr;
   size_t split_ws_cap = 0;
+  // stridedBatchGEMM's FP16 staging (narrowed input, FP16 triangles), grown on demand
+  uint8_t* strided_ws = nullptr;
+  size_t strided_ws_cap = 0;
+  int strided_mode = 0;  // FTDX_STRIDED_REFERENCE_FP16 or FTDX_STRIDED_SCALED_FP8
   std::map<std::tuple<int, int, int>, std::unique_ptr<ftdx::Plan>> plans;  // (N, kblocks, batch)
   std::map<uint64_t, std::shared_ptr<void>> vplans;  // batched-call plans by fingerprint
   // strategy of untuned calls (ftdx_set_strategy)

@@ -362,6 +362,7 @@ ftdx_status ftdx_destroy(ftdx_handle h) {
   if (h->z) cudaFree(h->z);
   if (h->aux) cudaFree(h->aux);
   if (h->split_ws) cudaFree(h->split_ws);
+  if (h->strided_ws) cudaFree(h->strided_ws);
   if (h->d_status) cudaFree(h->d_status);
   if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
   delete h;

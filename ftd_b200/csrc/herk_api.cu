@@ -709,27 +709,6 @@ ftdx_status ftdx_herk_ftd(ftdx_handle h, const void* raw, void* C, const ftdx_ft
   return launch_all(h, c, strat, static_cast<cudaStream_t>(stream));
 }
 
-long long ftdx_strided_batch_gemm(ftdx_handle h, const void* A, const void* B, void* C, int m,
-                                  int n, int k, int trans_a, int trans_b, int batch, int data_type,
-                                  void* stream) {
-  if (!h) return -1;
-  constexpr int kOpN = 0, kOpC = 2, kComplexFloat = 2;
-  const bool herk = A == B && trans_a == kOpC && trans_b == kOpN && m == n;
-  if (!herk || data_type != kComplexFloat) {
-    fail(h, FTDX_ERR_UNSUPPORTED,
-         "strided_batch_gemm: only the HERK pattern (A == B, op(A) = A^H, op(B) = B, m == n, "
-         "single complex) is implemented (got trans %d/%d, m %d, n %d, type %d)",
-         trans_a, trans_b, m, n, data_type);
-    return -1;
-  }
-  if (ftdx_herk(h, A, C, n, k, batch, FTDX_IN_FP32, FTDX_COMPUTE_FP8, FTDX_OUT_FP32,
-                FTDX_FORMAT_PACKED_TRIANGLE, 1.f, 0.f, stream, 1) != FTDX_OK)
-    return -1;
-  uint32_t bits = 0;
-  if (ftdx_device_status(h, stream, &bits) != FTDX_OK) return -1;
-  return 8LL * m * n * k * batch;
-}
-
 ftdx_status ftdx_xengine(ftdx_handle h, const void* payload, void* out, int n_ant, int K,
                          int batch, int mat_format, ftdx_output output, void* stream) {
   if (!h) return FTDX_ERR_INVALID_ARG;

@@ -30,9 +30,26 @@ struct CutlassComplexGemm::Impl {
       cfg.verbosity = strategy_verbosity > 1 ? strategy_verbosity : 0;
       cfg.tune_cache = tune_cache.empty() ? nullptr : tune_cache.c_str();
       create_status = ftdx_create(&h, &cfg);
-      if (create_status != FTDX_OK) h = nullptr;
+      if (create_status != FTDX_OK) {
+        h = nullptr;
+      } else {
+        if (direct_graph) ftdx_set_graph_mode(h, 1);
+        apply_mode();
+      }
     }
     return h;
+  }
+
+  // HerkMode -> this library's kernel (store mode of ftdx_set_strategy)
+  void apply_mode() {
+    if (!h) return;
+    switch (herk_mode) {
+      case HerkMode::ForceBaseline:
+        if (ftdx_set_strategy(h, 2, 0) != FTDX_OK) ftdx_set_strategy(h, 0, 0);
+        break;
+      case HerkMode::ForceDirect:
+      case HerkMode::Auto: ftdx_set_strategy(h, 0, 0); break;
+    }
   }
 };
 
@@ -52,7 +69,8 @@ int CutlassComplexGemm::herk(const void* A, void* C, int N, int K, int batch_cou
   return int(ftdx_herk(h, A, C, N, K, batch_count, ftdx_input(int(input)),
                        ftdx_compute(int(compute)), ftdx_output(int(output)),
                        ftdx_format(int(format)), alpha, beta, static_cast<void*>(stream),
-                       (tune || impl_->auto_tune) ? 1 : 0));
+                       ((tune || impl_->auto_tune) && impl_->herk_mode == HerkMode::Auto) ? 1
+                                                                                         : 0));
 }
 
 void CutlassComplexGemm::init_herk(int N, int K, int batch_count, cudaStream_t stream) {
@@ -74,15 +92,23 @@ void CutlassComplexGemm::set_gemm_tune_verbosity(int) {}
 void CutlassComplexGemm::set_gemm_tune_cache_path(const std::string&) {}
 void CutlassComplexGemm::set_kernel_tune_verbosity(int) {}
 void CutlassComplexGemm::set_kernel_tune_cache_path(const std::string&) {}
-void CutlassComplexGemm::set_herk_mode(HerkMode mode) { impl_->herk_mode = mode; }
+void CutlassComplexGemm::set_herk_mode(HerkMode mode) {
+  impl_->herk_mode = mode;
+  impl_->apply_mode();
+}
 void CutlassComplexGemm::set_tile_config(TileConfig config) { impl_->tile = config; }
 void CutlassComplexGemm::set_direct_tile_config(DirectTileConfig config) {
   impl_->direct_tile = config;
 }
-void CutlassComplexGemm::set_direct_herk_graph(bool enable) { impl_->direct_graph = enable; }
+void CutlassComplexGemm::set_direct_herk_graph(bool enable) {
+  impl_->direct_graph = enable;
+  if (impl_->h) ftdx_set_graph_mode(impl_->h, enable ? 1 : 0);
+}
 void CutlassComplexGemm::set_power_mode(PowerMode mode) { impl_->power = mode; }
 void CutlassComplexGemm::set_gemm_mode(GemmMode mode) { impl_->gemm = mode; }
 void CutlassComplexGemm::set_auto_tune(bool enable) { impl_->auto_tune = enable; }
+
+void* CutlassComplexGemm::native_handle() { return static_cast<void*>(impl_->get()); }
 
 void CutlassComplexGemm::print_build_info() {
   const int v = ftdx_version();

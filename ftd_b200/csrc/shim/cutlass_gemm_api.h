@@ -10,9 +10,17 @@
 //    combinations (compute precision FP6/FP4, which the reference maps to its
 //    MX block-scaled GEMMs).
 //  * K < 16 needs no padding by the caller (any K >= 1 is handled).
-//  * The CUTLASS-baseline tuning knobs (TileConfig, DirectTileConfig,
-//    HerkMode, PowerMode, GemmMode) are accepted and recorded; this library
-//    has one tcgen05 kernel family, whose launch shape the autotuner picks.
+//  * set_direct_herk_graph(true) turns on graph capture and replay of whole
+//    herk calls (ftdx_set_graph_mode), as the reference's direct-HERK graph
+//    cache does (cutlass_gemm_api.cu:200-315); false releases the graphs.
+//  * set_herk_mode picks this library's kernel: ForceDirect = the single-CTA
+//    persistent tcgen05 kernel, ForceBaseline = the CTA-pair (cta_group::2)
+//    kernel, Auto = the autotuner's choice.  While a mode is forced, herk
+//    calls skip the strategy tuning, so the forced kernel runs.
+//  * TileConfig, DirectTileConfig, PowerMode and GemmMode select tiles of the
+//    reference's CUTLASS and mma.sync kernels, which this library does not
+//    have; they are recorded and have no effect (the tcgen05 kernels' tiles
+//    and pipeline depth are fixed; the autotuner picks their launch shape).
 //  * The planar-complex GEMM / power-beamformer methods of the reference are
 //    not part of this library.
 #pragma once
@@ -70,6 +78,10 @@ class FTDX_SHIM_API CutlassComplexGemm {
   void set_auto_tune(bool enable);
 
   static void print_build_info();
+
+  // Not in the reference: the underlying ftdx_handle (created on first use),
+  // for callers that want this library's own C ABI on the same state.
+  void* native_handle();
 
   CutlassComplexGemm(const CutlassComplexGemm&) = delete;
   CutlassComplexGemm& operator=(const CutlassComplexGemm&) = delete;

@@ -1,11 +1,14 @@
 // ggp_cutlass_interface.cpp -- the GGP engine-boundary functions of
-// lib/cutlass_interface.cu:150-307 (namespace ggp), over one process-wide
-// CutlassComplexGemm, as the reference keeps one (:38-41).  Declarations are
-// the ones callers forward-declare (lib/visibility_pipeline.cu:11-22,
+// lib/cutlass_interface.cu:150-381: namespace ggp over one process-wide
+// CutlassComplexGemm, as the reference keeps one (:38-41), and
+// quda::stridedBatchGEMMCutlass.  The ggp:: declarations are the ones
+// callers forward-declare (lib/visibility_pipeline.cu:11-22,
 // lib/visibility_bf.cpp:15-21).  Returns 0 on success, never exits.
 #include <cuda_runtime.h>
 
 #include "cutlass_gemm_api.h"
+#include "ftdx.h"
+#include "ggp_blas_interface.h"
 
 using cutlass_gemm_api::ComputePrecision;
 using cutlass_gemm_api::CutlassComplexGemm;
@@ -60,3 +63,24 @@ FTDX_SHIM_API int herkBatchedCutlassFP16(const void* fp16_data, void* tri_output
 }
 
 }  // namespace ggp
+
+namespace quda {
+
+// The reference keeps this path on its process-wide CutlassComplexGemm; the
+// HERK-detecting BLAS entry needs this library's strided call, so it has its
+// own process-wide handle on the device current at the first call.
+long long stridedBatchGEMMCutlass(void* A_data, void* B_data, void* C_data, QudaBLASParam param,
+                                  QudaFieldLocation /*location*/) {
+  static ftdx_handle h = nullptr;
+  static ftdx_status created = [] {
+    ftdx_config cfg{};
+    cfg.device = -1;
+    return ftdx_create(&h, &cfg);
+  }();
+  if (created != FTDX_OK) return -1;
+  return ftdx_strided_batch_gemm(h, A_data, B_data, C_data, param.m, param.n, param.k,
+                                 int(param.trans_a), int(param.trans_b), param.batch_count,
+                                 int(param.data_type), nullptr);
+}
+
+}  // namespace quda

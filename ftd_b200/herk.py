@@ -168,6 +168,11 @@ class Correlator:
                                                    trans_a, trans_b, batch, data_type,
                                                    _stream(stream)))
 
+    def set_strided_mode(self, mode: int) -> None:
+        """Arithmetic of strided_batch_gemm: 0 the reference's FP16 narrowing
+        (default), 1 per-channel-scaled FP8 with FP32 output."""
+        check(self._h, self._L.ftdx_set_strided_mode(self._h, mode), "ftdx_set_strided_mode")
+
     def herk_kahan(self, A, S, comp, N: int, K: int, batch: int, input: int = IN_INT4,
                    compute: int = COMPUTE_FP8, stream=None) -> None:
         """S += A A^H with Kahan compensation kept in `comp` (both packed complex64)."""

@@ -257,11 +257,23 @@ FTDX_API ftdx_status ftdx_xengine(ftdx_handle h, const void* payload, void* out,
  * [batch][n][k] interleaved complex64 A into the packed lower triangle
  * (complex64) at C, and the reference's flop count 8*m*n*k*batch is returned
  * after the stream is synchronised.  Any other pattern returns -1 with the last
- * error set (the reference reports it through errorQuda).  FP8 with a
- * per-channel scale where the reference narrows to unscaled FP16 -> FP8. */
+ * error set (the reference reports it through errorQuda).
+ * Arithmetic (ftdx_set_strided_mode): by default the reference's own
+ * (FTDX_STRIDED_REFERENCE_FP16, lib/cutlass_interface.cu:333-367): each FP32
+ * component narrowed to FP16 (round to nearest), FP16 -> E4M3 unscaled
+ * (round to nearest, saturating at 448), FP32 accumulation, every result
+ * rounded to FP16 and widened to FP32 -- so results agree with the reference
+ * and share its range limits (FP16 output overflows past 65504).  Uses a
+ * library staging buffer of 4*(batch*n*k + batch*n(n+1)/2) bytes. */
 FTDX_API long long ftdx_strided_batch_gemm(ftdx_handle h, const void* A, const void* B, void* C,
                                            int m, int n, int k, int trans_a, int trans_b,
                                            int batch, int data_type, void* stream);
+/* Arithmetic of ftdx_strided_batch_gemm on this handle (no counterpart in the
+ * reference, which has only the first): FTDX_STRIDED_SCALED_FP8 runs the
+ * FP32-input FP8 mode with a per-channel scale (448 / max |component|) and
+ * FP32 output, for inputs outside FP16 / E4M3 range. */
+enum { FTDX_STRIDED_REFERENCE_FP16 = 0, FTDX_STRIDED_SCALED_FP8 = 1 };
+FTDX_API ftdx_status ftdx_set_strided_mode(ftdx_handle h, int mode);
 
 /* Kahan-compensated accumulation across integration dumps (no counterpart
  * in the reference): sum += A A^H with the FP32 rounding error of every

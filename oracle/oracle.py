@@ -595,6 +595,22 @@ def e4m3_rne(x: np.ndarray) -> np.ndarray:
     return np.copysign(q, x).astype(np.float32)
 
 
+def herk_fp16_narrowed(v: np.ndarray) -> np.ndarray:
+    """The reference's stridedBatchGEMMCutlass HERK arithmetic
+    (lib/cutlass_interface.cu:333-367) on complex64 voltages [batch, N, K]:
+    each FP32 component narrowed to FP16 (round to nearest), FP16 -> E4M3
+    unscaled (round to nearest, saturating at 448;
+    cutlass_interface/shared/cast_kernels_common.hpp:34-37), products summed
+    in FP64 (equal to the FP32 accumulation whenever every partial sum is
+    exact in FP32), Im of the diagonal 0, each result rounded to FP16 and
+    widened: packed lower triangles [batch, P, 2] float32."""
+    re = e4m3_rne(np.asarray(v.real, dtype=np.float32).astype(np.float16).astype(np.float32))
+    im = e4m3_rne(np.asarray(v.imag, dtype=np.float32).astype(np.float16).astype(np.float32))
+    B, N, K = v.shape
+    out = herk_c128(re.astype(np.float64) + 1j * im.astype(np.float64), N, K, B)
+    return out.astype(np.float16).astype(np.float32)
+
+
 def herk_fp8_scaled(v: np.ndarray, split: bool = False) -> np.ndarray:
     """Packed lower triangles [batch, P, 2] (float64) of the per-channel-scaled
     E4M3 product of complex64 voltages [batch, N, K] (split: hi hi + lo hi +

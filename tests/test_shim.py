@@ -31,3 +31,50 @@ def test_shim_caller_runs_bit_exact(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "OK" in r.stdout
+
+
+def _reference_include():
+    ref = os.environ.get("FTD_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
+    inc = os.path.join(ref, "include")
+    return inc if os.path.isfile(os.path.join(inc, "ggp.h")) else None
+
+
+def test_quda_blas_param_matches_reference_layout(tmp_path):
+    # the by-value QudaBLASParam of quda::stridedBatchGEMMCutlass: every member
+    # at the reference's offset (its own include/ggp.h, with an empty stand-in
+    # for the build-generated ggp_define.h), the same enumerator values, and a
+    # caller declared by the reference's header links against libftdx.so
+    inc = _reference_include()
+    if inc is None:
+        pytest.skip("reference headers not present")
+    src = os.path.join(ROOT, "tests", "cpp", "blas_layout.cpp")
+    stub = tmp_path / "stub"
+    stub.mkdir()
+    (stub / "ggp_define.h").write_text("")
+    outs = []
+    for ref in (True, False):
+        exe = str(tmp_path / ("ref" if ref else "ours"))
+        cmd = ["/usr/bin/g++", "-std=c++17", src, "-o", exe, "-I", f"{CUDA}/include",
+               "-L", LIBDIR, "-lftdx", f"-Wl,-rpath,{LIBDIR}", "-L", f"{CUDA}/lib64", "-lcudart",
+               f"-Wl,-rpath,{CUDA}/lib64"]
+        cmd += (["-DUSE_GGP_HEADER", "-I", inc, "-I", str(stub)] if ref else
+                ["-I", os.path.join(ROOT, "ftd_b200", "csrc", "shim"), "-I",
+                 os.path.join(ROOT, "include")])
+        subprocess.run(cmd, check=True, capture_output=True, text=True)
+        outs.append(subprocess.run([exe], capture_output=True, text=True, check=True).stdout)
+    assert outs[0] == outs[1]
+    assert outs[0].startswith("size 128\n")
+
+
+@pytest.mark.gpu
+def test_quda_strided_entry_refuses_non_herk_pattern(tmp_path):
+    # through the exported C++ symbol: a plain GEMM pattern returns -1
+    src = os.path.join(ROOT, "tests", "cpp", "blas_layout.cpp")
+    exe = str(tmp_path / "blas")
+    subprocess.run(["/usr/bin/g++", "-std=c++17", src, "-o", exe, "-I", f"{CUDA}/include",
+                    "-I", os.path.join(ROOT, "ftd_b200", "csrc", "shim"), "-I",
+                    os.path.join(ROOT, "include"), "-L", LIBDIR, "-lftdx",
+                    f"-Wl,-rpath,{LIBDIR}", "-L", f"{CUDA}/lib64", "-lcudart",
+                    f"-Wl,-rpath,{CUDA}/lib64"], check=True, capture_output=True, text=True)
+    r = subprocess.run([exe, "call"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "call -1" in r.stdout, r.stdout + r.stderr
