@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--no-extra", action="store_true", help="skip the extra workload legs")
     p.add_argument("--leg", default=None,
                    choices=["nvfp4", "nvfp4split", "raw", "imaging", "xengine", "splitk",
-                            "precision", "imaging_visbf", "batched", "xengine"],
+                            "precision", "imaging_visbf", "batched", "xengine", "peaks"],
                    help="run one extra workload alone and print its JSON (profiling cases); "
                         "nvfp4 and nvfp4split use --inputs/--channels/--k")
     p.add_argument("--strategy", default=None,
@@ -171,6 +171,17 @@ def measure_fp8_peak(torch, device):
         best = min(best, e0.elapsed_time(e1))
     del a, b
     return 2.0 * M ** 3 / best / 1e9
+
+
+def measure_tcgen05_peaks(device_index, iters=20000, reps=3):
+    """Dense tcgen05 throughput (TFLOPS) of the MMA shapes the correlators use,
+    from ftdx_peak_probe: M = N = 256 CTA-pair MMAs from fixed shared-memory
+    tiles, FP8 E4M3 (K = 32) and NVFP4 block16 (K = 64), no loads or stores."""
+    from ftd_b200 import Correlator
+    with Correlator(device=device_index) as c:
+        return {"fp8_e4m3": c.peak_probe(0, iters, reps), "nvfp4": c.peak_probe(1, iters, reps),
+                "what": f"{iters} back-to-back tcgen05.mma.cta_group::2 M=N=256 per SM pair, "
+                        f"best of {reps} launches"}
 
 
 def measure_int8_peak(torch, device):
@@ -398,9 +409,10 @@ def run_ours(args, rank, world, dist):
         precision = run_precision_leg(torch, dev)
         differentiation = run_diff_leg(torch, dev)
 
-    peak = None
+    peak = probes = None
     if not args.no_peak:
         peak = measure_fp8_peak(torch, dev)
+        probes = measure_tcgen05_peaks(local)
 
     if rank != 0:
         return 0
@@ -447,7 +459,9 @@ def run_ours(args, rank, world, dist):
                      "kernel": kernel_name,
                      "kernel_ms": herk_ms,
                      "peak_source": peak_source,
-                     "frac_of_nominal_4500": achieved / NOMINAL_FP8_TFLOPS},
+                     "frac_of_nominal_4500": achieved / NOMINAL_FP8_TFLOPS,
+                     "tcgen05_probe_peaks": probes,
+                     "frac_of_fp8_probe": (achieved / probes["fp8_e4m3"]) if probes else None},
         "kernels": {kernel_name + "_ms": herk_ms, prep_name + "_ms": prep_ms},
         "gpu_launches": 2 * args.steps,
         "strategy": {"tuned": tuned, "graph_replay": True},
@@ -839,7 +853,10 @@ def run_leg(args):
     import torch
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
-    if args.leg == "nvfp4":
+    if args.leg == "peaks":
+        out = measure_tcgen05_peaks(dev.index)
+        out["fp8_cublaslt_8192"] = measure_fp8_peak(torch, dev)
+    elif args.leg == "nvfp4":
         sm = int(args.strategy.split(",")[0]) if args.strategy else None
         out = run_nvfp4_case(torch, dev, args.inputs, args.k, args.channels, store_mode=sm)
     elif args.leg == "nvfp4split":

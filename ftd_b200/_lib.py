@@ -84,6 +84,7 @@ PROTOTYPES = {
     "ftdx_strided_batch_gemm": (ctypes.c_longlong, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _i,
                                                     _i, _vp]),
     "ftdx_set_strided_mode": (_i, [_vp, _i]),
+    "ftdx_peak_probe": (_i, [_vp, _i, _i, _i, ctypes.POINTER(ctypes.c_double)]),
     "ftdx_wait_selftest": (_i, [_vp, _i, _vp]),
     "ftdx_xengine": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
     "ftdx_image_beams": (_i, [_vp, ctypes.POINTER(ImagingConfig), _vp, _vp, _vp, _vp]),

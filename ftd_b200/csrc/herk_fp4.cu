@@ -246,16 +246,14 @@ struct Fp4Args {
 // Epilogue of one 32-column accumulator chunk: rows i0..i0+15 (columns 2m,
 // 2m+1 = Re, Im of row i0+m) of lane j's column.  Element (i, j <= i < n)
 // = r * alpha g_i g_j (+ beta * old), the diagonal the exact row power;
-// sc_j = alpha g_j.  The 16 row scales arrive in one load per lane and warp
-// shuffles; chunks wholly below the diagonal and inside n store unmasked.
-// Row i0+m of the packed triangle starts m i0 + m(m+1)/2 after row i0.
+// sc_j = alpha g_j, gl = g_(i0 + lane % 16) (prefetched; the 16 row scales
+// reach every lane by warp shuffles); chunks wholly below the diagonal and
+// inside n store unmasked.  Row i0+m of the packed triangle starts
+// m i0 + m(m+1)/2 after row i0.
 __device__ __forceinline__ void fp4_store_chunk(float2* __restrict__ outc, const uint32_t (&r)[32],
-                                                int i0, int j, int jw, int n, float sc_j,
-                                                const float* __restrict__ rs,
+                                                int i0, int j, int jw, int n, float sc_j, float gl,
                                                 const float* __restrict__ pw, float alpha,
-                                                float beta, int lane) {
-  const int il = i0 + (lane & 15);
-  const float gl = il < n ? __ldg(rs + il) : 0.f;
+                                                float beta) {
   const bool interior = (i0 + 15 < n) && (jw + 31 < i0);
   float2* p0 = outc + int64_t(i0) * (i0 + 1) / 2 + j;
 #pragma unroll
@@ -281,6 +279,105 @@ __device__ __forceinline__ void fp4_store_chunk(float2* __restrict__ outc, const
       }
       __stcs(p, make_float2(vr, vi));
     }
+  }
+}
+
+// Row scales one epilogue warp needs for one tile: alpha g_j of its lane's
+// column and g_i of row i0 + lane % 16 for each of its accumulator chunks.
+template <int kChunksPerWarp>
+struct Fp4TileScales {
+  float sc_j;
+  float gl[kChunksPerWarp];
+};
+
+// The epilogue warps' tile loop of both NVFP4 kernels.  A warp drains TMEM
+// lane quarter q (32 columns j) of each accumulator, chunks grp, grp +
+// kEpiGroups, ... of 32 columns (16 rows i).  The global loads a tile needs
+// run ahead of its accumulator: tile and channel descriptors two tiles ahead,
+// row scales one tile ahead, so that no tile's stores wait on a load (the
+// MMAs of a tile take about as long as one descriptor -> channel -> scale
+// chain of dependent loads).
+//   jt: inputs j per tile (TileDesc::tj unit); jo: this CTA's first j in it;
+//   it: inputs i per tile; kCols: accumulator columns (2 per input i).
+template <int kCols>
+__device__ __forceinline__ void fp4_epilogue(const Fp4Args& args, uint32_t tmem_base, int first,
+                                             int stride, int jt, int jo, int it, int q, int grp,
+                                             int lane, uint32_t tfull0, uint32_t tempty0,
+                                             bool cluster_release, volatile int* abort_flag) {
+  constexpr int kChunks = kCols / 32;
+  constexpr int kPer = (kChunks + k4EpiGroups - 1) / k4EpiGroups;
+  using Scales = Fp4TileScales<kPer>;
+  const int nt = args.num_tiles;
+  float2* out = static_cast<float2*>(args.out);
+  auto load_scales = [&](const TileDesc& td, const ChanDesc& cd) {
+    Scales sv;
+    const int j = int(td.tj) * jt + jo + q * 32 + lane;
+    sv.sc_j = args.alpha * (j < cd.n ? __ldg(args.row_scale + cd.row0 + j) : 0.f);
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int c = grp + k * k4EpiGroups;
+      const int il = int(td.ti) * it + 16 * c + (lane & 15);
+      sv.gl[k] = (c < kChunks && il < cd.n) ? __ldg(args.row_scale + cd.row0 + il) : 0.f;
+    }
+    return sv;
+  };
+  int t = first;
+  if (t >= nt) return;
+  TileDesc td0 = args.tiles[t];
+  ChanDesc cd0 = args.chans[td0.ch];
+  TileDesc td1 = t + stride < nt ? args.tiles[t + stride] : td0;
+  ChanDesc cd1 = args.chans[td1.ch];
+  Scales s0 = load_scales(td0, cd0);
+  int acc = 0;
+  uint32_t acc_phase = 0;
+  for (; t < nt; t += stride) {
+    const TileDesc td2 = t + 2 * stride < nt ? args.tiles[t + 2 * stride] : td1;
+    const Scales s1 = load_scales(td1, cd1);
+    const uint32_t tfull = tfull0 + 8u * uint32_t(acc);
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(tfull, acc_phase, abort_flag));
+    if (!ok) {
+      if (lane == 0) atomicOr(args.status, kStatusTimeoutEpilogue);
+      break;
+    }
+    tc_fence_after();
+    const int n = cd0.n;
+    const int jw = int(td0.tj) * jt + jo + q * 32;
+    const int j = jw + lane;
+    const int ib = int(td0.ti) * it;
+    float2* outc = out + cd0.out0;
+    const uint32_t tb = tmem_base + (uint32_t(q * 32) << 16) + uint32_t(acc * kCols);
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int c = grp + k * k4EpiGroups;
+      if (c >= kChunks) break;
+      const int i0 = ib + 16 * c;
+      if (i0 + 15 < jw || i0 >= n) continue;  // warp-uniform: nothing to store
+      uint32_t r[32];
+      __syncwarp();
+      tmem_ld_32x32b_x32(tb + 32u * c, r);
+      tmem_wait_ld();
+      fp4_store_chunk(outc, r, i0, j, jw, n, s0.sc_j, s0.gl[k], args.row_power + cd0.row0,
+                      args.alpha, args.beta);
+    }
+    tc_fence_before();
+    __syncwarp();
+    if (lane == 0) {
+      const uint32_t te = tempty0 + 8u * uint32_t(acc);
+      if (cluster_release)
+        mbar_arrive_cluster_relaxed(map_shared(te, 0));
+      else
+        mbar_arrive(te);
+    }
+    if (++acc == 2) {
+      acc = 0;
+      acc_phase ^= 1u;
+    }
+    const ChanDesc cd2 = args.chans[td2.ch];
+    td0 = td1;
+    cd0 = cd1;
+    s0 = s1;
+    td1 = td2;
+    cd1 = cd2;
   }
 }
 
@@ -436,46 +533,9 @@ __global__ void __launch_bounds__(k4Threads, 1)
   } else {
     // ------------------------------------------------ epilogue (warps 2..)
     // warp w drains lane quarter w % 4, column chunks c = (w - 2) / 4 mod groups
-    const int q = warp & 3;
-    const int grp = (warp - 2) >> 2;
-    int acc = 0;
-    uint32_t acc_phase = 0;
-    float2* out = static_cast<float2*>(args.out);
-    for (int t = blockIdx.x; t < args.num_tiles; t += gridDim.x) {
-      const TileDesc td = args.tiles[t];
-      const ChanDesc cd = args.chans[td.ch];
-      const bool ok = __all_sync(0xffffffffu, mbar_wait(tfull_bar(acc), acc_phase, abort_flag));
-      if (!ok) {
-        if (lane == 0) atomicOr(args.status, kStatusTimeoutEpilogue);
-        break;
-      }
-      tc_fence_after();
-      const int n = cd.n;
-      const int jw = int(td.tj) * k4J + q * 32;
-      const int j = jw + lane;
-      const int ib = int(td.ti) * k4I;
-      const float sc = args.alpha * (j < n ? args.row_scale[cd.row0 + j] : 0.f);  // alpha g_j
-      float2* outc = out + cd.out0;
-      const uint32_t tb = tmem_base + (uint32_t(q * 32) << 16) + uint32_t(acc * k4AccCols);
-#pragma unroll 1
-      for (int c = grp; c < k4AccCols / 32; c += k4EpiGroups) {
-        const int i0 = ib + 16 * c;
-        if (i0 + 15 < jw || i0 >= n) continue;
-        uint32_t r[32];
-        __syncwarp();
-        tmem_ld_32x32b_x32(tb + 32u * c, r);
-        tmem_wait_ld();
-        fp4_store_chunk(outc, r, i0, j, jw, n, sc, args.row_scale + cd.row0,
-                        args.row_power + cd.row0, args.alpha, args.beta, lane);
-      }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(tempty_bar(acc));
-      if (++acc == 2) {
-        acc = 0;
-        acc_phase ^= 1u;
-      }
-    }
+    fp4_epilogue<k4AccCols>(args, tmem_base, blockIdx.x, gridDim.x, k4J, 0, k4I, warp & 3,
+                            (warp - 2) >> 2, lane, tfull_bar(0), tempty_bar(0), false,
+                            abort_flag);
   }
   tc_fence_before();
   __syncthreads();
@@ -672,47 +732,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(k4pThreads, 1)
     }
   } else {
     // ------------------------------------------------ epilogue (warps 2.., both CTAs)
-    // warp w drains lane quarter w % 4, column chunks c = (w - 2) / 4 mod groups
-    const int q = warp & 3;
-    const int grp = (warp - 2) >> 2;
-    int acc = 0;
-    uint32_t acc_phase = 0;
-    float2* out = static_cast<float2*>(args.out);
-    for (int t = pair; t < args.num_tiles; t += npairs) {
-      const TileDesc td = args.tiles[t];
-      const ChanDesc cd = args.chans[td.ch];
-      const bool ok = __all_sync(0xffffffffu, mbar_wait(tfull_bar(acc), acc_phase, abort_flag));
-      if (!ok) {
-        if (lane == 0) atomicOr(args.status, kStatusTimeoutEpilogue);
-        break;
-      }
-      tc_fence_after();
-      const int n = cd.n;
-      const int jw = int(td.tj) * k4pJ + 128 * int(rank) + q * 32;
-      const int j = jw + lane;
-      const int ib = int(td.ti) * k4pI;
-      const float sc = args.alpha * (j < n ? args.row_scale[cd.row0 + j] : 0.f);  // alpha g_j
-      float2* outc = out + cd.out0;
-      const uint32_t tb = tmem_base + (uint32_t(q * 32) << 16) + uint32_t(acc * k4pAccCols);
-#pragma unroll 1
-      for (int c = grp; c < k4pAccCols / 32; c += k4EpiGroups) {
-        const int i0 = ib + 16 * c;
-        if (i0 + 15 < jw || i0 >= n) continue;  // warp-uniform: nothing to store
-        uint32_t r[32];
-        __syncwarp();
-        tmem_ld_32x32b_x32(tb + 32u * c, r);
-        tmem_wait_ld();
-        fp4_store_chunk(outc, r, i0, j, jw, n, sc, args.row_scale + cd.row0,
-                        args.row_power + cd.row0, args.alpha, args.beta, lane);
-      }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive_cluster_relaxed(map_shared(tempty_bar(acc), 0));
-      if (++acc == 2) {
-        acc = 0;
-        acc_phase ^= 1u;
-      }
-    }
+    // warp w drains lane quarter w % 4, column chunks c = (w - 2) / 4 mod groups;
+    // both CTAs release an accumulator on the leader's barrier
+    fp4_epilogue<k4pAccCols>(args, tmem_base, pair, npairs, k4pJ, 128 * int(rank), k4pI,
+                             warp & 3, (warp - 2) >> 2, lane, tfull_bar(0), tempty_bar(0), true,
+                             abort_flag);
   }
   tc_fence_before();
   __syncthreads();

@@ -168,6 +168,13 @@ class Correlator:
                                                    trans_a, trans_b, batch, data_type,
                                                    _stream(stream)))
 
+    def peak_probe(self, kind: int, iters: int = 20000, reps: int = 3) -> float:
+        """Measured dense tensor-core TFLOPS: kind 0 FP8 E4M3, 1 NVFP4."""
+        out = ctypes.c_double(0.0)
+        check(self._h, self._L.ftdx_peak_probe(self._h, kind, iters, reps, ctypes.byref(out)),
+              "ftdx_peak_probe")
+        return float(out.value)
+
     def set_strided_mode(self, mode: int) -> None:
         """Arithmetic of strided_batch_gemm: 0 the reference's FP16 narrowing
         (default), 1 per-channel-scaled FP8 with FP32 output."""

@@ -415,6 +415,15 @@ FTDX_API ftdx_status ftdx_gain_gradient(ftdx_handle h, const void* R_obs, const 
                                         const float* W, const void* g, int N, int n_chans,
                                         double* grad, double* loss, void* stream);
 
+/* Dense tensor-core throughput of this GPU (no counterpart in the reference),
+ * for roofline denominators: every SM pair issues `iters` back-to-back
+ * tcgen05.mma.cta_group::2 of M = N = 256 from fixed shared-memory tiles
+ * (kind 0: FP8 E4M3, K = 32; kind 1: NVFP4 E2M1 with UE4M3 block-16 scales,
+ * K = 64), FP32 accumulation, no loads or stores; the fastest of `reps`
+ * timed launches (after one warm-up) gives *tflops = 2 M N K MMAs / time.
+ * Synchronises the device. */
+FTDX_API ftdx_status ftdx_peak_probe(ftdx_handle h, int kind, int iters, int reps, double* tflops);
+
 /* Kernel timing (no counterpart in the reference; its benches time whole
  * calls).  While enabled, CUDA events are recorded on the caller's stream
  * around every kernel this handle launches.  ftdx_profile_read synchronises,
