@@ -839,6 +839,13 @@ def run_nvfp4_case(torch, dev, N, K, B, reps=5, seed=1, split=False, store_mode=
         ms = _timed(torch, lambda: c.herk(A, C, N, K, B, input=IN_FP32, compute=mode,
                                           output=OUT_FP32, tune=tune), reps=reps)
         tuned = c.lookup_tuned(N, K, B, input=IN_FP32, output=OUT_FP32) if tune else None
+        # per-phase CUDA-event times of the same calls (quantiser, correlator)
+        c.set_profiling(True)
+        for _ in range(reps):
+            c.herk(A, C, N, K, B, input=IN_FP32, compute=mode, output=OUT_FP32, tune=tune)
+        torch.cuda.synchronize()
+        prof = c.profile_read()
+        c.set_profiling(False)
         if c.device_status() != 0:
             raise RuntimeError("device status after the NVFP4 case")
     kernel = ("herk_fp4_pair_kernel" if (store_mode if store_mode is not None else
@@ -846,7 +853,9 @@ def run_nvfp4_case(torch, dev, N, K, B, reps=5, seed=1, split=False, store_mode=
               else "herk_fp4_tc_kernel")
     return {"workload": f"NVFP4{' hi+lo' if split else ''}: {N} inputs x {B} channels x K={K}, "
                         f"Gaussian FP32 complex", "kernel": kernel,
-            "value": herk_flops(N, K, B) / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms}
+            "value": herk_flops(N, K, B) / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms,
+            "quantiser_ms": prof["prep_ms"] / max(prof["prep_launches"], 1),
+            "correlator_ms": prof["herk_ms"] / max(prof["herk_launches"], 1)}
 
 
 def run_leg(args):

@@ -130,9 +130,16 @@ ftdx_status launch_fp4(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   if (st != FTDX_OK) return st;
   cudaError_t e;
   {
-    ScopedTimer tm(h, s, 0);
-    e = launch_nvfp4(c.A, rows, c.K, c.N, c.batch, h->z, plan->d_tiles, plan->d_chans, plan->num_tiles, c.C, c.alpha, c.beta,
-                     h->d_status, h->sm_count, tensor_map_encoder(), s, split, pair);
+    ScopedTimer tm(h, s, 1);  // quantiser passes
+    e = launch_nvfp4(c.A, rows, c.K, c.N, c.batch, h->z, plan->d_tiles, plan->d_chans,
+                     plan->num_tiles, c.C, c.alpha, c.beta, h->d_status, h->sm_count,
+                     tensor_map_encoder(), s, split, pair, 1);
+  }
+  if (e == cudaSuccess) {
+    ScopedTimer tm(h, s, 0);  // correlator
+    e = launch_nvfp4(c.A, rows, c.K, c.N, c.batch, h->z, plan->d_tiles, plan->d_chans,
+                     plan->num_tiles, c.C, c.alpha, c.beta, h->d_status, h->sm_count,
+                     tensor_map_encoder(), s, split, pair, 2);
   }
   return e == cudaSuccess ? FTDX_OK : cuda_fail(h, e, "NVFP4 launch");
 }

@@ -1,6 +1,6 @@
 // herk_fp4.cu -- NVFP4 correlator for float complex voltages.
 //
-// Quantisation (nvfp4_prepare_kernel, one pass over the input): per input
+// Quantisation (nvfp4_stats_kernel, nvfp4_order_kernel, nvfp4_quant_kernel): per input
 // row a an FP32 scale g_a = amax_a / (6 * 448); per block of 16 values along
 // K (8 complex samples, Re/Im interleaved) a UE4M3 block scale b >= amax_blk
 // / (6 g_a) (rounded up, so no element saturates); elements E2M1(v / (g_a b)),
@@ -66,11 +66,6 @@ __device__ __forceinline__ float ue4m3_value(uint32_t c) {
 __device__ __forceinline__ uint32_t fp4x2(float a, float b) {
   return uint32_t(__nv_cvt_float2_to_fp4x2(make_float2(a, b), __NV_E2M1, cudaRoundNearest));
 }
-// Values of a byte of two E2M1 codes.
-__device__ __forceinline__ float2 fp4x2_value(uint32_t byte) {
-  const __half2_raw h = __nv_cvt_fp4x2_to_halfraw2(__nv_fp4x2_storage_t(byte), __NV_E2M1);
-  return __half22float2(__half2(h));
-}
 
 // Block scales in the tcgen05 scale-factor atom: one 512-byte atom per 128
 // operand rows and k-step (64 E2M1 values = 4 blocks); row m of the group at
@@ -94,113 +89,261 @@ __device__ __forceinline__ int64_t sf_atom_byte(int64_t group, int nks, int nsub
   return ((group * nks + ks) * nsub + (m >> 7)) * 512 + (m & 31) * 16 + ((m >> 5) & 3) * 4 + blk;
 }
 
-// Quantise one 16-value block (8 complex samples x[2q] = Re, x[2q+1] = Im)
-// of input row r (channel c, input w) under the row's FP32 scale g: a UE4M3
-// block scale b >= amax_blk / (6 g) (rounded up, so no element saturates) and
-// E2M1(v / (g b)), round to nearest even, into the x = (re, im) and
-// y = (im, -re) operand rows.  split: each operand row holds the hi half
-// (pitch bytes) then the lo half, lo = E2M1 of the residual x - hi with its
-// own block scale (same g), so hi + lo carries about twice the bits; the lo
-// k-steps of the scales follow the hi ones.  Scales go to sfa (x rows, per
-// input) and sfb (x and y rows, two per input).
-__device__ __forceinline__ void nvfp4_block(float (&x)[16], float g, int64_t r, int c, int w,
-                                            int b, uint8_t* __restrict__ z,
-                                            uint8_t* __restrict__ sfa, uint8_t* __restrict__ sfb,
-                                            int pitch, const SfGeom& sg, int split) {
-  const int rpitch = split ? 2 * pitch : pitch;
-  const int ksh = pitch / 32;  // k-steps per half
+// Values of a byte of two E2M1 codes (low nibble first).
+__device__ __forceinline__ float2 fp4x2_value(uint32_t byte) {
+  const __half2_raw h = __nv_cvt_fp4x2_to_halfraw2(__nv_fp4x2_storage_t(byte), __NV_E2M1);
+  return __half22float2(__half2(h));
+}
+
+// E2M1 codes of x[0..15] * inv (round to nearest even, saturating at 6) into
+// w (x = (re, im) byte order: element 2q in the low nibble of byte q) and
+// the squared error sum of fl(d d), d = fma(-code, gb, x), in element order.
+__device__ __forceinline__ float nvfp4_codes_err(const float (&x)[16], float inv, float gb,
+                                                 uint32_t (&w)[2]) {
+  w[0] = w[1] = 0u;
+  float err = 0.f;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const uint32_t byte = fp4x2(__fmul_rn(x[2 * q], inv), __fmul_rn(x[2 * q + 1], inv));
+    w[q >> 2] |= byte << (8 * (q & 3));
+    const float2 h = fp4x2_value(byte);
+    const float d0 = __fmaf_rn(-h.x, gb, x[2 * q]), d1 = __fmaf_rn(-h.y, gb, x[2 * q + 1]);
+    err = __fadd_rn(err, __fmul_rn(d0, d0));
+    err = __fadd_rn(err, __fmul_rn(d1, d1));
+  }
+  return err;
+}
+
+// Quantise 16 values (8 complex samples, x[2q] = Re, x[2q+1] = Im) under the
+// row's FP32 scale g into E2M1 codes of the x = (re, im) and y = (im, -re)
+// operand rows.  The UE4M3 block scale is the better of two candidates by
+// squared error: c0 = the smallest E4M3 value >= amax / (6 g) (no element
+// saturates) and the next smaller code c0 - 1 when that is >= 1 (the largest
+// element may saturate at 6, the rest land on a finer grid).  Every step is
+// an explicitly rounded float32 operation (no contraction), so the choice is
+// reproducible: gb = g b, inv = 1 / gb, codes = E2M1(x inv),
+// err = sum of fl(d d) with d = fma(-code, gb, x); c0 - 1 wins only on a
+// strictly smaller err.  Returns the chosen code; gb_out = g b of it.
+__device__ __forceinline__ uint32_t nvfp4_quant16(const float (&x)[16], float g, uint32_t (&xw)[2],
+                                                  uint32_t (&yw)[2], float& gb_out) {
   float amax = 0.f;
 #pragma unroll
   for (int q = 0; q < 16; ++q) amax = fmaxf(amax, fabsf(x[q]));
-  const uint32_t bc = ue4m3_ceil(amax / (6.f * g));
-  const float inv = bc ? 1.f / (g * ue4m3_value(bc)) : 0.f;
-  uint32_t xw[2] = {0u, 0u}, yw[2] = {0u, 0u};
-#pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    const float re = x[2 * q] * inv, im = x[2 * q + 1] * inv;
-    xw[q >> 2] |= fp4x2(re, im) << (8 * (q & 3));
-    yw[q >> 2] |= fp4x2(im, -re) << (8 * (q & 3));
+  const uint32_t c0 = ue4m3_ceil(__fdiv_rn(amax, __fmul_rn(6.f, g)));
+  const float gb0 = c0 ? __fmul_rn(g, ue4m3_value(c0)) : 0.f;
+  const float err0 = nvfp4_codes_err(x, c0 ? __frcp_rn(gb0) : 0.f, gb0, xw);
+  uint32_t best = c0;
+  gb_out = gb0;
+  if (c0 >= 2) {
+    const float gb1 = __fmul_rn(g, ue4m3_value(c0 - 1));
+    uint32_t w1[2];
+    const float err1 = nvfp4_codes_err(x, __frcp_rn(gb1), gb1, w1);
+    if (err1 < err0) {
+      best = c0 - 1;
+      gb_out = gb1;
+      xw[0] = w1[0], xw[1] = w1[1];
+    }
   }
+  // y = (im, -re): swap the nibbles of every byte and flip the sign bit of
+  // the new high nibble (-0 for a zero code: the same value in the MMA)
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+    yw[h] = (((xw[h] & 0x0F0F0F0Fu) ^ 0x08080808u) << 4) | ((xw[h] >> 4) & 0x0F0F0F0Fu);
+  return best;
+}
+
+// One 16-value block b of input row r (channel c, input w): the hi codes and,
+// when `lo`, the residual r = fma(-code, g b, x) quantised again with its own
+// block scale (same g).  Each operand row holds the hi half (pitch bytes) then
+// the lo half; the lo k-steps of the scales follow the hi ones.  Scales go to
+// sfa (x rows, one per input) and sfb (x and y rows, two per input).
+__device__ __forceinline__ void nvfp4_block(const float (&x)[16], float g, int64_t r, int c, int w,
+                                            int b, uint8_t* __restrict__ z,
+                                            uint8_t* __restrict__ sfa, uint8_t* __restrict__ sfb,
+                                            int pitch, const SfGeom& sg, bool lo) {
+  const int rpitch = 2 * pitch;
+  const int ksh = pitch / 32;  // k-steps per half
+  uint32_t xw[2], yw[2];
+  float gb = 0.f;
+  const uint32_t bc = nvfp4_quant16(x, g, xw, yw, gb);
   *reinterpret_cast<uint2*>(z + (2 * r) * rpitch + 8 * b) = make_uint2(xw[0], xw[1]);
   *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + 8 * b) = make_uint2(yw[0], yw[1]);
   const int64_t ga = int64_t(c) * sg.gA + (w >> 7);
-  const int64_t gb = int64_t(c) * sg.gB + (2 * w) / sg.gbrows;
+  const int64_t gbk = int64_t(c) * sg.gB + (2 * w) / sg.gbrows;
   const int ob = (2 * w) % sg.gbrows;  // x row in the group; y row next (gbrows is even)
   const int ks = b >> 2, blk = b & 3;
   sfa[sf_atom_byte(ga, sg.nks, 1, ks, w & 127, blk)] = uint8_t(bc);
-  sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ks, ob, blk)] = uint8_t(bc);
-  sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ks, ob + 1, blk)] = uint8_t(bc);
-  if (split) {
-    // residual of the hi quantisation, then its own block scale
-    const float step = bc ? g * ue4m3_value(bc) : 0.f;
-    float amax2 = 0.f;
+  sfb[sf_atom_byte(gbk, sg.nks, sg.nsub, ks, ob, blk)] = uint8_t(bc);
+  sfb[sf_atom_byte(gbk, sg.nks, sg.nsub, ks, ob + 1, blk)] = uint8_t(bc);
+  if (lo) {  // the residual fma(-code, g b, x) quantised with its own block scale
+    float res[16];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const float2 h = fp4x2_value((xw[q >> 2] >> (8 * (q & 3))) & 0xFFu);
-      x[2 * q] -= h.x * step;
-      x[2 * q + 1] -= h.y * step;
-      amax2 = fmaxf(amax2, fmaxf(fabsf(x[2 * q]), fabsf(x[2 * q + 1])));
+      res[2 * q] = __fmaf_rn(-h.x, gb, x[2 * q]);
+      res[2 * q + 1] = __fmaf_rn(-h.y, gb, x[2 * q + 1]);
     }
-    const uint32_t bc2 = ue4m3_ceil(amax2 / (6.f * g));
-    const float inv2 = bc2 ? 1.f / (g * ue4m3_value(bc2)) : 0.f;
-    uint32_t xl[2] = {0u, 0u}, yl[2] = {0u, 0u};
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const float re = x[2 * q] * inv2, im = x[2 * q + 1] * inv2;
-      xl[q >> 2] |= fp4x2(re, im) << (8 * (q & 3));
-      yl[q >> 2] |= fp4x2(im, -re) << (8 * (q & 3));
-    }
+    uint32_t xl[2], yl[2];
+    float gb2 = 0.f;
+    const uint32_t bc2 = nvfp4_quant16(res, g, xl, yl, gb2);
     *reinterpret_cast<uint2*>(z + (2 * r) * rpitch + pitch + 8 * b) = make_uint2(xl[0], xl[1]);
     *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + pitch + 8 * b) = make_uint2(yl[0], yl[1]);
     sfa[sf_atom_byte(ga, sg.nks, 1, ksh + ks, w & 127, blk)] = uint8_t(bc2);
-    sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ksh + ks, ob, blk)] = uint8_t(bc2);
-    sfb[sf_atom_byte(gb, sg.nks, sg.nsub, ksh + ks, ob + 1, blk)] = uint8_t(bc2);
+    sfb[sf_atom_byte(gbk, sg.nks, sg.nsub, ksh + ks, ob, blk)] = uint8_t(bc2);
+    sfb[sf_atom_byte(gbk, sg.nks, sg.nsub, ksh + ks, ob + 1, blk)] = uint8_t(bc2);
   }
 }
 
-// One warp per input row, one pass over HBM.  Pass 1 reads the row for its
-// max |Re|, |Im| (the row's FP32 scale g_r = amax_r / (6 * 448), 1 for an
-// empty row; NaN counts as 0) and its autocorrelation sum_t |v_t|^2
-// (accumulated in FP64 in a fixed order, so deterministic); pass 2 reads it
-// again, now from L2, and quantises it block by block (lane l: blocks l,
-// l + 32, ...).  The correlator multiplies each product by g_i g_j.
-__global__ void __launch_bounds__(256) nvfp4_prepare_kernel(
-    const float2* __restrict__ a, uint8_t* __restrict__ z, uint8_t* __restrict__ sfa,
-    uint8_t* __restrict__ sfb, float* __restrict__ power, float* __restrict__ rscale,
-    int64_t rows, int K, int pitch, SfGeom sg, int split) {
+// Pass 1, one warp per input row: max |Re|, |Im| (the row's FP32 scale
+// g_r = amax_r / (6 * 448), 1 for an empty row; NaN counts as 0) and the
+// autocorrelation sum_t |v_t|^2 (FP64, fixed order, so deterministic).  With
+// `rfi`, a second read of the row (from L2) flags the time samples with
+// |v_t|^2 > 25 x the row's mean power in the channel's bitmap.
+constexpr double kRfiThreshold = 25.0;
+__global__ void __launch_bounds__(256) nvfp4_stats_kernel(
+    const float2* __restrict__ a, float* __restrict__ power, float* __restrict__ rscale,
+    uint32_t* __restrict__ flags, int64_t rows, int K, int n, int fwords, int rfi) {
   const int lane = threadIdx.x & 31;
-  const int blocks_per_row = pitch / 8;  // 8 bytes of E2M1 per block
+  // rows of an even K at a 16-byte aligned base: two samples per load
   const bool vec = (K & 1) == 0 && (reinterpret_cast<uintptr_t>(a) & 15) == 0;
   for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < rows;
        r += (int64_t(gridDim.x) * blockDim.x) >> 5) {
     const float2* p = a + r * K;
     double acc = 0.0;
     float m = 0.f;
-    for (int t0 = lane; t0 < K; t0 += 128) {  // four loads in flight per lane
-      float2 v[4];
+    if (vec) {
+      const float4* p4 = reinterpret_cast<const float4*>(p);
+      const int k2 = K >> 1;
+      for (int t0 = lane; t0 < k2; t0 += 128) {  // four 16-byte loads in flight per lane
+        float4 v[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
-        v[u] = (t0 + 32 * u < K) ? __ldg(p + t0 + 32 * u) : make_float2(0.f, 0.f);
+        for (int u = 0; u < 4; ++u)
+          v[u] = (t0 + 32 * u < k2) ? __ldg(p4 + t0 + 32 * u) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        acc += double(v[u].x) * v[u].x + double(v[u].y) * v[u].y;
-        m = fmaxf(m, fmaxf(fabsf(v[u].x), fabsf(v[u].y)));
+        for (int u = 0; u < 4; ++u) {
+          acc += double(v[u].x) * v[u].x + double(v[u].y) * v[u].y;
+          acc += double(v[u].z) * v[u].z + double(v[u].w) * v[u].w;
+          m = fmaxf(m, fmaxf(fmaxf(fabsf(v[u].x), fabsf(v[u].y)),
+                             fmaxf(fabsf(v[u].z), fabsf(v[u].w))));
+        }
+      }
+    } else {
+      for (int t0 = lane; t0 < K; t0 += 128) {  // four loads in flight per lane
+        float2 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          v[u] = (t0 + 32 * u < K) ? __ldg(p + t0 + 32 * u) : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          acc += double(v[u].x) * v[u].x + double(v[u].y) * v[u].y;
+          m = fmaxf(m, fmaxf(fabsf(v[u].x), fabsf(v[u].y)));
+        }
       }
     }
     for (int o = 16; o > 0; o >>= 1) {
       acc += __shfl_xor_sync(0xffffffffu, acc, o);
       m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     }
-    const float g = (m > 0.f && m < 3.0e38f) ? m / (6.f * 448.f) : 1.f;
     if (lane == 0) {
       power[r] = float(acc);
-      rscale[r] = g;
+      rscale[r] = (m > 0.f && m < 3.0e38f) ? m / (6.f * 448.f) : 1.f;
     }
+    if (rfi && acc > 0.0) {
+      const double thr = kRfiThreshold * acc / double(K);
+      uint32_t* f = flags + (r / n) * fwords;
+      for (int t = lane; t < K; t += 32) {
+        const float2 v = __ldg(p + t);
+        if (double(v.x) * v.x + double(v.y) * v.y > thr) atomicOr(f + (t >> 5), 1u << (t & 31));
+      }
+    }
+  }
+}
+
+// Pass 2, one block per channel: the channel's time order and lo extent.
+// Plain mode with F flagged samples: position (number of unflagged samples
+// before t) for an unflagged t, K - F + (number of flagged samples before t)
+// for a flagged one -- a correlation is invariant under a common permutation
+// of time, and the flagged samples (impulsive RFI, which E2M1 with one
+// mantissa bit renders worst) land together in the last stages, which alone
+// carry a lo residual.  src[p] = the source sample of position p (-1:
+// padding); nflag[c] = F; chans[c].pad = number of trailing k-blocks (of
+// 128 samples) with a lo residual (all of them in split mode).
+__global__ void __launch_bounds__(1024) nvfp4_order_kernel(const uint32_t* __restrict__ flags,
+                                                           int32_t* __restrict__ src,
+                                                           int32_t* __restrict__ nflag,
+                                                           ChanDesc* __restrict__ chans, int K,
+                                                           int kp, int fwords, int split) {
+  __shared__ int s_cnt[32];
+  __shared__ int s_total;
+  const int c = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t* f = flags + int64_t(c) * fwords;
+  int cnt = 0;
+  if (!split)
+    for (int x = threadIdx.x; x < fwords; x += blockDim.x) cnt += __popc(f[x]);
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if (lane == 0) s_cnt[warp] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int tot = 0;
+    for (int x = 0; x < nwarps; ++x) tot += s_cnt[x];
+    s_total = tot;
+  }
+  __syncthreads();
+  const int F = s_total;
+  const int kblocks = kp / 128;
+  if (threadIdx.x == 0) {
+    nflag[c] = F;
+    chans[c].pad = split ? kblocks : (F == 0 ? 0 : kblocks - (K - F) / 128);
+  }
+  int32_t* sc = src + int64_t(c) * kp;
+  for (int p = K + threadIdx.x; p < kp; p += blockDim.x) sc[p] = -1;
+  if (F == 0) {
+    for (int t = threadIdx.x; t < K; t += blockDim.x) sc[t] = t;
+    return;
+  }
+  int base = 0;  // flagged samples before this chunk
+  for (int t0 = 0; t0 < K; t0 += blockDim.x) {
+    const int t = t0 + threadIdx.x;
+    const bool fl = t < K && ((f[t >> 5] >> (t & 31)) & 1u);
+    const uint32_t bal = __ballot_sync(0xffffffffu, fl);
+    __syncthreads();  // s_cnt of the previous chunk consumed
+    if (lane == 0) s_cnt[warp] = __popc(bal);
+    __syncthreads();
+    int before = base + __popc(bal & ((1u << lane) - 1u));
+    int chunk = 0;
+    for (int x = 0; x < nwarps; ++x) {
+      if (x < warp) before += s_cnt[x];
+      chunk += s_cnt[x];
+    }
+    if (t < K) sc[fl ? (K - F + before) : (t - before)] = t;
+    base += chunk;
+  }
+}
+
+// Pass 3, one warp per input row: the E2M1 operands and UE4M3 scale atoms in
+// the channel's time order (lane l: blocks l, l + 32, ...), with the lo
+// residual in the blocks of the trailing chans[c].pad k-blocks.
+__global__ void __launch_bounds__(256, 4) nvfp4_quant_kernel(
+    const float2* __restrict__ a, const int32_t* __restrict__ src,
+    const int32_t* __restrict__ nflag, const ChanDesc* __restrict__ chans,
+    const float* __restrict__ rscale, uint8_t* __restrict__ z, uint8_t* __restrict__ sfa,
+    uint8_t* __restrict__ sfb, int64_t rows, int K, int kp, int pitch, SfGeom sg) {
+  const int lane = threadIdx.x & 31;
+  const int blocks_per_row = pitch / 8;  // 8 bytes of E2M1 per block
+  const bool vec = (K & 1) == 0 && (reinterpret_cast<uintptr_t>(a) & 15) == 0;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < rows;
+       r += (int64_t(gridDim.x) * blockDim.x) >> 5) {
+    const float2* p = a + r * K;
+    const float g = __ldg(rscale + r);
     const int c = int(r / sg.n), w = int(r - int64_t(c) * sg.n);
+    const bool permuted = __ldg(nflag + c) > 0;
+    const int lo_from = (kp / 128 - chans[c].pad) * 16;  // first block with a residual
+    const int32_t* sc = src + int64_t(c) * kp;
     for (int b = lane; b < blocks_per_row; b += 32) {
       const int t0 = 8 * b;
       float x[16];
-      if (vec && t0 + 8 <= K) {
+      if (!permuted && vec && t0 + 8 <= K) {
         const float4* p4 = reinterpret_cast<const float4*>(p + t0);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -210,11 +353,12 @@ __global__ void __launch_bounds__(256) nvfp4_prepare_kernel(
       } else {
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          const float2 v = (t0 + q < K) ? __ldg(p + t0 + q) : make_float2(0.f, 0.f);
+          const int t = permuted ? (t0 + q < kp ? __ldg(sc + t0 + q) : -1) : (t0 + q < K ? t0 + q : -1);
+          const float2 v = t >= 0 ? __ldg(p + t) : make_float2(0.f, 0.f);
           x[2 * q] = v.x, x[2 * q + 1] = v.y;
         }
       }
-      nvfp4_block(x, g, r, c, w, b, z, sfa, sfb, pitch, sg, split);
+      nvfp4_block(x, g, r, c, w, b, z, sfa, sfb, pitch, sg, b >= lo_from);
     }
   }
 }
@@ -237,11 +381,29 @@ struct Fp4Args {
   const uint8_t* sfa;      // scale atoms of the x rows (A)
   const uint8_t* sfb;      // scale atoms of the x/y rows (B)
   int gA, gB, nks;         // SfGeom: groups per channel, k-steps per row
-  // K segments (hi + lo split: hi.hi, hi.lo, lo.hi; at most 3): segment s pairs
-  // A k-blocks seg_a[s] + kk with B k-blocks seg_b[s] + kk; nseg = 1: plain
-  int nseg;
-  int seg_a[4], seg_b[4];
+  // k-blocks from a row's hi half to its lo half (the lo residual of the
+  // channel's trailing ChanDesc::pad k-blocks; see fp4_segment)
+  int lo_off;
 };
+
+// k-block kb of a channel's K loop -> (A k-block, B k-block): first the
+// kbl hi x hi k-blocks, then `lo` k-blocks of hi x lo (B's lo half, L k-blocks
+// into the row) and `lo` of lo x hi, both over the channel's last `lo`
+// k-blocks (ChanDesc::pad, written by nvfp4_order_kernel; lo x lo is left out).
+__device__ __forceinline__ void fp4_segment(int kb, int kbl, int lo, int L, int& ka, int& kbb) {
+  if (kb < kbl) {
+    ka = kbb = kb;
+    return;
+  }
+  const int m = kb - kbl, base = kbl - lo;
+  if (m < lo) {
+    ka = base + m;
+    kbb = L + base + m;
+  } else {
+    ka = L + base + (m - lo);
+    kbb = base + (m - lo);
+  }
+}
 
 // Epilogue of one 32-column accumulator chunk: rows i0..i0+15 (columns 2m,
 // 2m+1 = Re, Im of row i0+m) of lane j's column.  Element (i, j <= i < n)
@@ -441,18 +603,14 @@ __global__ void __launch_bounds__(k4Threads, 1)
         const int32_t rowB = int32_t(2 * (cd.row0 + int64_t(td.ti) * k4I));  // all rows
         const uint8_t* sfA = args.sfa + (int64_t(td.ch) * args.gA + td.tj) * args.nks * 512;
         const uint8_t* sfB = args.sfb + (int64_t(td.ch) * args.gB + td.ti) * args.nks * 512;
-        for (int kb = 0; kb < cd.kblocks * args.nseg; ++kb) {
+        for (int kb = 0; kb < cd.kblocks + 2 * cd.pad; ++kb) {
           if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
             atomicOr(args.status, kStatusTimeoutProducer);
             ok = false;
             break;
           }
-          const int seg = kb / cd.kblocks, kk = kb - seg * cd.kblocks;
-          // selects, not an indexed load: a dynamic index into the kernel
-          // parameters would copy them to local memory
-          const int sa = seg == 0 ? args.seg_a[0] : (seg == 1 ? args.seg_a[1] : args.seg_a[2]);
-          const int sb = seg == 0 ? args.seg_b[0] : (seg == 1 ? args.seg_b[1] : args.seg_b[2]);
-          const int ka = sa + kk, kbb = sb + kk;
+          int ka, kbb;
+          fp4_segment(kb, cd.kblocks, cd.pad, args.lo_off, ka, kbb);
           mbar_arrive_expect_tx(full_bar(stage), k4StageBytes);
           tma_load_2d(a_addr(stage), &tmA, ka * k4KB, rowA, full_bar(stage));
           tma_load_2d(b_addr(stage), &tmB, kbb * k4KB, rowB, full_bar(stage));
@@ -493,7 +651,7 @@ __global__ void __launch_bounds__(k4Threads, 1)
         }
         tc_fence_after();
         const uint32_t d = tmem_base + uint32_t(acc * k4AccCols);
-        for (int kb = 0; kb < cd.kblocks * args.nseg; ++kb) {
+        for (int kb = 0; kb < cd.kblocks + 2 * cd.pad; ++kb) {
           if (!mbar_wait(full_bar(stage), phase, abort_flag)) {
             atomicOr(args.status, kStatusTimeoutMma);
             ok = false;
@@ -643,18 +801,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(k4pThreads, 1)
         const int64_t ga = int64_t(td.ch) * args.gA + 2 * int64_t(td.tj) + rank;
         const int64_t gb = int64_t(td.ch) * args.gB + td.ti;
         bool ok = true;
-        for (int kb = 0; kb < cd.kblocks * args.nseg; ++kb) {
+        for (int kb = 0; kb < cd.kblocks + 2 * cd.pad; ++kb) {
           if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
             atomicOr(args.status, kStatusTimeoutProducer);
             ok = false;
             break;
           }
-          const int seg = kb / cd.kblocks, kk = kb - seg * cd.kblocks;
-          // selects, not an indexed load: a dynamic index into the kernel
-          // parameters would copy them to local memory
-          const int sa = seg == 0 ? args.seg_a[0] : (seg == 1 ? args.seg_a[1] : args.seg_a[2]);
-          const int sb = seg == 0 ? args.seg_b[0] : (seg == 1 ? args.seg_b[1] : args.seg_b[2]);
-          const int ka = sa + kk, kbb = sb + kk;
+          int ka, kbb;
+          fp4_segment(kb, cd.kblocks, cd.pad, args.lo_off, ka, kbb);
           if (leader) mbar_arrive_expect_tx(full_bar(stage), 2 * k4pStageBytes);
           const uint32_t fb = map_shared(full_bar(stage), 0);
           tma_load_2d_pair(a_addr(stage), &tmA, ka * k4KB, rowA, fb);
@@ -687,7 +841,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(k4pThreads, 1)
         }
         tc_fence_after();
         const uint32_t d = tmem_base + uint32_t(acc * k4pAccCols);
-        for (int kb = 0; kb < cd.kblocks * args.nseg; ++kb) {
+        for (int kb = 0; kb < cd.kblocks + 2 * cd.pad; ++kb) {
           if (!mbar_wait(full_bar(stage), phase, abort_flag)) {
             atomicOr(args.status, kStatusTimeoutMma);
             ok = false;
@@ -750,20 +904,25 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(k4pThreads, 1)
 
 }  // namespace
 
-// Workspace: E2M1 operand rows (2 per input; twice as long when split), then
-// their scale bytes, then the row powers.
 namespace {
-// Workspace carve-up of one NVFP4 call (every part 1 KB aligned).
+// Workspace carve-up of one NVFP4 call (every part 1 KB aligned): E2M1
+// operand rows (2 per input, each a hi half and a lo half of `pitch` bytes),
+// the scale atoms of the A and B views, the row powers and row scales, the
+// channels' RFI bitmaps, flagged counts and time orders.
 struct Fp4Ws {
   int64_t pitch, rpitch;   // E2M1 bytes per operand row: one half, whole row
+  int64_t kp;              // samples per row, padded to the 128-sample stage
+  int fwords;              // 32-bit words of one channel's RFI bitmap
   SfGeom sg;
-  int64_t z_bytes, sfa_bytes, sfb_bytes, total;
+  int64_t z_bytes, sfa_bytes, sfb_bytes, pw_bytes, flag_bytes, nflag_bytes, src_bytes, total;
 };
-Fp4Ws fp4_ws(int n, int batch, int K, int split, int pair) {
+Fp4Ws fp4_ws(int n, int batch, int K, int pair) {
   Fp4Ws w;
   const int64_t rows = int64_t(n) * batch;
   w.pitch = (2 * int64_t(K) + 255) / 256 * 128;
-  w.rpitch = split ? 2 * w.pitch : w.pitch;
+  w.rpitch = 2 * w.pitch;
+  w.kp = w.pitch;  // samples per padded row: two E2M1 values a byte, two a sample
+  w.fwords = int((K + 31) / 32);
   const int nks = int(w.rpitch / 32);
   if (pair)  // A: both 128-row halves of every 256-input tile; B: 224-row groups
     w.sg = SfGeom{n, 2 * ((n + k4pJ - 1) / k4pJ), (2 * n + k4pN - 1) / k4pN, nks, k4pN, 2};
@@ -773,7 +932,12 @@ Fp4Ws fp4_ws(int n, int batch, int K, int split, int pair) {
   w.z_bytes = up(2 * rows * w.rpitch);
   w.sfa_bytes = up(int64_t(batch) * w.sg.gA * w.sg.nks * 512);
   w.sfb_bytes = up(int64_t(batch) * w.sg.gB * w.sg.nks * w.sg.nsub * 512);
-  w.total = w.z_bytes + w.sfa_bytes + w.sfb_bytes + 2 * up(4 * rows);
+  w.pw_bytes = up(4 * rows);
+  w.flag_bytes = up(int64_t(batch) * w.fwords * 4);
+  w.nflag_bytes = up(int64_t(batch) * 4);
+  w.src_bytes = up(int64_t(batch) * w.kp * 4);
+  w.total = w.z_bytes + w.sfa_bytes + w.sfb_bytes + 2 * w.pw_bytes + w.flag_bytes +
+            w.nflag_bytes + w.src_bytes;
   return w;
 }
 }  // namespace
@@ -781,7 +945,8 @@ Fp4Ws fp4_ws(int n, int batch, int K, int split, int pair) {
 // Workspace: E2M1 operand rows (2 per input; twice as long when split), the
 // scale atoms of the A and B views, the row powers and the row scales.
 size_t nvfp4_workspace_bytes(int n, int batch, int K, int split, int pair) {
-  return size_t(fp4_ws(n, batch, K, split, pair).total);
+  (void)split;  // one layout for both modes: every row has room for its lo half
+  return size_t(fp4_ws(n, batch, K, pair).total);
 }
 
 // Pairs of the NVFP4 pair kernel that can be resident at once on the current
@@ -823,34 +988,50 @@ int nvfp4_kblocks(int K) { return int((2 * int64_t(K) + 255) / 256); }
 cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, uint8_t* ws,
                          const TileDesc* tiles, const ChanDesc* chans, int num_tiles, void* C,
                          float alpha, float beta, uint32_t* status, int sm_count, void* encode_fn,
-                         cudaStream_t s, int split, int pair) {
+                         cudaStream_t s, int split, int pair, int phases) {
   auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(encode_fn);
   if (!encode) return cudaErrorInvalidValue;
   if (pair && nvfp4_pair_limit() < 1) return cudaErrorInvalidConfiguration;
-  const Fp4Ws w = fp4_ws(n, batch, K, split, pair);
+  const Fp4Ws w = fp4_ws(n, batch, K, pair);
   const int64_t pitch = w.pitch, rpitch = w.rpitch;  // one half (hi or lo), whole row
   uint8_t* z = ws;
   uint8_t* sfa = ws + w.z_bytes;
   uint8_t* sfb = sfa + w.sfa_bytes;
   float* power = reinterpret_cast<float*>(sfb + w.sfb_bytes);
-  float* rscale = reinterpret_cast<float*>(sfb + w.sfb_bytes + (4 * rows + 1023) / 1024 * 1024);
+  float* rscale = reinterpret_cast<float*>(sfb + w.sfb_bytes + w.pw_bytes);
+  uint32_t* flags = reinterpret_cast<uint32_t*>(sfb + w.sfb_bytes + 2 * w.pw_bytes);
+  int32_t* nflag = reinterpret_cast<int32_t*>(reinterpret_cast<uint8_t*>(flags) + w.flag_bytes);
+  int32_t* src = reinterpret_cast<int32_t*>(reinterpret_cast<uint8_t*>(nflag) + w.nflag_bytes);
   // rows of a partial group get no scales from the quantiser: zero them
   // (their products land only in outputs the epilogue skips)
   cudaError_t e;
-  if (n % (pair ? k4pJ : 128) != 0 || (2 * n) % w.sg.gbrows != 0) {
-    e = cudaMemsetAsync(sfa, 0, size_t(w.sfa_bytes + w.sfb_bytes), s);
+  if (phases & 1) {  // the quantiser passes
+    if (n % (pair ? k4pJ : 128) != 0 || (2 * n) % w.sg.gbrows != 0) {
+      e = cudaMemsetAsync(sfa, 0, size_t(w.sfa_bytes + w.sfb_bytes), s);
+      if (e != cudaSuccess) return e;
+    }
+    const int rfi = split ? 0 : 1;
+    if (rfi) {
+      e = cudaMemsetAsync(flags, 0, size_t(w.flag_bytes), s);
+      if (e != cudaSuccess) return e;
+    }
+    int64_t blocks = (rows + 7) / 8;  // one warp per row
+    if (blocks > int64_t(sm_count) * 16) blocks = int64_t(sm_count) * 16;
+    // row scales, row powers and (plain mode) the channels' RFI bitmaps
+    nvfp4_stats_kernel<<<unsigned(blocks), 256, 0, s>>>(static_cast<const float2*>(A), power,
+                                                        rscale, flags, rows, K, n, w.fwords, rfi);
+    // time order and lo extent of every channel (written into the plan's table)
+    nvfp4_order_kernel<<<unsigned(batch), 1024, 0, s>>>(flags, src, nflag,
+                                                        const_cast<ChanDesc*>(chans), K,
+                                                        int(w.kp), w.fwords, split);
+    // E2M1 operands and UE4M3 scale atoms
+    nvfp4_quant_kernel<<<unsigned(blocks), 256, 0, s>>>(static_cast<const float2*>(A), src, nflag,
+                                                        chans, rscale, z, sfa, sfb, rows, K,
+                                                        int(w.kp), int(pitch), w.sg);
+    e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  // row scales, row powers and the E2M1 operands: one warp per row
-  {
-    int64_t blocks = (rows + 7) / 8;
-    if (blocks > int64_t(sm_count) * 16) blocks = int64_t(sm_count) * 16;
-    nvfp4_prepare_kernel<<<unsigned(blocks), 256, 0, s>>>(static_cast<const float2*>(A), z, sfa,
-                                                           sfb, power, rscale, rows, K,
-                                                           int(pitch), w.sg, split);
-  }
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  if (!(phases & 2)) return cudaSuccess;
 
   CUtensorMap tmA, tmB, tmSa, tmSb;
   const cuuint32_t estr[2] = {1, 1};
@@ -875,16 +1056,7 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
     return cudaErrorInvalidValue;
   Fp4Args args{tiles, chans, num_tiles, C, alpha, beta, rscale, status, power,
                sfa, sfb, w.sg.gA, w.sg.gB, w.sg.nks};
-  args.nseg = 1;
-  if (split) {
-    // hi.hi + hi.lo + lo.hi, lo at L k-blocks into each row; lo.lo (the square
-    // of the residual, ~1/64 of the signal) is left out as in split FP8, and the
-    // autocorrelations come from the exact row powers either way
-    const int L = int(pitch / k4KB);
-    const int sa[3] = {0, 0, L}, sb[3] = {0, L, 0};
-    args.nseg = 3;
-    for (int q = 0; q < 3; ++q) args.seg_a[q] = sa[q], args.seg_b[q] = sb[q];
-  }
+  args.lo_off = int(pitch / k4KB);  // hi . lo + lo . hi over each channel's lo k-blocks
   if (pair) {
     const int limit = nvfp4_pair_limit();
     const int pairs = num_tiles < limit ? num_tiles : limit;

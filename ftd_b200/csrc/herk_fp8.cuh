@@ -197,6 +197,8 @@ cudaError_t launch_channel_amax(const void* a, int64_t per_chan, int batch, uint
                                 int sm_count, cudaStream_t s);
 // NVFP4 correlator for float complex input (herk_fp4.cu).  Tiles: ti over 64
 // row inputs, tj over 128 column inputs; kblocks = nvfp4_kblocks(K).
+// phases: 1 = the quantiser passes (they also write each channel's lo extent
+// into chans[c].pad), 2 = the correlator, 3 = both.
 // pair: the CTA-pair kernel (tiles from nvfp4_pair_tiles: tj over 256 column
 // inputs, ti over 112 row inputs), when nvfp4_pair_limit() >= 1.
 size_t nvfp4_workspace_bytes(int n, int batch, int K, int split = 0, int pair = 0);
@@ -206,7 +208,7 @@ void nvfp4_pair_tiles(int n, int ch, std::vector<TileDesc>& out);
 cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, uint8_t* ws,
                          const TileDesc* tiles, const ChanDesc* chans, int num_tiles, void* C,
                          float alpha, float beta, uint32_t* status, int sm_count, void* encode_fn,
-                         cudaStream_t s, int split = 0, int pair = 0);
+                         cudaStream_t s, int split = 0, int pair = 0, int phases = 3);
 // Float complex [rows][K] -> scaled E4M3 planes of pitch zpitch (precision.cu).
 cudaError_t launch_float_to_planes(const void* a, uint8_t* z, int64_t rows, int K, int Kp,
                                    int zpitch, int n, int batch, int split, float* qscale,

@@ -13,7 +13,10 @@ namespace ftdx {
 namespace {
 
 constexpr int kProbeTile = 128 * 128;              // bytes: 128 rows x 128 B (SW128)
-constexpr size_t kProbeSmem = 1024 + 2 * kProbeTile + 4096 + 256;
+// more shared memory than two CTAs can share, so one CTA (and one 512-column
+// TMEM allocation) per SM; the tiles use the first 37 KB
+constexpr size_t kProbeSmem = 120 * 1024;
+static_assert(1024 + 2 * kProbeTile + 4096 + 256 <= kProbeSmem, "probe layout");
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(128, 1)
     peak_probe_kernel(int kind, int iters, uint32_t* status) {

@@ -457,13 +457,28 @@ def xengine(payload: np.ndarray, n_ant: int, K: int, batch: int, mat_format: int
 # A restatement of the library's NVFP4 quantisation (its own format; the
 # reference has none) in IEEE float32 steps, so that the GPU result can be
 # checked against the same quantised operands to FP32 accumulation rounding.
-# Per input row an FP32 scale g = amax_row / (6 * 448) (1 for an empty row);
-# per block of 16 values (8 complex samples, Re/Im interleaved) a UE4M3 scale
-# b = the smallest E4M3 value >= amax_blk / (6 g) (at most 448); elements
-# E2M1(v * (1 / (g b))), round to nearest with ties to the even code,
-# saturating at 6.  Split mode: the residual x - code * (g b) (one rounding,
-# as a fused multiply-add) quantised again with its own block scale.
+#  * Per input row: an FP32 scale g = amax_row / (6 * 448) (1 for an empty
+#    row) and the FP64 power P = sum_t |v_t|^2.
+#  * Block scale of 16 values (8 complex samples, Re/Im interleaved): the
+#    candidate UE4M3 codes c0 = the smallest E4M3 value >= amax_blk / (6 g)
+#    (at most 448) and c0 - 1 (a code >= 1 only); for each, gb = g b and
+#    inv = 1 / gb in float32, codes E2M1(x * inv) (round to nearest, ties to
+#    the even code, saturating at 6), d = fma(-code, gb, x) and
+#    err = sum of fl(d * d) in float32 in element order; c0 - 1 is kept only
+#    on a strictly smaller err.
+#  * A lo residual r = fma(-code, gb, x) is quantised the same way with its
+#    own block scale (same g) where the mode carries one:
+#      split: every stage (128 samples);
+#      plain: a channel's time samples t with |v_t|^2 > 25 P / K in any row
+#      (FP64 comparison) are flagged; the channel's time axis is permuted to
+#      the unflagged samples in order followed by the flagged ones in order
+#      (a correlation is invariant under a common permutation of time), and
+#      the stages from floor((K - F) / 128) on carry a lo residual (F flagged
+#      samples; none when F = 0).
+#  * The product is g_i g_j sum (hi_i + lo_i)(hi_j + lo_j)^* without lo lo.
 E2M1_GRID = np.array([0.0, 0.5, 1.0, 1.5, 2.0, 3.0, 4.0, 6.0])
+NVFP4_STAGE = 128          # samples per correlator stage (K granularity of the lo residual)
+NVFP4_RFI_THRESHOLD = 25.0  # |v_t|^2 > 25 x the row's mean power flags sample t
 
 
 def _e4m3_positive() -> np.ndarray:
@@ -476,15 +491,19 @@ def _e4m3_positive() -> np.ndarray:
     return np.array(sorted(set(vals)))
 
 
-_E4M3 = _e4m3_positive()
+_E4M3 = _e4m3_positive()  # index = E4M3 code of each non-negative value
 
 
 def ue4m3_ceil(v: np.ndarray) -> np.ndarray:
     """Smallest E4M3 value >= v (float32 in), 448 at most, 0 for v <= 0."""
+    return _E4M3[ue4m3_ceil_code(v)].astype(np.float32)
+
+
+def ue4m3_ceil_code(v: np.ndarray) -> np.ndarray:
+    """Code of the smallest E4M3 value >= v, 0x7E (448) at most, 0 for v <= 0."""
     v = np.asarray(v, dtype=np.float64)
-    idx = np.searchsorted(_E4M3, v, side="left")
-    out = _E4M3[np.minimum(idx, len(_E4M3) - 1)]
-    return np.where(v > 0, out, 0.0).astype(np.float32)
+    idx = np.minimum(np.searchsorted(_E4M3, v, side="left"), len(_E4M3) - 1)
+    return np.where(v > 0, idx, 0)
 
 
 def e2m1_rne(x: np.ndarray) -> np.ndarray:
@@ -501,25 +520,82 @@ def e2m1_rne(x: np.ndarray) -> np.ndarray:
     return np.copysign(q, x).astype(np.float32)
 
 
+def _fma32(a, b, c):
+    """float32 fma(a, b, c): exact in float64 for the operands used here
+    (a an E2M1 value, b and c float32 of comparable magnitude or a = 0), then
+    rounded once."""
+    return (np.asarray(a, np.float64) * np.asarray(b, np.float64)
+            + np.asarray(c, np.float64)).astype(np.float32)
+
+
 def _nvfp4_pass(x: np.ndarray, g: np.ndarray):
     """Quantise float32 values x[..., nblk, 16] under row scales g[..., 1, 1]:
-    (dequantised values / g, block scales)."""
+    (codes x block scale as float64, codes float32, g b float32), with the
+    block scale picked between two candidates by squared error."""
     f32 = np.float32
+    x = x.astype(f32)
     amax = np.abs(x).max(axis=-1, keepdims=True).astype(f32)
-    b = ue4m3_ceil((amax / (f32(6.0) * g)).astype(f32))
-    with np.errstate(divide="ignore"):
-        inv = np.where(b > 0, f32(1.0) / (g * b).astype(f32), f32(0.0)).astype(f32)
-    codes = e2m1_rne((x * inv).astype(f32))
-    return codes.astype(np.float64) * b.astype(np.float64), b
+    c0 = ue4m3_ceil_code((amax / (f32(6.0) * g)).astype(f32))
+    best_q = best_codes = best_gb = best_err = None
+    for d in (0, 1):
+        c = c0 - d
+        valid = (c >= 1) if d > 0 else np.ones_like(c, dtype=bool)
+        b = _E4M3[np.maximum(c, 0)].astype(f32)
+        gb = (g * b).astype(f32)
+        with np.errstate(divide="ignore"):
+            inv = np.where(b > 0, f32(1.0) / gb, f32(0.0)).astype(f32)
+        codes = e2m1_rne((x * inv).astype(f32))
+        dd = _fma32(-codes, gb, x)
+        err = np.zeros(dd.shape[:-1] + (1,), dtype=f32)
+        for k in range(16):
+            err = (err + (dd[..., k:k + 1] * dd[..., k:k + 1]).astype(f32)).astype(f32)
+        q = codes.astype(np.float64) * b.astype(np.float64)
+        if best_q is None:
+            best_q, best_codes, best_gb, best_err = q, codes, np.broadcast_to(gb, codes.shape), err
+            continue
+        take = valid & (err < best_err)
+        best_q = np.where(take, q, best_q)
+        best_codes = np.where(take, codes, best_codes)
+        best_gb = np.where(take, gb, best_gb)
+        best_err = np.where(take, err, best_err)
+    return best_q, best_codes, best_gb.astype(f32)
+
+
+def nvfp4_time_order(v: np.ndarray):
+    """Plain-mode time order of each channel of complex64 voltages
+    [batch, N, K]: (order [batch, K] source sample of each position,
+    flagged count [batch])."""
+    B, N, K = v.shape
+    e = v.real.astype(np.float64) ** 2 + v.imag.astype(np.float64) ** 2
+    p = e.sum(axis=-1, keepdims=True)
+    flag = (e > NVFP4_RFI_THRESHOLD * p / K).any(axis=1)
+    order = np.empty((B, K), dtype=np.int64)
+    for b in range(B):
+        order[b] = np.concatenate([np.nonzero(~flag[b])[0], np.nonzero(flag[b])[0]])
+    return order, flag.sum(axis=1)
+
+
+def nvfp4_lo_stages(K: int, flagged: int, split: bool) -> int:
+    """Number of trailing correlator stages that carry a lo residual."""
+    stages = (K + NVFP4_STAGE - 1) // NVFP4_STAGE
+    if split:
+        return stages
+    return 0 if flagged == 0 else stages - (K - flagged) // NVFP4_STAGE
 
 
 def nvfp4_quantize(v: np.ndarray, split: bool = False):
-    """Complex64 voltages [batch, N, K] -> (hi, lo or None, g): the dequantised
-    operands as complex128 without the row scale (the MMA operands code x
-    block scale), and the float32 row scales g [batch, N]."""
+    """Complex64 voltages [batch, N, K] -> (hi, lo, g): the dequantised
+    operands (code x block scale, without the row scale) as complex128 in the
+    quantiser's time order (plain mode permutes flagged samples to the end),
+    lo zero where no residual is carried, and the float32 row scales g."""
     f32 = np.float32
     B, N, K = v.shape
-    kp = (K + 7) // 8 * 8
+    if not split:
+        order, nflag = nvfp4_time_order(v)
+        v = np.take_along_axis(v, order[:, None, :], axis=-1)
+    else:
+        nflag = np.zeros(B, dtype=np.int64)
+    kp = (K + NVFP4_STAGE - 1) // NVFP4_STAGE * NVFP4_STAGE
     x = np.zeros((B, N, kp, 2), dtype=f32)
     x[:, :, :K, 0] = v.real
     x[:, :, :K, 1] = v.imag
@@ -527,28 +603,27 @@ def nvfp4_quantize(v: np.ndarray, split: bool = False):
     g = np.where((m > 0) & (m < f32(3.0e38)), m / f32(6.0 * 448.0), f32(1.0)).astype(f32)
     xb = x.reshape(B, N, kp // 8, 16)
     gb = g[:, :, None, None]
-    hi, b = _nvfp4_pass(xb, gb)
-    lo = None
-    if split:
-        step = (gb.astype(f32) * b.astype(f32)).astype(f32).astype(np.float64)
-        codes = hi / np.where(b > 0, b, 1.0)
-        resid = (xb.astype(np.float64) - codes * step).astype(f32)
-        lo, _ = _nvfp4_pass(resid, gb)
+    hi, codes, step = _nvfp4_pass(xb, gb)
+    resid = _fma32(-codes, step, xb)
+    lo, _, _ = _nvfp4_pass(resid, gb)
+    for b in range(B):  # keep the residual only in the stages that carry it
+        first = kp // 8 - nvfp4_lo_stages(K, int(nflag[b]), split) * (NVFP4_STAGE // 8)
+        lo[b, :, :first] = 0.0
+
     def cplx(a):
         a = a.reshape(B, N, kp, 2)[:, :, :K]
         return a[..., 0] + 1j * a[..., 1]
-    return cplx(hi), (cplx(lo) if split else None), g
+    return cplx(hi), cplx(lo), g
 
 
 def herk_nvfp4(v: np.ndarray, split: bool = False) -> np.ndarray:
     """Packed lower triangles [batch, P, 2] (float64) of the NVFP4 product:
-    g_i g_j sum_t q_i q_j^* over the quantised operands (split: hi hi + hi lo
-    + lo hi), autocorrelations the exact sum |v|^2 rounded to float32."""
+    g_i g_j sum_t (hi_i hi_j^* + lo_i hi_j^* + hi_i lo_j^*) over the quantised
+    operands, autocorrelations the exact sum |v|^2 rounded to float32."""
     B, N, K = v.shape
     hi, lo, g = nvfp4_quantize(v, split)
     R = np.einsum("bik,bjk->bij", hi, hi.conj())
-    if split:
-        R += np.einsum("bik,bjk->bij", lo, hi.conj()) + np.einsum("bik,bjk->bij", hi, lo.conj())
+    R += np.einsum("bik,bjk->bij", lo, hi.conj()) + np.einsum("bik,bjk->bij", hi, lo.conj())
     gg = g.astype(np.float64)
     R *= gg[:, :, None] * gg[:, None, :]
     pw = (v.real.astype(np.float64) ** 2 + v.imag.astype(np.float64) ** 2).sum(axis=-1)

@@ -258,6 +258,56 @@ def test_nvfp4_restatement_rounding_rules():
                           np.array([0, 1, 1.125, 448, 448, 2.0 ** -9], np.float32))
 
 
+def test_nvfp4_block_scale_by_squared_error():
+    # the block scale is the better of the rounded-up UE4M3 scale (no element
+    # saturates) and the next smaller code (the largest may saturate at 6, the
+    # rest land on finer steps): never worse than the rounded-up scale, and
+    # strictly better for a good share of Gaussian blocks
+    f32 = np.float32
+    rng = np.random.default_rng(3)
+    xs = (rng.normal(size=(2000, 16)) * np.exp(rng.normal(size=(2000, 1)))).astype(f32)[None]
+    q, codes, gb = oracle._nvfp4_pass(xs, np.ones((1, 1, 1), f32))
+    amax = np.abs(xs).max(-1, keepdims=True)
+    b0 = oracle.ue4m3_ceil((amax / f32(6)).astype(f32)).astype(np.float64)
+    q0 = oracle.e2m1_rne((xs * (f32(1) / b0.astype(f32))).astype(f32)) * b0
+    e, e0 = ((q - xs) ** 2).sum(-1), ((q0 - xs) ** 2).sum(-1)
+    assert np.all(e <= e0 * (1 + 1e-6))
+    smaller = gb[..., 0] < b0[..., 0].astype(f32)
+    assert 0.1 < smaller.mean() < 0.9 and np.all(e[smaller] < e0[smaller])
+    assert np.abs(codes[smaller]).max() == 6.0  # saturated elements occur
+
+
+def test_nvfp4_time_order_moves_bursts_last():
+    # flagged samples (|v|^2 > 25 x the row's mean power in any row) go to the
+    # end of the channel's time axis in order; the lo residual covers the
+    # stages from floor((K - F) / 128) on
+    B, N, K = 2, 40, 300
+    v = oracle.workload4_voltages(12, B, N, K, rfi_time_frac=0.02)  # 6 burst samples
+    order, nflag = oracle.nvfp4_time_order(v)
+    for b in range(B):
+        assert sorted(order[b]) == list(range(K))
+        F = int(nflag[b])
+        assert F == 6
+        burst = set(np.nonzero((np.abs(v[b]) > 10 * np.abs(v[b]).std()).any(0))[0])
+        assert set(order[b][K - F:]) == burst
+        assert np.all(np.diff(order[b][:K - F]) > 0) and np.all(np.diff(order[b][K - F:]) > 0)
+        assert oracle.nvfp4_lo_stages(K, F, False) == 3 - (K - F) // 128 == 1
+    assert oracle.nvfp4_lo_stages(K, 0, False) == 0 and oracle.nvfp4_lo_stages(K, 0, True) == 3
+    g = oracle.workload4_voltages(13, 1, 64, 512, rfi_time_frac=0.0)
+    assert oracle.nvfp4_time_order(g)[1][0] == 0  # Gaussian voltages: nothing flagged
+
+
+def test_nvfp4_restated_accuracy_on_the_burst_workload():
+    # the quantiser alone (FP64 products of its operands) on the precision
+    # configuration's distribution: plain NVFP4 within 2e-2, split within 5e-3
+    B, N, K = 2, 256, 1024
+    v = oracle.workload4_voltages(21, B, N, K)
+    ref = oracle.herk_c128(v.astype(np.complex128), N, K, B)
+    plain = oracle.correlation_errors(oracle.herk_nvfp4(v), ref, N)
+    split = oracle.correlation_errors(oracle.herk_nvfp4(v, split=True), ref, N)
+    assert plain["max_offdiag_norm"] < 2e-2 and split["max_offdiag_norm"] < 5e-3
+
+
 def test_e4m3_restatement_rounding_rules():
     # ties to the even code, saturation at 448, subnormals (spacing 2^-9)
     x = np.array([1.0625, 1.1875, 448.0, 480.0, 1000.0, 2.0 ** -10, 3 * 2.0 ** -10, -1.0625, 0.0],

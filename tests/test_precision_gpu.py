@@ -124,15 +124,16 @@ def test_nvfp4_exactly_representable_input_is_exact(store_mode):
 
 
 def test_nvfp4_error(workload):
+    # E2M1 with block-16 scales chosen by squared error: ~15% RMS quantisation
+    # noise per sample, ~0.15 sqrt(2/K) per normalised cross-correlation.  The
+    # time samples carrying 20-sigma bursts are moved to the last stage and
+    # carry a lo residual there, so the burst pairs no longer set the worst
+    # case (6e-2 without it).  Autocorrelations are exact.
     from ftd_b200._lib import COMPUTE_FP4
     v, ref = workload
     err = oracle.correlation_errors(run_float(v, COMPUTE_FP4), ref, v.shape[1])
     print("nvfp4", err)
-    # E2M1 with block-16 scales: ~17% RMS quantisation noise per sample, i.e.
-    # ~0.17 sqrt(2/K) per normalised cross-correlation; the largest errors are
-    # between inputs that share 20-sigma bursts (the small component of a
-    # burst sample keeps one mantissa bit).  Autocorrelations are exact.
-    assert err["rms_offdiag_norm"] < 1e-2 and err["max_offdiag_norm"] < 8e-2
+    assert err["rms_offdiag_norm"] < 5e-3 and err["max_offdiag_norm"] < 2e-2
     assert err["max_auto_rel"] < 1e-5
 
 
@@ -143,7 +144,71 @@ def test_nvfp4_error_without_rfi():
     ref = oracle.herk_c128(v.astype(np.complex128), N, K, B)
     err = oracle.correlation_errors(run_float(v, COMPUTE_FP4), ref, N)
     print("nvfp4 no-rfi", err)
-    assert err["rms_offdiag_norm"] < 1e-2 and err["max_offdiag_norm"] < 3e-2
+    assert err["rms_offdiag_norm"] < 5e-3 and err["max_offdiag_norm"] < 2e-2
+
+
+def _config4_voltages(seed, B, N, K, dev):
+    """The precision configuration on the device: complex Gaussian voltages
+    [B][N][K][2] float32, per-channel RMS log-uniform in [0.1, 10], and in
+    each channel 1% of the time samples carry 20-sigma bursts (random phase)
+    on 5% of the inputs."""
+    g = torch.Generator(device=dev).manual_seed(seed)
+    rms = torch.exp(torch.empty(B, device=dev).uniform_(float(np.log(0.1)), float(np.log(10.0)),
+                                                        generator=g))
+    V = torch.randn(B, N, K, 2, device=dev, generator=g) * (rms.view(B, 1, 1, 1) / 2 ** 0.5)
+    n_rfi, t_rfi = max(1, N // 20), max(1, K // 100)
+    for b in range(B):
+        ins = torch.randperm(N, device=dev, generator=g)[:n_rfi]
+        ts = torch.randperm(K, device=dev, generator=g)[:t_rfi]
+        ph = torch.rand(n_rfi, t_rfi, device=dev, generator=g) * (2 * np.pi)
+        amp = 20.0 * rms[b]
+        V[b, ins[:, None], ts[None, :]] = torch.stack([amp * torch.cos(ph), amp * torch.sin(ph)], -1)
+    return V
+
+
+def full_channel_errors(V, C):
+    """max and RMS over all channels of |dR_ij| / sqrt(R_ii R_jj), cross- and
+    autocorrelations, against FP64 products computed on the device."""
+    B, N = V.shape[0], V.shape[1]
+    ii, jj = torch.tril_indices(N, N, device=V.device)
+    order = torch.argsort(ii * N + jj)
+    ii, jj = ii[order], jj[order]
+    off = ii != jj
+    mx = mxa = 0.0
+    ss = 0.0
+    cnt = 0
+    for b in range(B):
+        Vb = torch.view_as_complex(V[b].double().contiguous())
+        R = Vb @ Vb.conj().T
+        auto = torch.diagonal(R).real
+        got = torch.view_as_complex(C[b].double().contiguous())
+        ref = R[ii, jj]
+        e = (got - ref).abs() / torch.sqrt(auto[ii] * auto[jj])
+        mx = max(mx, float(e[off].max()))
+        mxa = max(mxa, float(e[~off].max()))
+        ss += float(e[off].pow(2).sum())
+        cnt += int(off.sum())
+        del R, ref, got, e
+    return {"max_cross": mx, "rms_cross": (ss / cnt) ** 0.5, "max_auto": mxa}
+
+
+def test_nvfp4_config4_full_channels():
+    # The precision configuration at full size: 4096 inputs x 64 channels x
+    # K = 1024 with the RFI bursts; every element of every channel against
+    # FP64.  NVFP4 (E2M1, UE4M3 block-16 scales, burst samples permuted into a
+    # last stage that carries a lo residual): max <= 2e-2 over all 5.4e8
+    # normalised cross-correlations; the hi + lo split mode far below it.
+    from ftd_b200._lib import COMPUTE_FP4, COMPUTE_FP4_SPLIT
+    B, N, K = 64, 4096, 1024
+    V = _config4_voltages(2026, B, N, K, DEV)
+    C = torch.empty(B, tri_size(N), 2, device=DEV)
+    with Correlator() as c:
+        for compute, bound in ((COMPUTE_FP4, 2e-2), (COMPUTE_FP4_SPLIT, 1e-2)):
+            c.herk(V, C, N, K, B, input=IN_FP32, compute=compute, output=OUT_FP32, tune=False)
+            assert c.device_status() == 0
+            err = full_channel_errors(V, C)
+            print("config 4 full channels", compute, err)
+            assert err["max_cross"] <= bound and err["max_auto"] < 1e-5
 
 
 @pytest.mark.parametrize("store_mode", [0, 2])
