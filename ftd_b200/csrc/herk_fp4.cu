@@ -209,8 +209,14 @@ __global__ void __launch_bounds__(256) nvfp4_stats_kernel(
   for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < rows;
        r += (int64_t(gridDim.x) * blockDim.x) >> 5) {
     const float2* p = a + r * K;
-    double acc = 0.0;
+    double acc = 0.0, emax = 0.0;  // sum and largest of |v_t|^2 (each exact in FP64 before the sum)
     float m = 0.f;
+    auto take = [&](float x, float y) {
+      const double e = double(x) * x + double(y) * y;
+      acc += e;
+      emax = fmax(emax, e);
+      m = fmaxf(m, fmaxf(fabsf(x), fabsf(y)));
+    };
     if (vec) {
       const float4* p4 = reinterpret_cast<const float4*>(p);
       const int k2 = K >> 1;
@@ -221,10 +227,8 @@ __global__ void __launch_bounds__(256) nvfp4_stats_kernel(
           v[u] = (t0 + 32 * u < k2) ? __ldg(p4 + t0 + 32 * u) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          acc += double(v[u].x) * v[u].x + double(v[u].y) * v[u].y;
-          acc += double(v[u].z) * v[u].z + double(v[u].w) * v[u].w;
-          m = fmaxf(m, fmaxf(fmaxf(fabsf(v[u].x), fabsf(v[u].y)),
-                             fmaxf(fabsf(v[u].z), fabsf(v[u].w))));
+          take(v[u].x, v[u].y);
+          take(v[u].z, v[u].w);
         }
       }
     } else {
@@ -234,26 +238,34 @@ __global__ void __launch_bounds__(256) nvfp4_stats_kernel(
         for (int u = 0; u < 4; ++u)
           v[u] = (t0 + 32 * u < K) ? __ldg(p + t0 + 32 * u) : make_float2(0.f, 0.f);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          acc += double(v[u].x) * v[u].x + double(v[u].y) * v[u].y;
-          m = fmaxf(m, fmaxf(fabsf(v[u].x), fabsf(v[u].y)));
-        }
+        for (int u = 0; u < 4; ++u) take(v[u].x, v[u].y);
       }
     }
     for (int o = 16; o > 0; o >>= 1) {
       acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, o));
       m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     }
     if (lane == 0) {
       power[r] = float(acc);
       rscale[r] = (m > 0.f && m < 3.0e38f) ? m / (6.f * 448.f) : 1.f;
     }
-    if (rfi && acc > 0.0) {
-      const double thr = kRfiThreshold * acc / double(K);
+    const double thr = kRfiThreshold * acc / double(K);
+    // a row none of whose samples exceeds the threshold (every Gaussian row)
+    // sets no flag: the second read is skipped
+    if (rfi && acc > 0.0 && emax > thr) {
       uint32_t* f = flags + (r / n) * fwords;
-      for (int t = lane; t < K; t += 32) {
-        const float2 v = __ldg(p + t);
-        if (double(v.x) * v.x + double(v.y) * v.y > thr) atomicOr(f + (t >> 5), 1u << (t & 31));
+      for (int t0 = lane; t0 < K; t0 += 128) {  // four loads in flight per lane
+        float2 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          v[u] = (t0 + 32 * u < K) ? __ldg(p + t0 + 32 * u) : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int t = t0 + 32 * u;
+          if (t < K && double(v[u].x) * v[u].x + double(v[u].y) * v[u].y > thr)
+            atomicOr(f + (t >> 5), 1u << (t & 31));
+        }
       }
     }
   }
