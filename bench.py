@@ -180,6 +180,54 @@ def run_sustained(torch, step, stream, gpu_index, flops, seconds=2.5, chunk=50):
                                     for k, v in sorted(bins.items())}}
 
 
+def load_reference_direct():
+    """The reference's own direct mma.sync HERK kernel with its INT4 -> FP8
+    cast (baseline/build_direct_ref.sh builds it from the reference's
+    sources into baseline/_ref/), or None when it was not built."""
+    import ctypes
+    path = os.path.join(ROOT, "baseline", "_ref", "libref_direct_herk.so")
+    if not os.path.exists(path):
+        return None
+    L = ctypes.CDLL(path)
+    L.ref_direct_herk_staging_bytes.restype = ctypes.c_size_t
+    L.ref_direct_herk_staging_bytes.argtypes = [ctypes.c_int] * 3
+    L.ref_direct_herk_qc.restype = ctypes.c_int
+    L.ref_direct_herk_qc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    return L
+
+
+def run_reference_direct_leg(torch, dev, qc, C_ours, N, K, B, steps):
+    """The reference's Blackwell direct HERK path on the same GPU and the same
+    resident QC input: its INT4 -> interleaved-FP8 cast + herk_direct_fp8_precast
+    kernel (mma.sync m16n8k32, 32 x 32 antenna tiles, grid = lower-triangle
+    blocks x channels), FP32 packed lower triangles.  Timed with CUDA events;
+    its triangles compared with the library's (both exact for QC input)."""
+    L = load_reference_direct()
+    if L is None:
+        return None
+    import ctypes
+    from ftd_b200 import tri_size
+    stream = torch.cuda.current_stream(dev)
+    fp8 = torch.empty(int(L.ref_direct_herk_staging_bytes(N, K, B)), dtype=torch.uint8, device=dev)
+    C = torch.empty(B, tri_size(N), 2, device=dev)
+
+    def call():
+        rc = L.ref_direct_herk_qc(ctypes.c_void_p(qc.data_ptr()), ctypes.c_void_p(fp8.data_ptr()),
+                                  ctypes.c_void_p(C.data_ptr()), N, K, B,
+                                  ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"reference direct HERK launch failed ({rc})")
+    ms = _timed(torch, call, reps=max(3, min(steps, 10)), warm=2)
+    same = bool(torch.equal(C, C_ours))
+    del fp8, C
+    flops = herk_flops(N, K, B)
+    return {"what": "reference herk_direct_fp8_precast_kernel (mma.sync) + "
+                    "cast_int4_to_fp8_interleaved, built from its sources for sm_100a",
+            "value": flops / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms,
+            "bit_exact_vs_library": same}
+
+
 def run_config1_leg(torch, dev, N=128, K=256, B=32, seed=8):
     """The small plain configuration (64 antennas x 2 pols = 128 inputs, 32
     channels, K = 256): latency of one call, tuned and graph-replayed, and
@@ -481,6 +529,13 @@ def run_ours(args, rank, world, dist):
                  "what": f"{B} launches of batch=1 per step, one CTA per tile (not persistent), "
                          f"no graph, no tuning"}
 
+    # --- the reference's own Blackwell direct kernel on the same input
+    ref_direct = None
+    if not args.no_plain:
+        step()
+        torch.cuda.synchronize()
+        ref_direct = run_reference_direct_leg(torch, dev, qc, C, N, K, B, args.steps)
+
     # --- end to end through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
@@ -565,6 +620,8 @@ def run_ours(args, rank, world, dist):
                                     if probes else None} if batched else None),
         "plain_per_channel": plain,
         "speedup_vs_plain": (value / world / plain["value"]) if plain else None,
+        "reference_direct_mma_sync": ref_direct,
+        "vs_direct_mma_sync": (value / world / ref_direct["value"]) if ref_direct else None,
         "e2e": e2e,
         "batched_uneven_flagged": batched,
         "raw_layout_fused_corner_turn": raw_layout,
