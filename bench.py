@@ -60,7 +60,7 @@ def parse():
     p.add_argument("--leg", default=None,
                    choices=["nvfp4", "nvfp4split", "raw", "imaging", "xengine", "splitk",
                             "precision", "imaging_visbf", "batched", "xengine", "peaks",
-                            "config1"],
+                            "config1", "diff"],
                    help="run one extra workload alone and print its JSON (profiling cases); "
                         "nvfp4 and nvfp4split use --inputs/--channels/--k")
     p.add_argument("--strategy", default=None,
@@ -949,13 +949,38 @@ def run_diff_leg(torch, dev, N=2048, B=32, K=512, seed=5):
             raise RuntimeError("device wait timed out in the differentiation leg")
     adj_flops = 8.0 * N * N * K * B
     gg_bytes = float(B) * P * (8 + 8 + 4)
+    peaks = measured_peaks()
+    adj_pipe = 2.0 * adj_flops / (ms_adj * 1e-3) / 1e12  # hi + lo passes on the tensor pipe
+    gg_gbs = gg_bytes / (ms_gg * 1e-3) / 1e9
     return {"workload": f"{N} inputs x {B} channels x K={K}",
             "adjoint": {"value": adj_flops / (ms_adj * 1e-3) / 1e12, "unit": UNIT,
                         "ms_per_step": ms_adj,
                         "note": "8 N^2 K per channel; executed as bf16 hi + lo (2x that on "
-                                "the tensor cores), plus the G + G^H split pass"},
-            "gain_gradient": {"value": gg_bytes / (ms_gg * 1e-3) / 1e9, "unit": "GB/s",
-                              "ms_per_step": ms_gg, "bytes_per_step": gg_bytes}}
+                                "the tensor cores), plus the G + G^H split pass",
+                        "roofline": {"bound": "tensor", "achieved": adj_pipe, "unit": "TFLOPS",
+                                     "peak": peaks.get("bf16_tflops"),
+                                     "frac": (adj_pipe / peaks["bf16_tflops"])
+                                     if peaks.get("bf16_tflops") else None,
+                                     "peak_source": peaks.get("source")}},
+            "gain_gradient": {"value": gg_gbs, "unit": "GB/s",
+                              "ms_per_step": ms_gg, "bytes_per_step": gg_bytes,
+                              "roofline": {"bound": "hbm", "achieved": gg_gbs, "unit": "GB/s",
+                                           "peak": peaks.get("hbm_gbs"),
+                                           "frac": (gg_gbs / peaks["hbm_gbs"])
+                                           if peaks.get("hbm_gbs") else None,
+                                           "peak_source": peaks.get("source")}}}
+
+
+def measured_peaks():
+    """HBM GB/s and dense bf16 TFLOPS (burst) of this pool's B200s from
+    MEASURED_PEAKS.json when present, else the pool's earlier measurement."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]),
+                "source": "MEASURED_PEAKS.json (measured)"}
+    except (OSError, ValueError, KeyError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
 def run_e2e(torch, args, dev, qc_dev, N, K, B, flops, world, dist):
@@ -1032,6 +1057,8 @@ def run_leg(args):
     torch.cuda.set_device(dev)
     if args.leg == "config1":
         out = run_config1_leg(torch, dev)
+    elif args.leg == "diff":
+        out = run_diff_leg(torch, dev)
     elif args.leg == "peaks":
         out = measure_tcgen05_peaks(dev.index)
         out["fp8_cublaslt_8192"] = measure_fp8_peak(torch, dev)

@@ -8,9 +8,9 @@
 //   dV = S_hi V + S_lo V
 // runs on the tensor cores (tcgen05.mma kind::f16, FP32 accumulation).
 //
-//  * sym_split_kernel: S = G + G^H through 32 x 32 shared-memory tiles (the
-//    transposed read), written as four bf16 planes Re_hi, Im_hi, Re_lo, Im_lo
-//    [batch*N][N].
+//  * sym_split_kernel: S = G + G^H, one block per pair of mirrored 32 x 32
+//    tiles (each element of G read once), written as four bf16 planes Re_hi,
+//    Im_hi, Re_lo, Im_lo [batch*N][N].
 //  * vt_kernel: V [batch][N][K] QC -> V^T planes Re, Im [batch*K][N] bf16.
 //  * adjoint_tc_kernel: persistent; tile = 128 time samples (MMA M) x 128
 //    antennas (MMA N), K = antennas contracted, 2-stage TMA ring of six
@@ -42,33 +42,80 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bflo
   lo = __float2bfloat16_rn(x - __bfloat162float(hi));
 }
 
-// S = G + G^H, 32 x 32 tile per block (32 x 8 threads).
-__global__ void sym_split_kernel(const float2* __restrict__ G, __nv_bfloat16* __restrict__ S,
-                                 int n, int64_t plane_elems) {
-  __shared__ float2 tt[32][33];
-  const int b = blockIdx.z;
-  const int a0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+// S = G + G^H, one block per pair of mirrored 32 x 32 tiles (tile row i >=
+// tile column j, 16 x 16 threads): the block reads G's tiles (i, j) and
+// (j, i) once each -- every element of G crosses HBM once -- and writes S's
+// tiles (i, j) and (j, i):  S[a][c] = G[a][c] + conj(G[c][a]).  Thread (x, y)
+// owns rows y, y + 16 and columns 2x, 2x + 1 of a tile: its two elements of
+// a row arrive as one 16-byte load when G is 16-byte aligned, and each bf16
+// plane is written in pairs.  n is a multiple of 8, so tiles never straddle
+// the matrix edge by an odd column.
+__device__ __forceinline__ float4 load2(const float2* p, bool v16) {
+  if (v16) return __ldcs(reinterpret_cast<const float4*>(p));
+  const float2 u = __ldcs(p), v = __ldcs(p + 1);
+  return make_float4(u.x, u.y, v.x, v.y);
+}
+
+__global__ void __launch_bounds__(256) sym_split_kernel(const float2* __restrict__ G,
+                                                        __nv_bfloat16* __restrict__ S, int n,
+                                                        int64_t plane_elems) {
+  __shared__ float2 tile[2][32][33];  // [0] = G tile (i, j), [1] = G tile (j, i)
+  const int b = blockIdx.y;
+  const int r = blockIdx.x;  // lower-triangle tile index -> (ti, tj), tj <= ti
+  int ti = int((sqrtf(8.f * float(r) + 1.f) - 1.f) * 0.5f);
+  while (ti > 0 && ti * (ti + 1) / 2 > r) --ti;
+  while ((ti + 1) * (ti + 2) / 2 <= r) ++ti;
+  const int tj = r - ti * (ti + 1) / 2;
+  const int tx = threadIdx.x, ty = threadIdx.y;
   const float2* Gb = G + int64_t(b) * n * n;
-  // load G[c0 + y][a0 + x] (the transposed tile) into tt[y][x]
-  for (int y = threadIdx.y; y < 32; y += 8) {
-    const int r = c0 + y, c = a0 + threadIdx.x;
-    tt[y][threadIdx.x] = (r < n && c < n) ? Gb[int64_t(r) * n + c] : make_float2(0.f, 0.f);
+  const bool v16 = (reinterpret_cast<uintptr_t>(G) & 15) == 0;
+  const int nt = ti == tj ? 1 : 2;
+  // loads: both tiles, rows ty and ty + 16, columns 2 tx, 2 tx + 1
+  float4 v[2][2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int rb = (q == 0 ? ti : tj) * 32, cb = (q == 0 ? tj : ti) * 32;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int a = rb + ty + 16 * k, c = cb + 2 * tx;
+      v[q][k] = (q < nt && a < n && c < n) ? load2(Gb + int64_t(a) * n + c, v16)
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
   }
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      tile[q][ty + 16 * k][2 * tx] = make_float2(v[q][k].x, v[q][k].y);
+      tile[q][ty + 16 * k][2 * tx + 1] = make_float2(v[q][k].z, v[q][k].w);
+    }
   __syncthreads();
-  for (int y = threadIdx.y; y < 32; y += 8) {
-    const int a = a0 + y, c = c0 + threadIdx.x;
-    if (a >= n || c >= n) continue;
-    const float2 g = Gb[int64_t(a) * n + c];
-    const float2 gt = tt[threadIdx.x][y];  // G[c][a]
-    const float sr = g.x + gt.x, si = g.y - gt.y;  // G[a][c] + conj(G[c][a])
-    __nv_bfloat16 rh, rl, ih, il;
-    split_bf16(sr, rh, rl);
-    split_bf16(si, ih, il);
-    const int64_t o = (int64_t(b) * n + a) * n + c;
-    S[o] = rh;
-    S[plane_elems + o] = ih;
-    S[2 * plane_elems + o] = rl;
-    S[3 * plane_elems + o] = il;
+  // S tile (i, j) from tile[0] and the transpose of tile[1]; S tile (j, i)
+  // from tile[1] and the transpose of tile[0] (a diagonal tile: itself)
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    if (q >= nt) break;
+    const int rb = (q == 0 ? ti : tj) * 32, cb = (q == 0 ? tj : ti) * 32;
+    const int other = nt == 1 ? 0 : 1 - q;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int rl = ty + 16 * k, a = rb + rl, c = cb + 2 * tx;
+      if (a >= n || c >= n) continue;
+      const float2 g0 = tile[q][rl][2 * tx], g1 = tile[q][rl][2 * tx + 1];
+      const float2 t0 = tile[other][2 * tx][rl], t1 = tile[other][2 * tx + 1][rl];
+      const float sr0 = g0.x + t0.x, si0 = g0.y - t0.y;
+      const float sr1 = g1.x + t1.x, si1 = g1.y - t1.y;
+      __nv_bfloat16 rh0, rl0, ih0, il0, rh1, rl1, ih1, il1;
+      split_bf16(sr0, rh0, rl0);
+      split_bf16(si0, ih0, il0);
+      split_bf16(sr1, rh1, rl1);
+      split_bf16(si1, ih1, il1);
+      const int64_t o = (int64_t(b) * n + a) * n + c;
+      *reinterpret_cast<__nv_bfloat162*>(S + o) = __halves2bfloat162(rh0, rh1);
+      *reinterpret_cast<__nv_bfloat162*>(S + plane_elems + o) = __halves2bfloat162(ih0, ih1);
+      *reinterpret_cast<__nv_bfloat162*>(S + 2 * plane_elems + o) = __halves2bfloat162(rl0, rl1);
+      *reinterpret_cast<__nv_bfloat162*>(S + 3 * plane_elems + o) = __halves2bfloat162(il0, il1);
+    }
   }
 }
 
@@ -318,9 +365,10 @@ cudaError_t launch_adjoint(const void* G, const uint8_t* V, void* dV, int n, int
   __nv_bfloat16* S = reinterpret_cast<__nv_bfloat16*>(ws);
   __nv_bfloat16* VT = reinterpret_cast<__nv_bfloat16*>(
       ws + ((4 * size_t(s_plane) * 2 + 1023) / 1024) * 1024);
-  const dim3 tb(32, 8);
-  sym_split_kernel<<<dim3((n + 31) / 32, (n + 31) / 32, batch), tb, 0, s>>>(
+  const int nt = (n + 31) / 32;
+  sym_split_kernel<<<dim3(unsigned(nt * (nt + 1) / 2), unsigned(batch)), dim3(16, 16), 0, s>>>(
       static_cast<const float2*>(G), S, n, s_plane);
+  const dim3 tb(32, 8);
   vt_kernel<<<dim3((n + 31) / 32, (K + 31) / 32, batch), tb, 0, s>>>(V, VT, n, K, v_plane);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;

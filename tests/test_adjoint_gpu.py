@@ -44,6 +44,27 @@ def test_adjoint_general_g_ragged():
     assert err < 1e-4
 
 
+def test_adjoint_g_only_8_byte_aligned():
+    # G one complex64 into an allocation (8- but not 16-byte aligned): the
+    # symmetrisation pass reads it element-wise, same result as aligned
+    rng = np.random.default_rng(83)
+    N, K, B = 136, 72, 2
+    G = (rng.normal(size=(B, N, N)) + 1j * rng.normal(size=(B, N, N))).astype(np.complex64)
+    qc = oracle.gaussian_qc(84, B, N, K)
+    flat = np.concatenate([np.zeros(1, np.complex64), G.reshape(-1)])
+    buf = torch.from_numpy(flat.view(np.float32)).to(DEV)
+    dG = buf[2:]  # offset by one complex64
+    assert dG.data_ptr() % 16 == 8
+    dV = torch.from_numpy(qc.reshape(-1)).to(DEV)
+    out = torch.empty(B, N, K, 2, device=DEV)
+    with Correlator() as c:
+        c.herk_adjoint(dG, dV, out, N, K, B)
+        assert c.device_status() == 0
+    o = out.cpu().numpy()
+    got = o[..., 0].astype(np.float64) + 1j * o[..., 1]
+    assert np.array_equal(got, run(G, qc, N, K, B))
+
+
 def test_adjoint_matches_finite_differences():
     rng = np.random.default_rng(82)
     N, K, B = 64, 40, 1
