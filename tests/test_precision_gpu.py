@@ -342,3 +342,42 @@ def test_fp8_float_modes_match_restated_quantiser(store_mode):
         err = np.abs(got - ref).max() / np.abs(ref).max()
         print("fp8", store_mode, split, "max rel err vs restated quantiser", err)
         assert err <= tol
+
+
+def test_nvfp4_rfi_at_independent_times_and_handle_reuse():
+    # bursts at each input's own random times (the union of flagged samples is
+    # ~10x the shared-time case: F ~ 120 of K = 1024, still one lo stage), a
+    # channel with no bursts, and a silent input: the GPU equals the restated
+    # quantiser, the error stays within 2e-2, and calls alternating plain /
+    # split / plain on one handle give the plain result both times (the lo
+    # extent of every channel is rewritten by each call)
+    from ftd_b200._lib import COMPUTE_FP4, COMPUTE_FP4_SPLIT
+    rng = np.random.default_rng(412)
+    B, N, K = 3, 256, 1024
+    v = oracle.workload4_voltages(413, B, N, K, rfi_time_frac=0.0)
+    for b in (0, 1):  # channel 2 keeps no bursts
+        amp = 20.0 * np.sqrt(np.mean(np.abs(v[b]) ** 2))
+        for i in rng.choice(N, size=N // 20, replace=False):
+            ts = rng.choice(K, size=K // 100, replace=False)
+            v[b, i, ts] = (amp * np.exp(2j * np.pi * rng.uniform(size=ts.size))).astype(np.complex64)
+    v[1, 7] = 0  # a silent input
+    order, nflag = oracle.nvfp4_time_order(v)
+    assert nflag[0] > 50 and nflag[1] > 50 and nflag[2] == 0
+    A = torch.from_numpy(np.ascontiguousarray(v).view(np.float32).reshape(B, N, K, 2)).to(DEV)
+    C = torch.empty(B, tri_size(N), 2, device=DEV)
+    outs = []
+    with Correlator() as c:
+        c.set_strategy(2, 0)
+        for compute in (COMPUTE_FP4, COMPUTE_FP4_SPLIT, COMPUTE_FP4):
+            c.herk(A, C, N, K, B, input=IN_FP32, compute=compute, output=OUT_FP32, tune=False)
+            assert c.device_status() == 0
+            outs.append(C.cpu().numpy().astype(np.float64))
+    assert np.array_equal(outs[0], outs[2])
+    ref = oracle.herk_nvfp4(v)
+    scale = np.abs(ref).max()
+    assert np.abs(outs[0] - ref).max() <= 1e-6 * scale
+    exact = oracle.herk_c128(v.astype(np.complex128), N, K, B)
+    err = oracle.correlation_errors(outs[0], exact, N)
+    print("nvfp4 independent-time rfi", err)
+    assert err["max_offdiag_norm"] < 2e-2 and err["max_auto_rel"] < 1e-5
+    assert np.all(outs[0][1][tri_size(7) + 7] == 0)  # the silent input's autocorrelation
