@@ -329,54 +329,6 @@ __device__ __forceinline__ void store_chunk_xengine(Out2* ob, int i0, int j, int
   }
 }
 
-// Sector-aligned variant of the fast store for FP32 output, used when a whole
-// 32-row x 128-column block of the tile (the four warps of one epilogue half)
-// lies below n and strictly below the diagonal.  A row segment of 32
-// complex64 elements rarely starts on a 32-byte L2 sector, and a sector
-// written in two parts by two warps costs far more than a whole one.  So each
-// warp stores only the sectors it owns outright; the elements of the sectors
-// it shares with the neighbouring warps (at most 3 on each side) go to
-// shared memory, and after a barrier of the half those 96 sectors
-// (32 rows x 3 warp boundaries) are written whole, one 32-byte store per
-// thread.  Sectors shared with the neighbouring tiles stay split.
-// t0: element (i0, jt0) of the packed triangle, jt0 = first column of the
-// 128-column block; q = warp's 32-column quarter; sec: [32][3][4] elements.
-template <bool kScale>
-__device__ __forceinline__ void store_chunk_sectors(float2* t0, int i0, int q, int lane, float sc,
-                                                    float2 (*sec)[3][4], uint32_t bar_id,
-                                                    const uint32_t (&re)[32],
-                                                    const uint32_t (&im)[32]) {
-  float2* p = t0 + 32 * q + lane;
-#pragma unroll
-  for (int m = 0; m < 32; ++m) {
-    // first element of this warp's segment, modulo one sector (4 elements)
-    const int mw = int(((reinterpret_cast<uintptr_t>(p) >> 3) - uintptr_t(lane)) & 3u);
-    float vr = __uint_as_float(re[m]), vi = __uint_as_float(im[m]);
-    if (kScale) {
-      vr *= sc;
-      vi *= sc;
-    }
-    if (q > 0 && lane < ((4 - mw) & 3))
-      sec[m][q - 1][mw + lane] = make_float2(vr, vi);
-    else if (q < 3 && lane >= 32 - mw)
-      sec[m][q][lane - 32 + mw] = make_float2(vr, vi);
-    else
-      put(p, vr, vi);
-    p += i0 + m + 1;
-  }
-  named_bar_sync(bar_id, 128);
-  const int slot = q * 32 + lane;
-  if (slot < 96) {
-    const int r = slot / 3, b = slot - 3 * r + 1;
-    float2* sp = t0 + (r * i0 + r * (r + 1) / 2) + 32 * b;  // element (i0 + r, jt0 + 32 b)
-    const int mw = int((reinterpret_cast<uintptr_t>(sp) >> 3) & 3u);
-    if (mw != 0) {
-      const float4* v = reinterpret_cast<const float4*>(&sec[r][b - 1][0]);
-      st_global_cs_v8(sp - mw, v[0], v[1]);
-    }
-  }
-}
-
 template <typename Out2>
 __device__ __forceinline__ void store_chunk(Out2* p, float2* pc, int i0, int j, int n, bool full,
                                             float sc, const HerkArgs& args,
@@ -609,9 +561,6 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
     const uint32_t bar_id = 1u + uint32_t(half);
     const bool plain = (args.alpha == 1.f) && (args.beta == 0.f) && !args.kahan &&
                        args.chan_scale == nullptr;
-    // sector-aligned stores need no read of the old value
-    const bool sector_ok = (args.beta == 0.f) && !args.kahan;
-    uint32_t sec_it = 0;
     const uint32_t stg = smem_u32(stg_base) + uint32_t(half * 2 * kStgRows * kStgRowBytes);
     const bool issuer = (q == 0) && (lane < kStgRows);  // issues one row copy per sub-chunk
     int acc = 0;
@@ -732,20 +681,6 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
           }
           // element (i, j) lives at i(i+1)/2 + j; row i+1 starts i+1 later
           const int64_t e0 = int64_t(i0) * (i0 + 1) / 2 + j;
-          if constexpr (sizeof(Out2) == 8) {
-            // half-uniform: all 128 columns of these 32 rows below the diagonal and n
-            if (sector_ok && j0 + kTile - 1 < i0 && i0 + 31 < n) {
-              auto* sec = reinterpret_cast<float2(*)[3][4]>(
-                  stg_base + kSecOffset(half, int(sec_it & 1)));
-              ++sec_it;
-              float2* t0 = reinterpret_cast<float2*>(outc) + (int64_t(i0) * (i0 + 1) / 2 + j0);
-              if (sc == 1.f)
-                store_chunk_sectors<false>(t0, i0, q, lane, sc, sec, bar_id, re, im);
-              else
-                store_chunk_sectors<true>(t0, i0, q, lane, sc, sec, bar_id, re, im);
-              continue;
-            }
-          }
           // compensation buffer: same layout as the output (uniform calls only)
           float2* pc = args.kahan ? static_cast<float2*>(args.out2) + cd.out0 + e0 : nullptr;
           store_chunk(outc + e0, pc, i0, j, n, i0 + 31 < n && jw + 31 < i0, sc, args, re, im);
@@ -789,7 +724,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
 constexpr int kPairPlane = 128 * kStageK;  // 16 KB: 128 rows of 128 samples
 constexpr int kPairStageBytes = 4 * kPairPlane;
 constexpr int kPairStages = 3;
-// the epilogue area: sector buffers and, for the bulk store mode, staging
+// the epilogue area: staging for the bulk store mode
 constexpr size_t kPairSmem = 1024 + size_t(kPairStages) * kPairStageBytes + kStgBytes + 256;
 static_assert(kPairSmem <= 232448, "shared memory per CTA");
 
@@ -798,8 +733,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
     herk_fp8_pair_kernel(const __grid_constant__ CUtensorMap tmZ, const HerkArgs args) {
   extern __shared__ uint8_t smem_dyn[];
   uint8_t* smem = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
-  uint8_t* sec_base = smem + kPairStages * kPairStageBytes;  // epilogue shared sectors
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sec_base + kStgBytes);
+  uint8_t* stg_base = smem + kPairStages * kPairStageBytes;  // epilogue staging (kStgBytes)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(stg_base + kStgBytes);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kPairStages + 5);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const uint32_t smem0 = smem_u32(smem);
@@ -950,9 +885,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
     int acc = 0;
     uint32_t acc_phase = 0;
     Out2* out = static_cast<Out2*>(args.out);
-    const bool sector_ok = (args.beta == 0.f) && !args.kahan;
     const uint32_t bar_id = 1u + uint32_t(half);
-    uint32_t sec_it = 0;
     for (int t = pair; t < args.num_tiles; t += npairs) {
       const TileDesc td = args.tiles[t];
       const ChanDesc cd = args.chans[td.ch];
@@ -1028,7 +961,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
         // time staged in shared memory (keeping each row's 16-byte phase),
         // one bulk copy per row; a row starting 8 mod 16 stores its first
         // and last element directly.
-        const uint32_t stg = smem_u32(sec_base) + uint32_t(half * 2 * kStgRows * kStgRowBytes);
+        const uint32_t stg = smem_u32(stg_base) + uint32_t(half * 2 * kStgRows * kStgRowBytes);
         const bool issuer = (q == 0) && (lane < kStgRows);
 #pragma unroll 1
         for (int sub = 0; sub < (kTile / 2) / kStgRows; ++sub) {
@@ -1095,20 +1028,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
           continue;
         }
         const int64_t e0 = int64_t(i0) * (i0 + 1) / 2 + j;
-        if constexpr (sizeof(Out2) == 8) {
-          const int jt0 = jw - q * 32;  // first column of this CTA's 128
-          if (sector_ok && jt0 + 127 < i0 && i0 + 31 < n) {  // half-uniform
-            auto* sec = reinterpret_cast<float2(*)[3][4]>(
-                sec_base + kSecOffset(half, int(sec_it & 1)));
-            ++sec_it;
-            float2* t0 = reinterpret_cast<float2*>(outc) + (int64_t(i0) * (i0 + 1) / 2 + jt0);
-            if (sc == 1.f)
-              store_chunk_sectors<false>(t0, i0, q, lane, sc, sec, bar_id, re, im);
-            else
-              store_chunk_sectors<true>(t0, i0, q, lane, sc, sec, bar_id, re, im);
-            continue;
-          }
-        }
         float2* pc = args.kahan ? static_cast<float2*>(args.out2) + cd.out0 + e0 : nullptr;
         store_chunk(outc + e0, pc, i0, j, n, i0 + 31 < n && jw + 31 < i0, sc, args, re, im);
       }

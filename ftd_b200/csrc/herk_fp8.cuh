@@ -38,18 +38,6 @@ constexpr int kStgRows = 8;
 constexpr int kStgRowBytes = kTile * 8 + 16;
 constexpr int kStgBytes = 2 /*halves*/ * 2 /*buffers*/ * kStgRows * kStgRowBytes;
 constexpr size_t kHerkSmem = 1024 + size_t(kStages) * kStageBytes + kStgBytes + 256;
-// Shared sectors of the sector-aligned epilogue: per half, two buffers of
-// 32 rows x 3 warp boundaries x 4 complex64 elements, inside that half's
-// staging buffer 0 (kSecOffset): a bulk-stored tile ends with only its copy
-// from buffer 1 still reading shared memory (an even number of 8-row
-// sub-chunks), so a following tile's sector stores never overwrite data a
-// copy still reads, in either half.
-constexpr int kSecBufBytes = 32 * 3 * 4 * 8;
-constexpr int kSecBytes = 2 /*halves*/ * 2 /*buffers*/ * kSecBufBytes;
-__host__ __device__ constexpr int kSecOffset(int half, int parity) {
-  return half * 2 * kStgRows * kStgRowBytes + parity * kSecBufBytes;
-}
-static_assert(2 * kSecBufBytes <= kStgRows * kStgRowBytes, "sector buffers fit in buffer 0");
 static_assert(((kTile / 2) / kStgRows) % 2 == 0, "bulk tiles end on staging buffer 1");
 
 // One lower-triangle tile: channel, row block ti (i), column block tj (j), tj <= ti.

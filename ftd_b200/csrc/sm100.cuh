@@ -162,13 +162,6 @@ __device__ __forceinline__ void st_shared_v2(uint32_t addr, uint32_t a, uint32_t
   asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(addr), "r"(a), "r"(b) : "memory");
 }
 
-// 32-byte streaming store (one whole L2 sector) from one thread.
-__device__ __forceinline__ void st_global_cs_v8(void* p, float4 a, float4 b) {
-  asm volatile("st.global.cs.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(a.x),
-               "f"(a.y), "f"(a.z), "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w)
-               : "memory");
-}
-
 // ---------------------------------------------------------------- CTA pairs
 // (a cluster of two CTAs running one tcgen05 cta_group::2 MMA together)
 __device__ __forceinline__ uint32_t cluster_rank() {
