@@ -300,13 +300,19 @@ def measure_fp8_peak(torch, device):
 
 def measure_tcgen05_peaks(device_index, iters=20000, reps=3):
     """Dense tcgen05 throughput (TFLOPS) of the MMA shapes the correlators use,
-    from ftdx_peak_probe: M = N = 256 CTA-pair MMAs from fixed shared-memory
-    tiles, FP8 E4M3 (K = 32) and NVFP4 block16 (K = 64), no loads or stores."""
+    from ftdx_peak_probe, no loads or stores: M = N = 256 CTA-pair MMAs on
+    zero tiles (FP8 E4M3, K = 32, and NVFP4 block16, K = 64), and the two FP8
+    correlators' own MMA streams on QC-valued operands (CTA pair: two
+    M = N = 256 MMAs per 32 samples; single CTA: four M = N = 128)."""
     from ftd_b200 import Correlator
     with Correlator(device=device_index) as c:
         return {"fp8_e4m3": c.peak_probe(0, iters, reps), "nvfp4": c.peak_probe(1, iters, reps),
-                "what": f"{iters} back-to-back tcgen05.mma.cta_group::2 M=N=256 per SM pair, "
-                        f"best of {reps} launches"}
+                "fp8_qc_data_pair": c.peak_probe(2, iters, reps),
+                "fp8_qc_data_single_cta": c.peak_probe(3, iters, reps),
+                "what": f"{iters} back-to-back tcgen05.mma per SM pair (cta_group::2, M=N=256) "
+                        f"or per SM (fp8_qc_data_single_cta: cta_group::1, M=N=128), best of "
+                        f"{reps} launches; fp8_e4m3 / nvfp4 on zero tiles, fp8_qc_data_* on "
+                        f"E4M3 codes of random integers -7..7"}
 
 
 def measure_int8_peak(torch, device):

@@ -169,7 +169,9 @@ class Correlator:
                                                    _stream(stream)))
 
     def peak_probe(self, kind: int, iters: int = 20000, reps: int = 3) -> float:
-        """Measured dense tensor-core TFLOPS: kind 0 FP8 E4M3, 1 NVFP4."""
+        """Measured dense tensor-core TFLOPS: kind 0 FP8 E4M3 and 1 NVFP4 (CTA-pair
+        MMAs on zero tiles); 2 and 3 the CTA-pair and single-CTA correlators'
+        FP8 MMA streams on QC-valued operands."""
         out = ctypes.c_double(0.0)
         check(self._h, self._L.ftdx_peak_probe(self._h, kind, iters, reps, ctypes.byref(out)),
               "ftdx_peak_probe")

@@ -416,12 +416,19 @@ FTDX_API ftdx_status ftdx_gain_gradient(ftdx_handle h, const void* R_obs, const 
                                         double* grad, double* loss, void* stream);
 
 /* Dense tensor-core throughput of this GPU (no counterpart in the reference),
- * for roofline denominators: every SM pair issues `iters` back-to-back
- * tcgen05.mma.cta_group::2 of M = N = 256 from fixed shared-memory tiles
- * (kind 0: FP8 E4M3, K = 32; kind 1: NVFP4 E2M1 with UE4M3 block-16 scales,
- * K = 64), FP32 accumulation, no loads or stores; the fastest of `reps`
- * timed launches (after one warm-up) gives *tflops = 2 M N K MMAs / time.
- * Synchronises the device. */
+ * for roofline denominators: back-to-back tcgen05 MMAs from shared-memory
+ * tiles, FP32 accumulation, no loads or stores.
+ *   kind 0: every SM pair issues `iters` cta_group::2 M = N = 256 FP8 E4M3
+ *           (K = 32) MMAs on zero tiles;
+ *   kind 1: the same with NVFP4 E2M1 and UE4M3 block-16 scales (K = 64);
+ *   kind 2: as kind 0 on QC-valued operands (E4M3 codes of integers -7..7),
+ *           in the CTA-pair correlator's order (two MMAs per 32 samples);
+ *   kind 3: every SM issues `iters` cta_group::1 M = N = 128 FP8 MMAs on
+ *           QC-valued operands in the single-CTA correlator's order (four
+ *           per 32 samples into two accumulators).
+ * Kinds 2 and 3 round `iters` up to whole 32-sample steps.  The fastest of
+ * `reps` timed launches (after one warm-up) gives
+ * *tflops = 2 M N K x MMAs x issuers / time.  Synchronises the device. */
 FTDX_API ftdx_status ftdx_peak_probe(ftdx_handle h, int kind, int iters, int reps, double* tflops);
 
 /* Kernel timing (no counterpart in the reference; its benches time whole
