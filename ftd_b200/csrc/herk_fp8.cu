@@ -433,9 +433,10 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       uint32_t phase = 0;
       int issued = 0;
       bool ok = true;
-      for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
-        const TileDesc td = args.tiles[t];
-        const ChanDesc cd = args.chans[td.ch];
+      for (TileWalk w(args.tiles, args.chans, args.num_tiles, blockIdx.x, gridDim.x);
+           w.valid() && ok; w.advance()) {
+        const TileDesc td = w.td;
+        const ChanDesc cd = w.cd;
         // the packed-upper output format swaps the blocks: TMEM lane = larger index
         const bool swap = args.out_format == 1;
         const int32_t rowJ = int32_t(cd.row0 + int64_t(swap ? td.ti : td.tj) * kTile);
@@ -494,9 +495,10 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       int acc = 0;
       uint32_t acc_phase = 0;
       bool ok = true;
-      for (int t = blockIdx.x; t < args.num_tiles && ok; t += gridDim.x) {
-        const TileDesc td = args.tiles[t];
-        const ChanDesc cd = args.chans[td.ch];
+      for (TileWalk w(args.tiles, args.chans, args.num_tiles, blockIdx.x, gridDim.x);
+           w.valid() && ok; w.advance()) {
+        const TileDesc td = w.td;
+        const ChanDesc cd = w.cd;
         const bool diag = td.ti == td.tj;
         if (!mbar_wait(tempty_bar(acc), acc_phase ^ 1u, abort_flag)) {
           atomicOr(args.status, kStatusTimeoutMma);
@@ -566,9 +568,10 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
     int acc = 0;
     uint32_t acc_phase = 0;
     Out2* out = static_cast<Out2*>(args.out);
-    for (int t = blockIdx.x; t < args.num_tiles; t += gridDim.x) {
-      const TileDesc td = args.tiles[t];
-      const ChanDesc cd = args.chans[td.ch];
+    for (TileWalk w(args.tiles, args.chans, args.num_tiles, blockIdx.x, gridDim.x); w.valid();
+         w.advance()) {
+      const TileDesc td = w.td;
+      const ChanDesc cd = w.cd;
       const bool ok = bar_red_and(bar_id, 128, mbar_wait(tfull_bar(acc), acc_phase, abort_flag));
       if (!ok) {
         if (lane == 0) atomicOr(args.status, kStatusTimeoutEpilogue);
@@ -783,9 +786,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
-      for (int t = pair; t < args.num_tiles; t += npairs) {
-        const TileDesc td = args.tiles[t];
-        const ChanDesc cd = args.chans[td.ch];
+      for (TileWalk w(args.tiles, args.chans, args.num_tiles, pair, npairs); w.valid();
+           w.advance()) {
+        const TileDesc td = w.td;
+        const ChanDesc cd = w.cd;
         const int32_t rowJ = int32_t(cd.row0 + int64_t(td.tj) * 256 + 128 * rank);
         const int32_t rowI = int32_t(cd.row0 + int64_t(td.ti) * kTile);
         const int32_t pX = int32_t(rank), pY = int32_t(rank) + 1;  // leader: Re, Im; partner: Im, -Re
@@ -827,8 +831,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
       int stage = 0, acc = 0;
       uint32_t phase = 0, acc_phase = 0;
       bool ok = true;
-      for (int t = pair; t < args.num_tiles && ok; t += npairs) {
-        const ChanDesc cd = args.chans[args.tiles[t].ch];
+      for (TileWalk w(args.tiles, args.chans, args.num_tiles, pair, npairs); w.valid() && ok;
+           w.advance()) {
+        const ChanDesc cd = w.cd;
         if (!mbar_wait(tempty_bar(acc), acc_phase ^ 1u, abort_flag)) {
           atomicOr(args.status, kStatusTimeoutMma);
           break;
@@ -886,9 +891,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
     uint32_t acc_phase = 0;
     Out2* out = static_cast<Out2*>(args.out);
     const uint32_t bar_id = 1u + uint32_t(half);
-    for (int t = pair; t < args.num_tiles; t += npairs) {
-      const TileDesc td = args.tiles[t];
-      const ChanDesc cd = args.chans[td.ch];
+    for (TileWalk w(args.tiles, args.chans, args.num_tiles, pair, npairs); w.valid();
+         w.advance()) {
+      const TileDesc td = w.td;
+      const ChanDesc cd = w.cd;
       // the four warps of a half agree, so none is left alone at a named barrier
       const bool ok = bar_red_and(bar_id, 128, mbar_wait(tfull_bar(acc), acc_phase, abort_flag));
       if (!ok) {

@@ -105,6 +105,43 @@ struct HerkArgs {
   int32_t s8;
 };
 
+// A persistent CTA's walk over its tiles (first, first + step, ...) with the
+// descriptors loaded ahead: the tile descriptor two tiles ahead and the
+// channel descriptor one tile ahead (its index comes from a tile descriptor
+// that arrived a tile earlier), so that no role waits on global memory at a
+// tile boundary.  Loads past the end of the list are not issued.
+struct TileWalk {
+  const TileDesc* tiles;
+  const ChanDesc* chans;
+  int t, step, num;
+  TileDesc td, td1, td2;  // this tile, the next, the one after
+  ChanDesc cd, cd1;       // this tile's channel, the next tile's
+  __device__ __forceinline__ TileWalk(const TileDesc* tiles_, const ChanDesc* chans_, int num_,
+                                      int first, int step_)
+      : tiles(tiles_), chans(chans_), t(first), step(step_), num(num_) {
+    td = tile_at(t);
+    cd = chan_of(td, t);
+    td1 = tile_at(t + step);
+    cd1 = chan_of(td1, t + step);
+    td2 = tile_at(t + 2 * step);
+  }
+  __device__ __forceinline__ TileDesc tile_at(int u) const {
+    return u < num ? tiles[u] : TileDesc{0, 0, 0};
+  }
+  __device__ __forceinline__ ChanDesc chan_of(const TileDesc& d, int u) const {
+    return u < num ? chans[d.ch] : ChanDesc{};
+  }
+  __device__ __forceinline__ bool valid() const { return t < num; }
+  __device__ __forceinline__ void advance() {
+    t += step;
+    td = td1;
+    cd = cd1;
+    td1 = td2;
+    cd1 = chan_of(td1, t + step);
+    td2 = tile_at(t + 2 * step);
+  }
+};
+
 // A plain single-segment argument block.
 inline HerkArgs herk_args_default() {
   HerkArgs a{};
