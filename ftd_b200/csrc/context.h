@@ -29,6 +29,7 @@ struct Plan {
 
 constexpr int kStoreFp6 = 4;
 constexpr int kStoreS8 = 8;   // with store mode 2: signed 8-bit operands, kind::i8 MMAs
+constexpr int kStoreFused = 16;  // alone (mode 0 + 16): QC promotion fused into the single-CTA kernel
 // Launch strategy of the correlator kernel; chosen by the autotuner.
 struct Strategy {
   // 0: direct stores, 1: shared-memory staging + bulk copies,
@@ -36,6 +37,8 @@ struct Strategy {
   // 3: CTA-pair kernel with bulk-copy stores for interior tiles;
   // + kStoreFp6: operands as packed FP6 E3M2 planes (QC input, exact);
   // + kStoreS8 (pair only): signed 8-bit planes, integer MMAs (QC input, exact)
+  // kStoreFused (alone): single CTA, direct stores, the QC bytes converted to
+  // E4M3 inside the correlator (uniform INT4 calls; others run as 0)
   int store_mode = 0;
   int grid = 0;        // persistent CTAs (0: one per SM); -1: one CTA per tile (not persistent)
   int splits = 1;      // split-K: K is cut into this many ranges, partials summed afterwards
@@ -143,6 +146,9 @@ ftdx_status ensure_split_ws(ftdx_handle h, size_t bytes, cudaStream_t s);
 ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t Kp,
                               CUtensorMap* tm, int box_rows = kTile, int nplanes = 2,
                               bool fp6 = false);
+// 2-D map over raw QC bytes [rows][K] (K a multiple of 16, qc 16-byte
+// aligned): 128-byte x 128-row boxes, unswizzled, zeros past K.
+ftdx_status encode_qc_map(ftdx_handle h, const void* qc, int64_t rows, int K, CUtensorMap* tm);
 // Even number of CTAs of the pair kernel that can be resident at once.
 int pair_grid_limit(ftdx_handle h);
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }

@@ -259,6 +259,20 @@ ftdx_status encode_planes_map(ftdx_handle h, uint8_t* z, int64_t rows, int64_t K
   return FTDX_OK;
 }
 
+ftdx_status encode_qc_map(ftdx_handle h, const void* qc, int64_t rows, int K, CUtensorMap* tm) {
+  auto enc = get_encode_fn();
+  if (!enc) return fail(h, FTDX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  const cuuint32_t estr[2] = {1, 1};
+  const cuuint64_t dims[2] = {cuuint64_t(K), cuuint64_t(rows)};
+  const cuuint64_t strides[1] = {cuuint64_t(K)};
+  const cuuint32_t box[2] = {cuuint32_t(kStageK), cuuint32_t(kTile)};
+  CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(qc), dims, strides, box,
+                   estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(h, FTDX_ERR_CUDA, "QC tensor map encode failed: %d", int(r));
+  return FTDX_OK;
+}
+
 static cudaEvent_t pool_event(ftdx_handle h) {
   if (!h->event_pool.empty()) {
     cudaEvent_t e = h->event_pool.back();

@@ -150,6 +150,13 @@ bool fp6_ok(const HerkCall& c) {
   return c.input == FTDX_IN_INT4 && !c.ftd && !c.xeng && !is_split(c) && !is_fp4(c);
 }
 
+// The fused-promotion kernel: uniform QC input (TMA rows of K bytes, so K a
+// multiple of 16 and A 16-byte aligned), FP8 compute, packed lower triangle.
+bool fused_ok(const HerkCall& c) {
+  return fp6_ok(c) && c.compute == FTDX_COMPUTE_FP8 && c.out_format == 0 && c.K % 16 == 0 &&
+         (reinterpret_cast<uintptr_t>(c.A) & 15) == 0;
+}
+
 bool use_pair(ftdx_handle h, const Strategy& strat) {
   return (strat.store_mode & 3) >= 2 && pair_grid_limit(h) >= 2;
 }
@@ -164,12 +171,13 @@ int effective_splits(const HerkCall& c, const Strategy& strat) {
 
 // Workspace and tile plan for a call; allocates, so never while capturing.
 ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan** plan,
-                    bool pair = false, int splits = 1) {
+                    bool pair = false, int splits = 1, bool fused = false) {
   const int64_t Kp = round_up(c.K, kStageK);
   const int64_t zpitch = is_split(c) ? 2 * Kp : Kp;
   const int64_t rows = int64_t(c.N) * c.batch;
-  // the pair kernel reads a third plane, -Re
-  ftdx_status st = ensure_workspace(h, size_t((pair ? 3 : 2) * rows * zpitch), s);
+  // the pair kernel reads a third plane, -Re; the fused kernel no planes
+  ftdx_status st =
+      fused ? FTDX_OK : ensure_workspace(h, size_t((pair ? 3 : 2) * rows * zpitch), s);
   if (st != FTDX_OK) return st;
   if (c.input == FTDX_IN_FP32) {
     st = ensure_aux(h, size_t(12) * size_t(c.batch) + 256, s);
@@ -187,9 +195,10 @@ ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan
 ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, cudaStream_t s) {
   if (is_fp4(c)) return launch_fp4(h, c, strat, s);
   const bool pair = use_pair(h, strat);
+  const bool fused = strat.store_mode == kStoreFused && fused_ok(c);
   const int splits = effective_splits(c, strat);
   const Plan* plan = nullptr;
-  ftdx_status st = prepare(h, c, s, &plan, pair, splits);
+  ftdx_status st = prepare(h, c, s, &plan, pair, splits, fused);
   if (st != FTDX_OK) return st;
   const int64_t Kp = round_up(c.K, kStageK);
   const int64_t zpitch = is_split(c) ? 2 * Kp : Kp;
@@ -199,8 +208,8 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   float* qscale = reinterpret_cast<float*>(h->aux);
   float* out_scale = qscale + c.batch;
   uint32_t* amax = reinterpret_cast<uint32_t*>(out_scale + c.batch);
-  cudaError_t e;
-  {
+  cudaError_t e = cudaSuccess;
+  if (!fused) {
     ScopedTimer tm(h, s, 1);
     if (c.xeng) {
       FtdGeom g{};
@@ -236,8 +245,9 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
     }
   }
   if (e != cudaSuccess) return cuda_fail(h, e, "operand promotion launch");
-  CUtensorMap tmZ;
-  st = encode_planes_map(h, h->z, rows, zpitch, &tmZ, kTile, pair ? 3 : 2, fp6);
+  CUtensorMap tmZ;  // the operand planes, or (fused) the raw QC bytes
+  st = fused ? encode_qc_map(h, c.A, rows, c.K, &tmZ)
+             : encode_planes_map(h, h->z, rows, zpitch, &tmZ, kTile, pair ? 3 : 2, fp6);
   if (st != FTDX_OK) return st;
   HerkArgs args = herk_args_default();
   args.tiles = plan->d_tiles;
@@ -284,7 +294,7 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
     if (strat.grid < 0) grid = plan->num_tiles;   // one tile per CTA
     if (grid > plan->num_tiles) grid = plan->num_tiles;
     ScopedTimer tm(h, s, 0);
-    e = launch_herk_fp8(tmZ, args, grid, s);
+    e = fused ? launch_herk_fp8_fused(tmZ, args, grid, s) : launch_herk_fp8(tmZ, args, grid, s);
   }
   if (e != cudaSuccess) return cuda_fail(h, e, "correlator kernel launch");
   if (splits > 1) {
@@ -316,6 +326,8 @@ ftdx_status run_tune(ftdx_handle h, const HerkCall& c, cudaStream_t s, TuneEntry
       is_fp4(c) ? std::vector<Strategy>{Strategy{0, h->sm_count}}
                 : default_candidates(h, c.output == FTDX_OUT_FP32, true);
   if (is_fp4(c) && nvfp4_pair_limit() >= 1) cands.push_back(Strategy{2, 0});
+  // QC input: promotion fused into the single-CTA correlator
+  if (fused_ok(c)) cands.push_back(Strategy{kStoreFused, h->sm_count});
   // QC input: the pair kernel on signed 8-bit operands (kind::i8, exact)
   if (fp6_ok(c) && c.compute == FTDX_COMPUTE_FP8 && !c.comp && pair_grid_limit(h) >= 2) {
     cands.push_back(Strategy{2 | kStoreS8, pair_grid_limit(h)});
@@ -486,8 +498,10 @@ void release_graphs(ftdx_handle h) {
   h->graphs.clear();
 }
 
-// Store modes 0..3, each optionally + kStoreFp6, or 2 / 3 + kStoreS8.
+// Store modes 0..3, each optionally + kStoreFp6, or 2 / 3 + kStoreS8, or
+// kStoreFused alone.
 static bool valid_store_mode(int m) {
+  if (m == kStoreFused) return true;
   if (m < 0 || (m & ~(3 | kStoreFp6 | kStoreS8)) != 0) return false;
   return !(m & kStoreS8) || m == (2 | kStoreS8) || m == (3 | kStoreS8);
 }

@@ -877,16 +877,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(k4pThreads, 1)
                           sdesc_sw128_kmajor(b_addr(stage) + 32 * s), idesc, sfa_t + 4 * s,
                           sfb_t + 8 * s, (kb | s) != 0);
           }
-          mma_commit_pair(empty_bar(stage));
-          mma_commit_pair(map_shared(empty_bar(stage), 1));
+          mma_commit_pair_both(empty_bar(stage));
           if (++stage == k4pStages) {
             stage = 0;
             phase ^= 1u;
           }
         }
         if (!ok) break;
-        mma_commit_pair(tfull_bar(acc));
-        mma_commit_pair(map_shared(tfull_bar(acc), 1));
+        mma_commit_pair_both(tfull_bar(acc));
         if (++acc == 2) {
           acc = 0;
           acc_phase ^= 1u;

@@ -376,25 +376,40 @@ __device__ __forceinline__ void store_chunk(Out2* p, float2* pc, int i0, int j, 
   }
 }
 
-template <typename OutT>
-__global__ void __launch_bounds__(kHerkThreads, 1)
+// kFused (QC input only): tmZ maps the raw QC bytes [rows][K] instead of the
+// operand planes; the producer loads raw tiles (128 rows x 128 samples, one
+// byte each) into a ring of kRawStages, and four converter warps (warps 10-13)
+// turn each into the E4M3 Re / Im planes of an operand stage in the 128-byte
+// swizzled layout the TMA would have written, then release it to the MMA warp.
+template <typename OutT, bool kFused>
+__global__ void __launch_bounds__(kFused ? kFusedThreads : kHerkThreads, 1)
     herk_fp8_tc_kernel(const __grid_constant__ CUtensorMap tmZ, const HerkArgs args) {
+  constexpr int kOpStages = kFused ? kFusedStages : kStages;
+  constexpr int kBarCount = 2 * kOpStages + 5 + (kFused ? 2 * kRawStages : 0);
   extern __shared__ uint8_t smem_dyn[];
   // 128 B swizzled operand tiles must start on 1024 B boundaries of the
   // shared window.
   uint8_t* smem = smem_dyn + ((1024u - (smem_u32(smem_dyn) & 1023u)) & 1023u);
-  uint8_t* stg_base = smem + kStages * kStageBytes;  // epilogue staging (kStgBytes)
-  uint64_t* bars = reinterpret_cast<uint64_t*>(stg_base + kStgBytes);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 5);
+  // epilogue staging (kStgBytes); with kFused the raw QC ring instead
+  uint8_t* stg_base = smem + kOpStages * kStageBytes;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(
+      stg_base + (kFused ? size_t(kRawStages) * kRawStageBytes : size_t(kStgBytes)));
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kBarCount);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const uint32_t smem0 = smem_u32(smem);
   const uint32_t bar0 = smem_u32(bars);
   auto full_bar = [&](int s) { return bar0 + 8u * s; };
-  auto empty_bar = [&](int s) { return bar0 + 8u * (kStages + s); };
-  auto tfull_bar = [&](int b) { return bar0 + 8u * (2 * kStages + b); };
-  auto tempty_bar = [&](int b) { return bar0 + 8u * (2 * kStages + 2 + b); };
-  const uint32_t done_bar = bar0 + 8u * (2 * kStages + 4);
+  auto empty_bar = [&](int s) { return bar0 + 8u * (kOpStages + s); };
+  auto tfull_bar = [&](int b) { return bar0 + 8u * (2 * kOpStages + b); };
+  auto tempty_bar = [&](int b) { return bar0 + 8u * (2 * kOpStages + 2 + b); };
+  const uint32_t done_bar = bar0 + 8u * (2 * kOpStages + 4);
+  // raw ring (kFused): rfull = the TMA's bytes landed, rempty = converted
+  auto rfull_bar = [&](int r) { return bar0 + 8u * (2 * kOpStages + 5 + r); };
+  auto rempty_bar = [&](int r) { return bar0 + 8u * (2 * kOpStages + 5 + kRawStages + r); };
+  auto raw_addr = [&](int r) {
+    return smem0 + uint32_t(kOpStages * kStageBytes + r * kRawStageBytes);
+  };
   // plane p of stage s: 0 = Re_j, 1 = Im_j, 2 = Re_i, 3 = Im_i
   auto plane_addr = [&](int s, int p) {
     return smem0 + uint32_t(s * kStageBytes + p * kPlaneBytes);
@@ -404,8 +419,8 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
   const int lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(full_bar(s), 1);
+    for (int s = 0; s < kOpStages; ++s) {
+      mbar_init(full_bar(s), kFused ? kConvThreads : 1);  // converter threads or the TMA
       mbar_init(empty_bar(s), 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -413,6 +428,12 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       mbar_init(tempty_bar(b), kEpiWarps);
     }
     mbar_init(done_bar, 1);
+    if (kFused) {
+      for (int r = 0; r < kRawStages; ++r) {
+        mbar_init(rfull_bar(r), 1);
+        mbar_init(rempty_bar(r), kConvThreads);
+      }
+    }
     *abort_flag = 0;
     fence_mbar_init();
   }
@@ -428,7 +449,49 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
 
   if (warp == 0) {
     // ------------------------------------------------ TMA producer
-    if (lane == 0) {
+    if (kFused && lane == 0) {
+      // raw QC tiles: the j block's 128 rows, then (off the diagonal) the i
+      // block's, 128 bytes (samples) each; bytes past K arrive as zeros
+      int r = 0;
+      uint32_t rph = 0;
+      int issued = 0;
+      bool ok = true;
+      for (TileWalk w(args.tiles, args.chans, args.num_tiles, blockIdx.x, gridDim.x);
+           w.valid() && ok; w.advance()) {
+        const TileDesc td = w.td;
+        const ChanDesc cd = w.cd;
+        const int32_t rowJ = int32_t(cd.row0 + int64_t(td.tj) * kTile);
+        const int32_t rowI = int32_t(cd.row0 + int64_t(td.ti) * kTile);
+        const bool diag = td.ti == td.tj;
+        for (int kb = 0; kb < cd.kblocks; ++kb) {
+          if (!mbar_wait(rempty_bar(r), rph ^ 1u, abort_flag)) {
+            atomicOr(args.status, kStatusTimeoutProducer);
+            ok = false;
+            break;
+          }
+          const int32_t x = (cd.kb0 + kb) * kStageK;
+          mbar_arrive_expect_tx(rfull_bar(r), diag ? kPlaneBytes : 2 * kPlaneBytes);
+          tma_load_2d(raw_addr(r), &tmZ, x, rowJ, rfull_bar(r));
+          if (!diag) tma_load_2d(raw_addr(r) + kPlaneBytes, &tmZ, x, rowI, rfull_bar(r));
+          ++issued;
+          if (++r == kRawStages) {
+            r = 0;
+            rph ^= 1u;
+          }
+        }
+      }
+      if (!ok) {
+        // Let every load still in flight land before the CTA exits.
+        for (int n = 0; n < kRawStages && n < issued; ++n) {
+          if (--r < 0) {
+            r = kRawStages - 1;
+            rph ^= 1u;
+          }
+          volatile int never = 0;
+          if (!mbar_wait(rfull_bar(r), rph, &never)) atomicOr(args.status, kStatusTimeoutOther);
+        }
+      }
+    } else if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
       int issued = 0;
@@ -534,7 +597,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
             mma_f8f6f4(d_im, daim, dbre, idesc_neg, 1);     // Im -= Im_j Re_i
           }
           mma_commit(empty_bar(stage));
-          if (++stage == kStages) {
+          if (++stage == kOpStages) {
             stage = 0;
             phase ^= 1u;
           }
@@ -551,7 +614,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       volatile int never = 0;
       if (!mbar_wait(done_bar, 0, &never)) atomicOr(args.status, kStatusTimeoutOther);
     }
-  } else {
+  } else if (warp < 2 + kEpiWarps) {
     // ------------------------------------------------ epilogue warps
     // Warp w may read TMEM lanes 32*(w%4)..+31 (columns j); the four warps
     // of a half own rows [64h, 64h+64) of the tile and sync on barrier 1+h.
@@ -585,7 +648,7 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       const int ib = int(td.ti) * kTile;
       const uint32_t tb = tmem_base + (uint32_t(q * 32) << 16) + uint32_t(acc * kAccCols);
       Out2* outc = cd.out_ptr ? reinterpret_cast<Out2*>(cd.out_ptr) : out + cd.out0;
-      if (kBulkOut && args.bulk_store && plain && td.ti != td.tj && ib + kTile <= n) {
+      if (!kFused && kBulkOut && args.bulk_store && plain && td.ti != td.tj && ib + kTile <= n) {
         // Interior tile: stage kStgRows row segments (128 consecutive packed
         // elements each) in shared memory, then one bulk copy per row.  A
         // row whose global start is 8 mod 16 keeps that phase in shared
@@ -698,6 +761,64 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
       }
     }
     if (issuer) bulk_wait<0>();  // bulk stores complete before the CTA exits
+  } else if (kFused) {
+    // ------------------------------------------------ converter warps (kFused)
+    // Per stage: 2048 16-byte chunks (1024 on the diagonal).  Chunk
+    // q * 128 + ct (q < 16) is row q * 16 + (ct >> 3) (rows 128-255 = the i
+    // block) and 16-byte column ct & 7; a warp's load covers 4 whole raw rows.
+    // In the 128-byte swizzled layout, column c of row r sits at
+    // r * 128 + ((c ^ (r & 7)) << 4) of its plane; r & 7 = (ct >> 3) & 7 for
+    // every q, so each chunk's source and destination are this thread's base
+    // plus a constant.  All loads of a stage are issued before any convert.
+    const int ct = threadIdx.x - 32 * (2 + kEpiWarps);
+    const int src_t = 16 * ct;
+    const int dst_t = (ct >> 3) * 128 + (((ct & 7) ^ ((ct >> 3) & 7)) << 4);
+    int r = 0, stage = 0;
+    uint32_t rph = 0, phase = 0;
+    bool ok = true;
+    for (TileWalk w(args.tiles, args.chans, args.num_tiles, blockIdx.x, gridDim.x);
+         w.valid() && ok; w.advance()) {
+      const bool diag = w.td.ti == w.td.tj;  // i block == j block: 8 chunks each
+      for (int kb = 0; kb < w.cd.kblocks; ++kb) {
+        if (!mbar_wait(rfull_bar(r), rph, abort_flag) ||
+            !mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
+          atomicOr(args.status, kStatusTimeoutOther);
+          ok = false;
+          break;
+        }
+        const uint8_t* src = smem + (raw_addr(r) - smem0) + src_t;
+        uint8_t* dst = smem + (plane_addr(stage, 0) - smem0) + dst_t;
+        uint4 v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          if (q < 8 || !diag) v[q] = *reinterpret_cast<const uint4*>(src + q * 2048);
+        mbar_arrive(rempty_bar(r));  // the raw stage is in registers: refill it
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          if (q < 8 || !diag) {
+            uint4 re, im;
+            qc4_to_e4m3(v[q].x, re.x, im.x);
+            qc4_to_e4m3(v[q].y, re.y, im.y);
+            qc4_to_e4m3(v[q].z, re.z, im.z);
+            qc4_to_e4m3(v[q].w, re.w, im.w);
+            // rows 0-127: planes 0 / 1 (Re_j / Im_j); 128-255: planes 2 / 3
+            const int off = (q & 7) * 2048 + (q >> 3) * 2 * kPlaneBytes;
+            *reinterpret_cast<uint4*>(dst + off) = re;
+            *reinterpret_cast<uint4*>(dst + off + kPlaneBytes) = im;
+          }
+        }
+        fence_proxy_async_smem();  // the planes are read by the tensor core
+        mbar_arrive(full_bar(stage));
+        if (++r == kRawStages) {
+          r = 0;
+          rph ^= 1u;
+        }
+        if (++stage == kOpStages) {
+          stage = 0;
+          phase ^= 1u;
+        }
+      }
+    }
   }
 
   tc_fence_before();
@@ -722,7 +843,8 @@ __global__ void __launch_bounds__(kHerkThreads, 1)
 // N = 128: each MMA reads half as many operand bytes per multiply-add from
 // shared memory, which bounds the single-CTA kernel.  The leader CTA (rank 0)
 // owns the full barriers (the partner's loads count their bytes there) and
-// issues the MMAs; each commit is sent to the matching barrier of both CTAs;
+// issues the MMAs; each commit arrives on the matching barrier of both CTAs
+// (one multicast commit);
 // both CTAs' epilogue warps release an accumulator on the leader's barrier.
 constexpr int kPairPlane = 128 * kStageK;  // 16 KB: 128 rows of 128 samples
 constexpr int kPairStageBytes = 4 * kPairPlane;
@@ -862,16 +984,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kHerkThreads, 1)
               mma_f8f6f4_pair(d, daim, dby, idesc, 1);
             }
           }
-          mma_commit_pair(empty_bar(stage));
-          mma_commit_pair(map_shared(empty_bar(stage), 1));
+          mma_commit_pair_both(empty_bar(stage));
           if (++stage == kPairStages) {
             stage = 0;
             phase ^= 1u;
           }
         }
         if (!ok) break;
-        mma_commit_pair(tfull_bar(acc));
-        mma_commit_pair(map_shared(tfull_bar(acc), 1));
+        mma_commit_pair_both(tfull_bar(acc));
         if (++acc == 2) {
           acc = 0;
           acc_phase ^= 1u;
@@ -1116,13 +1236,15 @@ cudaError_t launch_gather_qc_to_planes(const GatherDesc* g, int nch, int max_n, 
   return cudaGetLastError();
 }
 
-template <typename OutT>
+template <typename OutT, bool kFused>
 static cudaError_t launch_herk_t(const CUtensorMap& tmZ, const HerkArgs& a, int grid,
                                  cudaStream_t s) {
+  constexpr size_t smem = kFused ? kFusedSmem : kHerkSmem;
+  constexpr int threads = kFused ? kFusedThreads : kHerkThreads;
   cudaError_t e =
-      ensure_smem_limit(reinterpret_cast<const void*>(herk_fp8_tc_kernel<OutT>), kHerkSmem);
+      ensure_smem_limit(reinterpret_cast<const void*>(herk_fp8_tc_kernel<OutT, kFused>), smem);
   if (e != cudaSuccess) return e;
-  herk_fp8_tc_kernel<OutT><<<grid, kHerkThreads, kHerkSmem, s>>>(tmZ, a);
+  herk_fp8_tc_kernel<OutT, kFused><<<grid, threads, smem, s>>>(tmZ, a);
   return cudaGetLastError();
 }
 
@@ -1210,7 +1332,16 @@ cudaError_t launch_split_reduce(const float2* ws, void* out, int out_fp16, int64
 }
 
 cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s) {
-  return a.out_fp16 ? launch_herk_t<__half>(tmZ, a, grid, s) : launch_herk_t<float>(tmZ, a, grid, s);
+  return a.out_fp16 ? launch_herk_t<__half, false>(tmZ, a, grid, s)
+                    : launch_herk_t<float, false>(tmZ, a, grid, s);
+}
+
+cudaError_t launch_herk_fp8_fused(const CUtensorMap& tmQ, const HerkArgs& a, int grid,
+                                  cudaStream_t s) {
+  if (a.nseg != 1 || a.out_format != 0 || a.bulk_store || a.fp6 || a.s8)
+    return cudaErrorInvalidValue;
+  return a.out_fp16 ? launch_herk_t<__half, true>(tmQ, a, grid, s)
+                    : launch_herk_t<float, true>(tmQ, a, grid, s);
 }
 
 }  // namespace ftdx

@@ -39,6 +39,20 @@ constexpr int kStgRowBytes = kTile * 8 + 16;
 constexpr int kStgBytes = 2 /*halves*/ * 2 /*buffers*/ * kStgRows * kStgRowBytes;
 constexpr size_t kHerkSmem = 1024 + size_t(kStages) * kStageBytes + kStgBytes + 256;
 static_assert(((kTile / 2) / kStgRows) % 2 == 0, "bulk tiles end on staging buffer 1");
+// Fused promotion (store-mode flag kStoreFused, QC input): the producer loads
+// raw QC bytes by TMA and kConvWarps converter warps write the E4M3 operand
+// planes into shared memory, so no operand planes exist in HBM.  Two operand
+// stages and three raw stages (128 A rows + 128 B rows of 128 QC bytes); no
+// bulk-store staging.
+constexpr int kConvWarps = 4;
+constexpr int kConvThreads = 32 * kConvWarps;
+constexpr int kFusedThreads = kHerkThreads + kConvThreads;
+constexpr int kFusedStages = 2;
+constexpr int kRawStages = 3;
+constexpr int kRawStageBytes = 2 * kPlaneBytes;
+constexpr size_t kFusedSmem =
+    1024 + size_t(kFusedStages) * kStageBytes + size_t(kRawStages) * kRawStageBytes + 256;
+static_assert(kFusedSmem <= 232448, "shared memory per CTA");
 
 // One lower-triangle tile: channel, row block ti (i), column block tj (j), tj <= ti.
 struct TileDesc {
@@ -197,6 +211,11 @@ cudaError_t launch_gather_qc_to_planes(const GatherDesc* g, int nch, int max_n, 
                                        int64_t total_rows, int Kp, cudaStream_t s,
                                        int neg_plane = 0);
 cudaError_t launch_herk_fp8(const CUtensorMap& tmZ, const HerkArgs& a, int grid, cudaStream_t s);
+// The single-CTA kernel with fused promotion: tmQ maps the raw QC bytes
+// [rows][K] (2-D, 128 x 128-byte boxes, no swizzle); a.nseg must be 1,
+// a.out_format 0 and a.bulk_store 0.
+cudaError_t launch_herk_fp8_fused(const CUtensorMap& tmQ, const HerkArgs& a, int grid,
+                                  cudaStream_t s);
 // Split-K reduction: C[c] = alpha * cs_c * sum_s ws[c*splits + s] + beta * C[c].
 cudaError_t launch_split_reduce(const float2* ws, void* out, int out_fp16, int64_t P, int batch,
                                 int splits, float alpha, float beta, const float* chan_scale,

@@ -100,8 +100,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(128, 1)
       const uint32_t idesc = (1u << 7) | (1u << 10) | ((256u >> 3) << 17) | ((256u >> 4) << 24);
       for (int it = 0; it < iters; ++it) dev::mma_nvf4_pair(tmem, a, b, idesc, sfa, sfb, it > 0);
     }
-    dev::mma_commit_pair(dev::smem_u32(bar));
-    dev::mma_commit_pair(dev::map_shared(dev::smem_u32(bar), 1));
+    dev::mma_commit_pair_both(dev::smem_u32(bar));
   }
   // every thread of both CTAs waits for the MMAs (bounded)
   volatile int never = 0;

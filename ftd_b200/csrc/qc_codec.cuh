@@ -7,18 +7,19 @@ namespace ftdx {
 
 // Four QC bytes -> E4M3 bytes of the four Re parts and of the four Im parts.
 // Sign-magnitude nibble: bit 3 sign, bits 2:0 magnitude (0..7).  E4M3 codes of
-// the integers 0..7 are 00 38 40 44 48 4A 4C 4E; a byte permute indexed by the
-// magnitude looks them up, the sign goes to bit 7.
+// the integers 0..7 are 00 38 40 44 48 4A 4C 4E.  The magnitude nibbles of two
+// bytes (Im0, Re0, Im1, Re1, low to high) are the four selectors of one byte
+// permute over that table, giving the codes of two samples interleaved; two
+// more permutes split them into the Re and the Im word, and each sign goes to
+// bit 7 (Re: bit 7 of the byte already; Im: bit 3, shifted up by 4).
 __device__ __forceinline__ void qc4_to_e4m3(uint32_t w, uint32_t& re, uint32_t& im) {
   constexpr uint32_t kLo = 0x44403800u, kHi = 0x4E4C4A48u;
-  const uint32_t mr = (w >> 4) & 0x07070707u;
-  const uint32_t mi = w & 0x07070707u;
-  uint32_t sr = mr | (mr >> 4);
-  sr = (sr & 0xFFu) | ((sr >> 8) & 0xFF00u);
-  uint32_t si = mi | (mi >> 4);
-  si = (si & 0xFFu) | ((si >> 8) & 0xFF00u);
-  re = __byte_perm(kLo, kHi, sr) | (w & 0x80808080u);
-  im = __byte_perm(kLo, kHi, si) | ((w << 4) & 0x80808080u);
+  const uint32_t m = w & 0x77777777u;
+  // a byte permute reads only the low 16 bits (four selectors) of its selector
+  const uint32_t c01 = __byte_perm(kLo, kHi, m);        // Im0 Re0 Im1 Re1
+  const uint32_t c23 = __byte_perm(kLo, kHi, m >> 16);  // Im2 Re2 Im3 Re3
+  re = __byte_perm(c01, c23, 0x7531u) | (w & 0x80808080u);
+  im = __byte_perm(c01, c23, 0x6420u) | ((w << 4) & 0x80808080u);
 }
 
 // Four QC bytes -> FP6 E3M2 codes (one per byte, bits 5:0) of the four Re

@@ -270,6 +270,15 @@ __device__ __forceinline__ void mma_commit_pair(uint32_t bar_cluster) {
                    bar_cluster)
                : "memory");
 }
+// One commit that arrives on the mbarrier at the same shared-memory offset
+// `bar` (a CTA-local address) in both CTAs of the pair.
+__device__ __forceinline__ void mma_commit_pair_both(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+      " [%0], %1;" ::"r"(bar),
+      "h"(uint16_t(3))
+      : "memory");
+}
 
 // ---------------------------------------------------------------- tcgen05
 __device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {

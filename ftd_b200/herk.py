@@ -238,8 +238,10 @@ class Correlator:
     def set_strategy(self, store_mode: int = 0, grid: int = 0, splits: int | None = None) -> None:
         """Strategy of untuned calls (ftdx_set_strategy): store_mode 0 direct,
         1 bulk, 2 CTA pair, 3 CTA pair with bulk stores; + 4 FP6 operands,
-        2 / 3 + 8 the pair on INT8 operands (INT4 input).  grid=-1 is a plain one-tile-per-CTA launch; splits = split-K
-        ranges (None leaves it unchanged)."""
+        2 / 3 + 8 the pair on INT8 operands (INT4 input); 16 the single-CTA
+        kernel with the INT4 promotion fused into it.  grid=-1 is a plain
+        one-tile-per-CTA launch; splits = split-K ranges (None leaves it
+        unchanged)."""
         check(self._h, self._L.ftdx_set_strategy(self._h, store_mode, grid), "ftdx_set_strategy")
         if splits is not None:
             check(self._h, self._L.ftdx_set_split_k(self._h, splits), "ftdx_set_split_k")

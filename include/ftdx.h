@@ -337,12 +337,18 @@ FTDX_API int ftdx_graph_count(ftdx_handle h);
  * + 4 = operands as packed FP6 E3M2 planes (INT4 input; exact);
  * 2 + 8, 3 + 8 = CTA-pair kernel on signed 8-bit operands (kind::i8, S32
  * accumulation; uniform INT4 input; exact; ftdx_herk_batched_v runs these
- * as 2 and 3 on E4M3 operands).  For NVFP4 compute, store_mode 2 selects
- * the NVFP4 CTA-pair kernel and 0 / 1 the single-CTA one.
+ * as 2 and 3 on E4M3 operands);
+ * 16 = the single-CTA kernel with the INT4 -> E4M3 promotion fused into it:
+ * raw QC bytes are loaded by the correlator and converted in shared memory,
+ * so no operand planes are written to or read from HBM and no workspace is
+ * allocated for them (uniform INT4 calls with FP8 compute, K a multiple of 16
+ * and A 16-byte aligned; other calls run as 0; not combinable with 4 or 8).
+ * For NVFP4 compute, store_mode 2 selects the NVFP4 CTA-pair kernel and 0 / 1
+ * the single-CTA one.
  * grid > 0 = that many persistent CTAs (capped at one per SM; even and capped
  * at the co-resident pairs for store_mode 2), 0 = one per SM, -1 = one CTA
  * (pair) per tile (a plain, non-persistent launch).  The tuner also times
- * store_mode 2, 3, 2 + 8 and 3 + 8 for uniform INT4 calls, 2 and 3 for
+ * store_mode 2, 3, 2 + 8, 3 + 8 and 16 for uniform INT4 calls, 2 and 3 for
  * ftdx_herk_batched_v, and both NVFP4 kernels. */
 FTDX_API ftdx_status ftdx_set_strategy(ftdx_handle h, int store_mode, int grid);
 

@@ -166,10 +166,10 @@ def test_strategies_under_graph_replay(mode):
         assert c.graph_count() >= 1 and c.device_status() == 0
 
 
-@pytest.mark.parametrize("bad", [-1, 9, 12, 13, 14, 15, 16, 32, 2 + 8 + 4])
+@pytest.mark.parametrize("bad", [-1, 9, 12, 13, 14, 15, 17, 18, 20, 24, 32, 2 + 8 + 4])
 def test_invalid_store_modes_refused(bad):
     # 8 (int8 operands) only with the pair modes 2 / 3, never with 4 (FP6);
-    # no bits above 8
+    # 16 (fused promotion) only alone; no bits above 16
     with Correlator() as c:
         with pytest.raises(FtdxError):
             c.set_strategy(bad, 0)

@@ -119,8 +119,8 @@ def test_fp16_input(corr):
 
 # None: the autotuner's choice on this GPU; then every strategy it can pick
 # for QC input: 1 single CTA + bulk stores, 2 CTA pair, 3 pair + bulk stores,
-# 10 / 11 the pair on int8 operands
-@pytest.mark.parametrize("strategy", [None, 1, 2, 3, 10, 11])
+# 10 / 11 the pair on int8 operands, 16 promotion fused into the single CTA
+@pytest.mark.parametrize("strategy", [None, 1, 2, 3, 10, 11, 16])
 def test_dsa2000_scale_spot_rows(strategy):
     # 4096 inputs x 64 channels x K = 1024 (the DSA-2000 configuration): full
     # output on the GPU, exact check of two whole channels, of row blocks in
@@ -165,3 +165,58 @@ def test_ggp_entry_point(corr):
     assert herk_batched_cutlass_qc(qc, C, N, K, B) == 0
     torch.cuda.synchronize()
     assert np.array_equal(C.cpu().numpy(), oracle.herk_qc(qc_np, N, K, B).astype(np.float32))
+
+
+# Promotion fused into the correlator (strategy 16): raw QC tiles by TMA,
+# converted to E4M3 in shared memory.  Bit-exact against the oracle, over
+# ragged N (partial tiles, channel rows running into the next channel's),
+# K tails that are multiples of 16 but not of 128 (zeros from the TMA past K),
+# K = 16, alpha / beta, FP16 output, split-K; and calls it cannot take (K not
+# a multiple of 16, A not 16-byte aligned) run the two-pass path and stay exact.
+@pytest.mark.parametrize("N,K,B", [(200, 208, 3), (128, 1024, 2), (300, 16, 2), (64, 48, 5),
+                                   (260, 100, 2)])
+def test_fused_promotion_exact(N, K, B):
+    qc = oracle.gaussian_qc(4000 + N + K, B, N, K)
+    ref = oracle.herk_qc(qc, N, K, B).astype(np.float32)
+    with Correlator() as c:
+        c.set_strategy(16, 0)
+        got = run_qc(c, qc, N, K, B).cpu().numpy()
+        assert c.device_status() == 0
+    assert np.array_equal(got, ref)
+
+
+def test_fused_promotion_options():
+    N, K, B = 192, 320, 3
+    qc = oracle.gaussian_qc(4100, B, N, K)
+    ref = oracle.herk_qc(qc, N, K, B)
+    with Correlator() as c:
+        c.set_strategy(16, 0)
+        # FP16 output: the FP32 result rounded to nearest
+        h = run_qc(c, qc, N, K, B, out=OUT_FP16).cpu().numpy()
+        assert np.array_equal(h, ref.astype(np.float32).astype(np.float16))
+        # alpha and beta
+        old = torch.randn(B, tri_size(N), 2, device=DEV)
+        C = old.clone()
+        run_qc(c, qc, N, K, B, alpha=0.5, beta=-2.0, C=C)
+        want = 0.5 * ref.astype(np.float64) + (-2.0) * old.double().cpu().numpy()
+        np.testing.assert_allclose(C.double().cpu().numpy(), want, rtol=1e-6, atol=1e-4)
+        # split-K into 3 ranges, exact
+        c.set_strategy(16, 0, splits=3)
+        got = run_qc(c, qc, N, K, B).cpu().numpy()
+        assert np.array_equal(got, ref.astype(np.float32))
+        assert c.device_status() == 0
+
+
+def test_fused_promotion_falls_back_when_misaligned():
+    N, K, B = 96, 64, 2
+    qc = oracle.gaussian_qc(4200, B, N, K)
+    buf = torch.zeros(qc.size + 16, dtype=torch.uint8, device=DEV)
+    A = buf[1:1 + qc.size]  # 1 byte past a 16-byte boundary
+    A.copy_(torch.from_numpy(qc.reshape(-1)).to(DEV))
+    C = torch.full((B, tri_size(N), 2), float("nan"), device=DEV)
+    with Correlator() as c:
+        c.set_strategy(16, 0)
+        c.herk(A, C, N, K, B, input=IN_INT4, output=OUT_FP32, tune=False)
+        torch.cuda.synchronize()
+        assert c.device_status() == 0
+    assert np.array_equal(C.cpu().numpy(), oracle.herk_qc(qc, N, K, B).astype(np.float32))

@@ -25,7 +25,7 @@ def test_tune_writes_and_reloads_cache(tmp_path):
     with Correlator(tune_cache=path) as c:
         assert c.lookup_tuned(N, K, B) is None
         win = c.tune(d, C, N, K, B)
-        assert win["store_mode"] in (0, 1, 2, 3, 10, 11) and win["ms"] > 0
+        assert win["store_mode"] in (0, 1, 2, 3, 10, 11, 16) and win["ms"] > 0
         assert c.lookup_tuned(N, K, B)["store_mode"] == win["store_mode"]
         torch.cuda.synchronize()
         # the sweep leaves a correct result behind
