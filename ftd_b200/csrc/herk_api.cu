@@ -768,9 +768,10 @@ ftdx_status ftdx_herk_kahan(ftdx_handle h, const void* A, void* sum, void* comp,
   cudaError_t e = cudaSetDevice(h->device);
   if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
   // Read-modify-write of sum and compensation: no tuning sweep (it would
-  // accumulate the same dump several times); direct stores only.
+  // accumulate the same dump several times); direct stores only (the
+  // single-CTA kernel, two-pass or with the promotion fused in).
   Strategy strat = h->default_strategy;
-  strat.store_mode = 0;
+  if (strat.store_mode != kStoreFused) strat.store_mode = 0;
   return launch_all(h, c, strat, static_cast<cudaStream_t>(stream));
 }
 

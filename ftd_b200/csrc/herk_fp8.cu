@@ -329,21 +329,21 @@ __device__ __forceinline__ void store_chunk_xengine(Out2* ob, int i0, int j, int
   }
 }
 
-template <typename Out2>
+template <int R, typename Out2>
 __device__ __forceinline__ void store_chunk(Out2* p, float2* pc, int i0, int j, int n, bool full,
                                             float sc, const HerkArgs& args,
-                                            const uint32_t (&re)[32], const uint32_t (&im)[32]) {
+                                            const uint32_t (&re)[R], const uint32_t (&im)[R]) {
   const bool general = args.kahan || args.beta != 0.f;
   if (full && !general) {
     if (sc == 1.f) {
 #pragma unroll
-      for (int m = 0; m < 32; ++m) {
+      for (int m = 0; m < R; ++m) {
         put(p, __uint_as_float(re[m]), __uint_as_float(im[m]));
         p += i0 + m + 1;
       }
     } else {
 #pragma unroll
-      for (int m = 0; m < 32; ++m) {
+      for (int m = 0; m < R; ++m) {
         put(p, __uint_as_float(re[m]) * sc, __uint_as_float(im[m]) * sc);
         p += i0 + m + 1;
       }
@@ -351,7 +351,7 @@ __device__ __forceinline__ void store_chunk(Out2* p, float2* pc, int i0, int j, 
     return;
   }
 #pragma unroll
-  for (int m = 0; m < 32; ++m) {
+  for (int m = 0; m < R; ++m) {
     const int i = i0 + m;
     if (i < n && j <= i) {
       float vr = __uint_as_float(re[m]) * sc;
@@ -688,7 +688,7 @@ __global__ void __launch_bounds__(kFused ? kFusedThreads : kHerkThreads, 1)
           }
           named_bar_sync(bar_id, 128);
         }
-      } else if (args.out_format == 1) {
+      } else if (!kFused && args.out_format == 1) {
         // Packed upper triangle, row-major (the XEngine's format): the producer
         // swapped the blocks, so TMEM lane = column c (the i block) and TMEM
         // column = row r (the j block), and the accumulator holds
@@ -735,6 +735,24 @@ __global__ void __launch_bounds__(kFused ? kFusedThreads : kHerkThreads, 1)
           const int c = half * kChunks + cc;
           const int i0 = ib + 32 * c;
           if (i0 + 31 < jw || i0 >= n) continue;  // warp-uniform: nothing to store
+          if constexpr (kFused) {
+            // 16 rows at a time: the fused kernel's 448 threads get 128 registers
+#pragma unroll 1
+            for (int hr = 0; hr < 2; ++hr) {
+              const int i0h = i0 + 16 * hr;
+              if (i0h + 15 < jw || i0h >= n) continue;  // warp-uniform
+              uint32_t re[16], im[16];
+              __syncwarp();
+              tmem_ld_32x32b_x16(tb + 32u * c + 16u * hr, re);
+              tmem_ld_32x32b_x16(tb + uint32_t(kTile) + 32u * c + 16u * hr, im);
+              tmem_wait_ld();
+              const int64_t e0 = int64_t(i0h) * (i0h + 1) / 2 + j;
+              float2* pc = args.kahan ? static_cast<float2*>(args.out2) + cd.out0 + e0 : nullptr;
+              store_chunk(outc + e0, pc, i0h, j, n, i0h + 15 < n && jw + 31 < i0h, sc, args, re,
+                          im);
+            }
+            continue;
+          }
           uint32_t re[32], im[32];
           __syncwarp();
           tmem_ld_32x32b_x32(tb + 32u * c, re);
@@ -788,25 +806,28 @@ __global__ void __launch_bounds__(kFused ? kFusedThreads : kHerkThreads, 1)
         }
         const uint8_t* src = smem + (raw_addr(r) - smem0) + src_t;
         uint8_t* dst = smem + (plane_addr(stage, 0) - smem0) + dst_t;
-        uint4 v[16];
+        // two halves of 8 chunks (the j block's rows, then the i block's)
 #pragma unroll
-        for (int q = 0; q < 16; ++q)
-          if (q < 8 || !diag) v[q] = *reinterpret_cast<const uint4*>(src + q * 2048);
-        mbar_arrive(rempty_bar(r));  // the raw stage is in registers: refill it
+        for (int hb = 0; hb < 2; ++hb) {
+          if (hb == 1 && diag) break;
+          uint4 v[8];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          if (q < 8 || !diag) {
+          for (int q = 0; q < 8; ++q)
+            v[q] = *reinterpret_cast<const uint4*>(src + (hb * 8 + q) * 2048);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
             uint4 re, im;
             qc4_to_e4m3(v[q].x, re.x, im.x);
             qc4_to_e4m3(v[q].y, re.y, im.y);
             qc4_to_e4m3(v[q].z, re.z, im.z);
             qc4_to_e4m3(v[q].w, re.w, im.w);
             // rows 0-127: planes 0 / 1 (Re_j / Im_j); 128-255: planes 2 / 3
-            const int off = (q & 7) * 2048 + (q >> 3) * 2 * kPlaneBytes;
+            const int off = q * 2048 + hb * 2 * kPlaneBytes;
             *reinterpret_cast<uint4*>(dst + off) = re;
             *reinterpret_cast<uint4*>(dst + off + kPlaneBytes) = im;
           }
         }
+        mbar_arrive(rempty_bar(r));  // every raw chunk has been read
         fence_proxy_async_smem();  // the planes are read by the tensor core
         mbar_arrive(full_bar(stage));
         if (++r == kRawStages) {

@@ -220,3 +220,30 @@ def test_fused_promotion_falls_back_when_misaligned():
         torch.cuda.synchronize()
         assert c.device_status() == 0
     assert np.array_equal(C.cpu().numpy(), oracle.herk_qc(qc, N, K, B).astype(np.float32))
+
+
+def test_fused_promotion_kahan_and_graph_replay():
+    # Kahan accumulation over three dumps, and graph replay with new voltages
+    # in the same buffers: the fused kernel reads the QC bytes at every replay.
+    N, K, B = 256, 192, 2
+    dumps = [oracle.gaussian_qc(4300 + i, B, N, K) for i in range(3)]
+    want = sum(oracle.herk_qc(q, N, K, B) for q in dumps).astype(np.float32)
+    with Correlator() as c:
+        c.set_strategy(16, 0)
+        S = torch.zeros(B, tri_size(N), 2, device=DEV)
+        comp = torch.zeros_like(S)
+        for q in dumps:
+            c.herk_kahan(torch.from_numpy(q.reshape(-1)).to(DEV), S, comp, N, K, B,
+                         input=IN_INT4)
+        torch.cuda.synchronize()
+        assert np.array_equal(S.cpu().numpy(), want)
+        c.set_graph_mode(True)
+        A = torch.empty(B * N * K, dtype=torch.uint8, device=DEV)
+        C = torch.empty(B, tri_size(N), 2, device=DEV)
+        for q in dumps:
+            A.copy_(torch.from_numpy(q.reshape(-1)).to(DEV))
+            C.fill_(float("nan"))
+            c.herk(A, C, N, K, B, input=IN_INT4, output=OUT_FP32, tune=False)
+            torch.cuda.synchronize()
+            assert np.array_equal(C.cpu().numpy(), oracle.herk_qc(q, N, K, B).astype(np.float32))
+        assert c.graph_count() >= 1 and c.device_status() == 0
