@@ -601,7 +601,9 @@ def run_ours(args, rank, world, dist):
         "config": {"workload": f"DSA-2000 correlator: {N} inputs x {B} channels x K={K}, "
                                f"QC int4 -> packed complex64 lower triangle",
                    "inputs": N, "channels": B, "k": K, "per_gpu_channels": B,
-                   "l2": "inputs (268 MB) and outputs (4.3 GB) exceed L2; no flush needed",
+                   "l2": (f"inputs {B * N * K / 1e6:.0f} MB, outputs {B * P * 8 / 1e9:.2f} GB "
+                          f"({'both exceed' if B * N * K > 126e6 else 'the outputs exceed'} "
+                          f"the 126 MB L2); no flush needed"),
                    "parallelism": f"replicas x{world} (independent channels)"},
         "roofline": {"bound": "tensor", "achieved": achieved,
                      "peak": peak, "unit": UNIT,
