@@ -228,6 +228,89 @@ def run_reference_direct_leg(torch, dev, qc, C_ours, N, K, B, steps):
             "bit_exact_vs_library": same}
 
 
+def load_reference_api():
+    """The reference's own public HERK API (cutlass_gemm_api::CutlassComplexGemm,
+    its CUTLASS tcgen05 sub-GEMM baseline and direct kernels), compiled
+    unmodified from its sources by baseline/build_cutlass_ref.sh into
+    baseline/_ref/, or None when it was not built."""
+    import ctypes
+    path = os.path.join(ROOT, "baseline", "_ref", "libref_cutlass_api.so")
+    if not os.path.exists(path):
+        return None
+    L = ctypes.CDLL(path)
+    vp, i = ctypes.c_void_p, ctypes.c_int
+    L.ref_api_create.restype = vp
+    L.ref_api_destroy.argtypes = [vp]
+    L.ref_api_init_herk.restype = i
+    L.ref_api_init_herk.argtypes = [vp, i, i, i, vp]
+    L.ref_api_herk_qc_fp32.restype = i
+    L.ref_api_herk_qc_fp32.argtypes = [vp, vp, vp, i, i, i, i, vp]
+    return L
+
+
+class _StdoutToStderr:
+    """Sends what a C library prints to stdout to stderr meanwhile, so that
+    the bench's stdout stays one JSON line."""
+
+    def __enter__(self):
+        import ctypes
+        sys.stdout.flush()
+        self.libc = ctypes.CDLL(None)
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        self.libc.fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
+def run_reference_api_leg(torch, dev, qc, C_ours, N, K, B, steps):
+    """The reference's GPU HERK through its own public API on the same GPU and
+    resident QC input (INT4 -> FP8 compute -> FP32 packed triangles, tune =
+    false): its default K-adaptive dispatch (HerkMode::Auto) and its CUTLASS
+    tcgen05 baseline (HerkMode::ForceBaseline: cast, sub-GEMMs, pack).  Timed
+    with CUDA events after init_herk; triangles compared with the library's."""
+    L = load_reference_api()
+    if L is None:
+        return None
+    import ctypes
+    from ftd_b200 import tri_size
+    stream = torch.cuda.current_stream(dev)
+    out = {"what": "reference cutlass_gemm_api::CutlassComplexGemm::herk, built unmodified "
+                   "from its sources for sm_100a (nvcc 12.9, CUTLASS 4.5 headers, 1x1 clusters)"}
+    with _StdoutToStderr():
+        h = L.ref_api_create()
+        if not h:
+            return {**out, "unavailable": "CutlassComplexGemm construction failed"}
+        try:
+            if L.ref_api_init_herk(h, N, K, B, ctypes.c_void_p(stream.cuda_stream)) != 0:
+                return {**out, "unavailable": "init_herk failed"}
+            C = torch.empty(B, tri_size(N), 2, device=dev)
+            for name, mode in (("auto", 0), ("cutlass_baseline", 2)):
+                def call():
+                    rc = L.ref_api_herk_qc_fp32(h, ctypes.c_void_p(qc.data_ptr()),
+                                                ctypes.c_void_p(C.data_ptr()), N, K, B, mode,
+                                                ctypes.c_void_p(stream.cuda_stream))
+                    if rc != 0:
+                        raise RuntimeError(f"reference herk failed ({rc})")
+                C.fill_(float("nan"))
+                try:
+                    ms = _timed(torch, call, reps=max(3, min(steps, 10)), warm=2)
+                except RuntimeError as e:
+                    out[name] = {"unavailable": str(e)}
+                    continue
+                out[name] = {"value": herk_flops(N, K, B) / (ms * 1e-3) / 1e12, "unit": UNIT,
+                             "ms_per_step": ms, "bit_exact_vs_library": bool(torch.equal(C, C_ours))}
+            del C
+        finally:
+            torch.cuda.synchronize()
+            L.ref_api_destroy(h)
+    return out
+
+
 def run_config1_leg(torch, dev, N=128, K=256, B=32, seed=8):
     """The small plain configuration (64 antennas x 2 pols = 128 inputs, 32
     channels, K = 256): latency of one call, tuned and graph-replayed, and
@@ -536,11 +619,13 @@ def run_ours(args, rank, world, dist):
                          f"no graph, no tuning"}
 
     # --- the reference's own Blackwell direct kernel on the same input
-    ref_direct = None
+    ref_direct = ref_api = None
     if not args.no_plain:
         step()
         torch.cuda.synchronize()
         ref_direct = run_reference_direct_leg(torch, dev, qc, C, N, K, B, args.steps)
+        if world == 1:  # the reference's CUTLASS kernels: one-GPU runs only
+            ref_api = run_reference_api_leg(torch, dev, qc, C, N, K, B, args.steps)
 
     # --- end to end through the C ABI with host buffers
     e2e = None
@@ -630,6 +715,12 @@ def run_ours(args, rank, world, dist):
         "speedup_vs_plain": (value / world / plain["value"]) if plain else None,
         "reference_direct_mma_sync": ref_direct,
         "vs_direct_mma_sync": (value / world / ref_direct["value"]) if ref_direct else None,
+        "reference_api_gpu": ref_api,
+        "vs_reference_api_default": ((value / ref_api["auto"]["value"])
+                                     if ref_api and "value" in ref_api.get("auto", {}) else None),
+        "vs_reference_cutlass_baseline": (
+            (value / ref_api["cutlass_baseline"]["value"])
+            if ref_api and "value" in ref_api.get("cutlass_baseline", {}) else None),
         "e2e": e2e,
         "batched_uneven_flagged": batched,
         "raw_layout_fused_corner_turn": raw_layout,
