@@ -58,4 +58,24 @@ int ref_api_herk_qc_fp32(void* h, const void* A, void* C, int N, int K, int batc
   }
 }
 
+// C = alpha A A^H + beta C through the reference's herk with its other input
+// and output forms: input 0 = interleaved FP16 complex [batch][N][K][2],
+// 1 = QC int4 bytes; output 0 = FP16, 1 = FP32 packed triangles; FP8 compute;
+// mode as above.
+int ref_api_herk(void* h, const void* A, void* C, int N, int K, int batch, int input, int output,
+                 float alpha, float beta, int mode, void* stream) {
+  try {
+    auto* g = static_cast<CutlassComplexGemm*>(h);
+    g->set_herk_mode(mode == 1   ? HerkMode::ForceDirect
+                     : mode == 2 ? HerkMode::ForceBaseline
+                                 : HerkMode::Auto);
+    return g->herk(A, C, N, K, batch, input == 1 ? InputPrecision::INT4 : InputPrecision::FP16,
+                   ComputePrecision::FP8, output == 1 ? OutputPrecision::FP32 : OutputPrecision::FP16,
+                   OutputFormat::PackedTriangle, alpha, beta, static_cast<cudaStream_t>(stream),
+                   false);
+  } catch (...) {
+    return -1;
+  }
+}
+
 }  // extern "C"

@@ -245,6 +245,8 @@ def load_reference_api():
     L.ref_api_init_herk.argtypes = [vp, i, i, i, vp]
     L.ref_api_herk_qc_fp32.restype = i
     L.ref_api_herk_qc_fp32.argtypes = [vp, vp, vp, i, i, i, i, vp]
+    L.ref_api_herk.restype = i
+    L.ref_api_herk.argtypes = [vp, vp, vp, i, i, i, i, i, ctypes.c_float, ctypes.c_float, i, vp]
     return L
 
 

@@ -5,7 +5,9 @@
  * where A_b is an N x K complex voltage matrix (N inputs = antennas x pols,
  * K time samples) and C_b is stored as the packed lower triangle, row-major:
  * element (i, j <= i) at i(i+1)/2 + j, interleaved (re, im), with Im(C_ii)
- * forced to 0 before beta is applied.
+ * forced to 0 before beta is applied (as the reference's direct HERK kernel
+ * does; its CUTLASS baseline path instead zeroes Im(C_ii) after beta, which
+ * differs only when the old C has a non-zero imaginary diagonal).
  *
  * All data pointers are DEVICE pointers owned by the caller.  Work is queued
  * on the caller's stream (`stream` is a cudaStream_t; NULL = legacy default
