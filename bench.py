@@ -701,7 +701,11 @@ def run_ours(args, rank, world, dist):
                      "peak_source": peak_source,
                      "frac_of_nominal_4500": achieved / NOMINAL_FP8_TFLOPS,
                      "tcgen05_probe_peaks": probes,
-                     "frac_of_fp8_probe": (achieved / probes["fp8_e4m3"]) if probes else None},
+                     "frac_of_fp8_probe": (achieved / probes["fp8_e4m3"]) if probes else None,
+                     # against this kernel's own MMA stream on QC-valued operands
+                     "frac_of_own_mma_stream_probe": (
+                         achieved / probes["fp8_qc_data_pair" if (mode & 3) >= 2
+                                           else "fp8_qc_data_single_cta"]) if probes else None},
         "kernels": {kernel_name + "_ms": herk_ms, prep_name + "_ms": prep_ms},
         "gpu_launches": 2 * args.steps,
         "strategy": {"tuned": tuned, "graph_replay": True},
