@@ -313,6 +313,59 @@ def run_reference_api_leg(torch, dev, qc, C_ours, N, K, B, steps):
     return out
 
 
+def run_fp16_output_leg(torch, dev, qc, N, K, B, world):
+    """The DSA-2000 workload with FP16 packed triangles (herkBatchedCutlassQC_FP16's
+    form): half the output bytes of the FP32 line.  Tuned, graph-replayed,
+    CUDA events; beside it (one-GPU runs) the reference's own API on the same
+    output form (default dispatch and CUTLASS baseline), each checked
+    bit-exact against this library's triangles."""
+    import ctypes
+    from ftd_b200 import Correlator, tri_size
+    from ftd_b200._lib import IN_INT4, OUT_FP16
+    C = torch.empty(B, tri_size(N), 2, dtype=torch.float16, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    with Correlator(device=dev.index) as corr:
+        corr.init_herk(N, K, B)
+        corr.tune(qc, C, N, K, B, input=IN_INT4, output=OUT_FP16, stream=stream)
+        corr.set_graph_mode(True)
+        ms = _timed(torch, lambda: corr.herk(qc, C, N, K, B, input=IN_INT4, output=OUT_FP16,
+                                             stream=stream, tune=True), reps=20, warm=3)
+        tuned = corr.lookup_tuned(N, K, B, input=IN_INT4, output=OUT_FP16)
+    flops = herk_flops(N, K, B)
+    out = {"workload": f"{N} inputs x {B} channels x K={K}, QC int4 -> packed FP16 triangles",
+           "value": flops / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms,
+           "output_bytes_per_step": int(C.numel() * 2), "tuned": tuned}
+    L = load_reference_api() if world == 1 else None
+    if L is not None:
+        R = torch.empty_like(C)
+        with _StdoutToStderr():
+            h = L.ref_api_create()
+            try:
+                if h and L.ref_api_init_herk(h, N, K, B, ctypes.c_void_p(stream.cuda_stream)) == 0:
+                    for name, mode in (("reference_default", 0), ("reference_cutlass_baseline", 2)):
+                        def call():
+                            rc = L.ref_api_herk(h, ctypes.c_void_p(qc.data_ptr()),
+                                                ctypes.c_void_p(R.data_ptr()), N, K, B, 1, 0,
+                                                1.0, 0.0, mode, ctypes.c_void_p(stream.cuda_stream))
+                            if rc != 0:
+                                raise RuntimeError(f"reference herk failed ({rc})")
+                        try:
+                            rms = _timed(torch, call, reps=5, warm=2)
+                        except RuntimeError as e:
+                            out[name] = {"unavailable": str(e)}
+                            continue
+                        out[name] = {"value": flops / (rms * 1e-3) / 1e12, "unit": UNIT,
+                                     "ms_per_step": rms,
+                                     "bit_exact_vs_library": bool(torch.equal(R, C))}
+            finally:
+                torch.cuda.synchronize()
+                if h:
+                    L.ref_api_destroy(h)
+        del R
+    del C
+    return out
+
+
 def run_config1_leg(torch, dev, N=128, K=256, B=32, seed=8):
     """The small plain configuration (64 antennas x 2 pols = 128 inputs, 32
     channels, K = 256): latency of one call, tuned and graph-replayed, and
@@ -635,9 +688,10 @@ def run_ours(args, rank, world, dist):
         e2e = run_e2e(torch, args, dev, qc, N, K, B, flops, world, dist)
 
     batched = precision = differentiation = raw_layout = imaging = xengine = splitk = None
-    imaging_visbf = config1 = None
+    imaging_visbf = config1 = fp16_out = None
     if not args.no_extra:
         config1 = run_config1_leg(torch, dev)
+        fp16_out = run_fp16_output_leg(torch, dev, qc, N, K, B, world)
         batched = run_batched_leg(torch, dev)
         raw_layout = run_ftd_leg(torch, dev)
         imaging = run_imaging_leg(torch, dev)
@@ -711,6 +765,7 @@ def run_ours(args, rank, world, dist):
         "strategy": {"tuned": tuned, "graph_replay": True},
         "sustained": sustained,
         "config1_small": config1,
+        "fp16_output": fp16_out,
         "config3_batched_uneven": ({"value": batched["value"], "unit": UNIT,
                                     "ms_per_step": batched["ms_per_step"],
                                     "frac_of_fp8_cublaslt": (batched["value"] / peak)
