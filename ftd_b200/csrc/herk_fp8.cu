@@ -199,9 +199,13 @@ __device__ __forceinline__ uint32_t h2_to_e4m3x2(__half2 h) {
                                              __NV_E4M3));
 }
 
+// With `vec` (uniform: K a multiple of 4 and the input 16-byte aligned) a
+// thread's 8 samples are two 16-byte loads; otherwise, and past K, one
+// sample at a time.
 __global__ void __launch_bounds__(256) fp16_to_planes_kernel(const __half2* __restrict__ a,
                                                              uint8_t* __restrict__ z, int64_t rows,
-                                                             int K, int Kp, int rows_per_block) {
+                                                             int K, int Kp, int rows_per_block,
+                                                             int vec) {
   const int chunks = Kp >> 3;  // 8 samples per thread
   const int64_t r0 = int64_t(blockIdx.x) * rows_per_block;
   const int64_t nrows64 = rows - r0 < rows_per_block ? rows - r0 : rows_per_block;
@@ -212,15 +216,26 @@ __global__ void __launch_bounds__(256) fp16_to_planes_kernel(const __half2* __re
     const int t0 = (l - rl * chunks) << 3;
     const int64_t r = r0 + rl;
     uint32_t re[2], im[2];
+    __half2 hv[8];
+    if (vec && t0 + 8 <= K) {
+      const uint4* p4 = reinterpret_cast<const uint4*>(a + r * K + t0);
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const uint4 v = __ldg(p4 + q);
+        const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int b = 0; b < 4; ++b) hv[4 * q + b] = *reinterpret_cast<const __half2*>(&w4[b]);
+      }
+    } else {
+#pragma unroll
+      for (int b = 0; b < 8; ++b)
+        hv[b] = (t0 + b < K) ? a[r * K + t0 + b] : __floats2half2_rn(0.f, 0.f);
+    }
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       uint32_t pr[4];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int t = t0 + 4 * q + b;
-        const __half2 h = (t < K) ? a[r * K + t] : __floats2half2_rn(0.f, 0.f);
-        pr[b] = h2_to_e4m3x2(h);  // byte 0 Re, byte 1 Im
-      }
+      for (int b = 0; b < 4; ++b) pr[b] = h2_to_e4m3x2(hv[4 * q + b]);  // byte 0 Re, byte 1 Im
       const uint32_t lo = pr[0] | (pr[1] << 16), hi = pr[2] | (pr[3] << 16);
       re[q] = __byte_perm(lo, hi, 0x6420);
       im[q] = __byte_perm(lo, hi, 0x7531);
@@ -1244,8 +1259,9 @@ cudaError_t launch_fp16_to_planes(const void* a16, uint8_t* z, int64_t rows, int
                                   cudaStream_t s) {
   const int rpb = rows_per_block(Kp >> 3);
   const int64_t blocks = (rows + rpb - 1) / rpb;
-  fp16_to_planes_kernel<<<unsigned(blocks), 256, 0, s>>>(static_cast<const __half2*>(a16), z,
-                                                         rows, K, Kp, rpb);
+  fp16_to_planes_kernel<<<unsigned(blocks), 256, 0, s>>>(
+      static_cast<const __half2*>(a16), z, rows, K, Kp, rpb,
+      (K % 4 == 0 && (reinterpret_cast<uintptr_t>(a16) & 15) == 0) ? 1 : 0);
   return cudaGetLastError();
 }
 

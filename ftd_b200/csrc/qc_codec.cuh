@@ -64,21 +64,25 @@ __device__ __forceinline__ void pack16_u6(const uint32_t (&c)[4], uint32_t (&p)[
 
 // Four (4,4)b two's-complement bytes (low nibble Re, high nibble Im, each in
 // [-8, 7]: the XEngine's packet format, promote_data.cuh:66-67) -> E4M3 bytes
-// of the Re and of the Im parts.  Nibbles 0..7 are 0..7; 8..15 are -8..-1,
-// E4M3 codes D0 CE CC CA C8 C4 C0 B8.
-__device__ __forceinline__ uint32_t tc_nibbles_to_e4m3(uint32_t nib) {  // 4 bytes of 0..15
+// of the Re and of the Im parts.  Nibbles 0..7 are 0..7 (E4M3 codes 00 38 40
+// 44 48 4A 4C 4E); 8..15 are -8..-1 (D0 CE CC CA C8 C4 C0 B8).  For two bytes
+// at a time the low three bits of the nibbles (Re0, Im0, Re1, Im1) select from
+// the positive and from the negative table, and a third permute over 00 / FF
+// turns each nibble's bit 3 into a byte mask that picks between them; two more
+// permutes split the interleaved codes into the Re and the Im word.
+__device__ __forceinline__ uint32_t tc_pick(uint32_t m, uint32_t signsel) {
   constexpr uint32_t kP0 = 0x44403800u, kP1 = 0x4E4C4A48u;
   constexpr uint32_t kN0 = 0xCACCCED0u, kN1 = 0xB8C0C4C8u;
-  const uint32_t m = nib & 0x07070707u;
-  uint32_t sel = m | (m >> 4);
-  sel = (sel & 0xFFu) | ((sel >> 8) & 0xFF00u);
-  const uint32_t pos = __byte_perm(kP0, kP1, sel), neg = __byte_perm(kN0, kN1, sel);
-  const uint32_t mask = ((nib >> 3) & 0x01010101u) * 0xFFu;
+  const uint32_t pos = __byte_perm(kP0, kP1, m), neg = __byte_perm(kN0, kN1, m);
+  const uint32_t mask = __byte_perm(0u, 0xFFFFFFFFu, signsel);  // selector 4: FF, 0: 00
   return (pos & ~mask) | (neg & mask);
 }
 __device__ __forceinline__ void tc4_to_e4m3(uint32_t w, uint32_t& re, uint32_t& im) {
-  re = tc_nibbles_to_e4m3(w & 0x0F0F0F0Fu);
-  im = tc_nibbles_to_e4m3((w >> 4) & 0x0F0F0F0Fu);
+  const uint32_t m = w & 0x77777777u;
+  const uint32_t c01 = tc_pick(m, (w >> 1) & 0x4444u);         // Re0 Im0 Re1 Im1
+  const uint32_t c23 = tc_pick(m >> 16, (w >> 17) & 0x4444u);  // Re2 Im2 Re3 Im3
+  re = __byte_perm(c01, c23, 0x6420u);
+  im = __byte_perm(c01, c23, 0x7531u);
 }
 
 }  // namespace ftdx
