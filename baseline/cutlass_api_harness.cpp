@@ -30,6 +30,29 @@ void* ref_api_create() {
 
 void ref_api_destroy(void* h) { delete static_cast<CutlassComplexGemm*>(h); }
 
+// Tile configuration of the reference's CUTLASS baseline GEMMs
+// (cutlass_gemm_api::TileConfig ordinal): only the single-CTA-cluster ones
+// are accepted (0 Auto, 1 HerkOptimal 128x128, 2 GemmOptimal 128x128,
+// 3 WideN 128x256, 6 SmallTile 128x64); -2 for any other.
+int ref_api_set_tile_config(void* h, int cfg) {
+  using cutlass_gemm_api::TileConfig;
+  TileConfig tc;
+  switch (cfg) {
+    case 0: tc = TileConfig::Auto; break;
+    case 1: tc = TileConfig::HerkOptimal; break;
+    case 2: tc = TileConfig::GemmOptimal; break;
+    case 3: tc = TileConfig::WideN; break;
+    case 6: tc = TileConfig::SmallTile; break;
+    default: return -2;
+  }
+  try {
+    static_cast<CutlassComplexGemm*>(h)->set_tile_config(tc);
+    return 0;
+  } catch (...) {
+    return -1;
+  }
+}
+
 // Pre-allocates the reference's HERK buffers for up to (N, K, batch).
 int ref_api_init_herk(void* h, int N, int K, int batch, void* stream) {
   try {

@@ -247,6 +247,8 @@ def load_reference_api():
     L.ref_api_herk_qc_fp32.argtypes = [vp, vp, vp, i, i, i, i, vp]
     L.ref_api_herk.restype = i
     L.ref_api_herk.argtypes = [vp, vp, vp, i, i, i, i, i, ctypes.c_float, ctypes.c_float, i, vp]
+    L.ref_api_set_tile_config.restype = i
+    L.ref_api_set_tile_config.argtypes = [vp, i]
     return L
 
 
@@ -291,7 +293,14 @@ def run_reference_api_leg(torch, dev, qc, C_ours, N, K, B, steps):
             if L.ref_api_init_herk(h, N, K, B, ctypes.c_void_p(stream.cuda_stream)) != 0:
                 return {**out, "unavailable": "init_herk failed"}
             C = torch.empty(B, tri_size(N), 2, device=dev)
-            for name, mode in (("auto", 0), ("cutlass_baseline", 2)):
+            # its default tile configuration, then the other single-CTA-cluster
+            # ones its autotuner could pick (GemmOptimal, WideN, SmallTile)
+            runs = [("auto", 0, 0), ("cutlass_baseline", 2, 0), ("cutlass_baseline_gemm_optimal", 2, 2),
+                    ("cutlass_baseline_wide_n", 2, 3), ("cutlass_baseline_small_tile", 2, 6)]
+            for name, mode, cfg in runs:
+                if L.ref_api_set_tile_config(h, cfg) != 0:
+                    out[name] = {"unavailable": f"tile configuration {cfg} refused"}
+                    continue
                 def call():
                     rc = L.ref_api_herk_qc_fp32(h, ctypes.c_void_p(qc.data_ptr()),
                                                 ctypes.c_void_p(C.data_ptr()), N, K, B, mode,
@@ -306,6 +315,11 @@ def run_reference_api_leg(torch, dev, qc, C_ours, N, K, B, steps):
                     continue
                 out[name] = {"value": herk_flops(N, K, B) / (ms * 1e-3) / 1e12, "unit": UNIT,
                              "ms_per_step": ms, "bit_exact_vs_library": bool(torch.equal(C, C_ours))}
+            L.ref_api_set_tile_config(h, 0)
+            best = [v for k, v in out.items() if k.startswith("cutlass_baseline")
+                    and isinstance(v, dict) and "value" in v]
+            if best:
+                out["cutlass_baseline_best"] = max(best, key=lambda v: v["value"])
             del C
         finally:
             torch.cuda.synchronize()
@@ -688,10 +702,11 @@ def run_ours(args, rank, world, dist):
         e2e = run_e2e(torch, args, dev, qc, N, K, B, flops, world, dist)
 
     batched = precision = differentiation = raw_layout = imaging = xengine = splitk = None
-    imaging_visbf = config1 = fp16_out = None
+    imaging_visbf = config1 = fp16_out = nvfp4_gauss = None
     if not args.no_extra:
         config1 = run_config1_leg(torch, dev)
         fp16_out = run_fp16_output_leg(torch, dev, qc, N, K, B, world)
+        nvfp4_gauss = run_nvfp4_case(torch, dev, N, K, B)
         batched = run_batched_leg(torch, dev)
         raw_layout = run_ftd_leg(torch, dev)
         imaging = run_imaging_leg(torch, dev)
@@ -766,6 +781,7 @@ def run_ours(args, rank, world, dist):
         "sustained": sustained,
         "config1_small": config1,
         "fp16_output": fp16_out,
+        "nvfp4_gaussian": nvfp4_gauss,
         "config3_batched_uneven": ({"value": batched["value"], "unit": UNIT,
                                     "ms_per_step": batched["ms_per_step"],
                                     "frac_of_fp8_cublaslt": (batched["value"] / peak)
@@ -780,8 +796,8 @@ def run_ours(args, rank, world, dist):
         "vs_reference_api_default": ((value / ref_api["auto"]["value"])
                                      if ref_api and "value" in ref_api.get("auto", {}) else None),
         "vs_reference_cutlass_baseline": (
-            (value / ref_api["cutlass_baseline"]["value"])
-            if ref_api and "value" in ref_api.get("cutlass_baseline", {}) else None),
+            (value / ref_api["cutlass_baseline_best"]["value"])
+            if ref_api and "value" in ref_api.get("cutlass_baseline_best", {}) else None),
         "e2e": e2e,
         "batched_uneven_flagged": batched,
         "raw_layout_fused_corner_turn": raw_layout,
@@ -1179,7 +1195,7 @@ def run_nvfp4_case(torch, dev, N, K, B, reps=5, seed=1, split=False, store_mode=
     timed with CUDA events.  split: the hi + lo mode (three products).
     store_mode 0 / 2: single-CTA / CTA-pair kernel (None: autotuned)."""
     from ftd_b200 import Correlator, tri_size
-    from ftd_b200._lib import COMPUTE_FP4, COMPUTE_FP4_SPLIT, IN_FP32, OUT_FP32
+    from ftd_b200._lib import COMPUTE_FP4, COMPUTE_FP4_SPLIT, COMPUTE_FP8, IN_FP32, OUT_FP32
     mode = COMPUTE_FP4_SPLIT if split else COMPUTE_FP4
     g = torch.Generator(device=dev).manual_seed(seed)
     A = torch.randn(B, N, K, 2, device=dev, generator=g)
@@ -1192,6 +1208,11 @@ def run_nvfp4_case(torch, dev, N, K, B, reps=5, seed=1, split=False, store_mode=
         ms = _timed(torch, lambda: c.herk(A, C, N, K, B, input=IN_FP32, compute=mode,
                                           output=OUT_FP32, tune=tune), reps=reps)
         tuned = c.lookup_tuned(N, K, B, input=IN_FP32, output=OUT_FP32) if tune else None
+        # the FP8 path on the same FP32 input (per-channel scale), for comparison
+        c.herk(A, C, N, K, B, input=IN_FP32, compute=COMPUTE_FP8, output=OUT_FP32, tune=tune)
+        fp8_ms = _timed(torch, lambda: c.herk(A, C, N, K, B, input=IN_FP32, compute=COMPUTE_FP8,
+                                              output=OUT_FP32, tune=tune), reps=reps)
+        c.herk(A, C, N, K, B, input=IN_FP32, compute=mode, output=OUT_FP32, tune=tune)
         # per-phase CUDA-event times of the same calls (quantiser, correlator)
         c.set_profiling(True)
         for _ in range(reps):
@@ -1208,7 +1229,9 @@ def run_nvfp4_case(torch, dev, N, K, B, reps=5, seed=1, split=False, store_mode=
                         f"Gaussian FP32 complex", "kernel": kernel,
             "value": herk_flops(N, K, B) / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms,
             "quantiser_ms": prof["prep_ms"] / max(prof["prep_launches"], 1),
-            "correlator_ms": prof["herk_ms"] / max(prof["herk_launches"], 1)}
+            "correlator_ms": prof["herk_ms"] / max(prof["herk_launches"], 1),
+            "fp8_channel_scaled_same_input_ms": fp8_ms,
+            "speedup_vs_fp8_same_input": fp8_ms / ms}
 
 
 def run_leg(args):

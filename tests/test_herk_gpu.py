@@ -174,7 +174,7 @@ def test_ggp_entry_point(corr):
 # K = 16, alpha / beta, FP16 output, split-K; and calls it cannot take (K not
 # a multiple of 16, A not 16-byte aligned) run the two-pass path and stay exact.
 @pytest.mark.parametrize("N,K,B", [(200, 208, 3), (128, 1024, 2), (300, 16, 2), (64, 48, 5),
-                                   (260, 100, 2)])
+                                   (260, 100, 2), (1, 16, 3), (129, 2048, 1)])
 def test_fused_promotion_exact(N, K, B):
     qc = oracle.gaussian_qc(4000 + N + K, B, N, K)
     ref = oracle.herk_qc(qc, N, K, B).astype(np.float32)

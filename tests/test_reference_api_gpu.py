@@ -126,3 +126,28 @@ def test_reference_api_alpha_beta(alpha, beta):
     want = C.clone()
     want[:, diag, 1] = 0.0
     assert torch.equal(Rb, want)
+
+
+@pytest.mark.parametrize("cfg", [2, 3, 6])  # GemmOptimal, WideN, SmallTile
+def test_reference_baseline_tile_configs_equal_library(cfg):
+    # the reference's CUTLASS baseline under each single-CTA-cluster tile
+    # configuration its autotuner can choose gives this library's triangles
+    L = _need_api()
+    N, K, B = 256, 256, 2
+    qc = torch.from_numpy(oracle.gaussian_qc(4800, B, N, K).reshape(B, N, K)).to(DEV)
+    C = torch.full((B, tri_size(N), 2), float("nan"), device=DEV)
+    with Correlator() as c:
+        c.herk(qc, C, N, K, B, input=IN_INT4, output=OUT_FP32, tune=False)
+    R = torch.full_like(C, float("nan"))
+    with bench._StdoutToStderr():
+        h = L.ref_api_create()
+        try:
+            assert L.ref_api_set_tile_config(h, cfg) == 0
+            assert L.ref_api_set_tile_config(h, 4) == -2  # cluster configurations are refused
+            assert L.ref_api_set_tile_config(h, cfg) == 0
+            rc = L.ref_api_herk(h, ctypes.c_void_p(qc.data_ptr()), ctypes.c_void_p(R.data_ptr()),
+                                N, K, B, 1, 1, 1.0, 0.0, 2, None)
+            torch.cuda.synchronize()
+        finally:
+            L.ref_api_destroy(h)
+    assert rc == 0 and torch.equal(R, C)
