@@ -39,8 +39,8 @@ FLAGS=(-gencode arch=compute_100a,code=sm_100a -O3 -std=c++17 --expt-relaxed-con
 P1=$!
 "$NVCC" "${FLAGS[@]}" -c "$CI/gemm_blockscaled_dispatch.cu" -o "$OUT/ref_blockscaled.o" &
 P2=$!
-wait $P1
-wait $P2
+wait $P1 || { kill $P2 2>/dev/null; wait $P2 2>/dev/null; echo "build_cutlass_ref: cutlass_gemm_api.cu failed" >&2; exit 1; }
+wait $P2 || { echo "build_cutlass_ref: gemm_blockscaled_dispatch.cu failed" >&2; exit 1; }
 "$NVCC" "${FLAGS[@]}" -x cu -c "$HERE/cutlass_api_harness.cpp" -o "$OUT/ref_cutlass_harness.o"
 "$NVCC" -gencode arch=compute_100a,code=sm_100a -shared -o "$OUT/libref_cutlass_api.so.tmp" \
   "$OUT/ref_cutlass_harness.o" "$OUT/ref_cutlass_gemm_api.o" "$OUT/ref_blockscaled.o" -lcuda
