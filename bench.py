@@ -1207,7 +1207,8 @@ def run_nvfp4_case(torch, dev, N, K, B, reps=5, seed=1, split=False, store_mode=
         c.herk(A, C, N, K, B, input=IN_FP32, compute=mode, output=OUT_FP32, tune=tune)
         ms = _timed(torch, lambda: c.herk(A, C, N, K, B, input=IN_FP32, compute=mode,
                                           output=OUT_FP32, tune=tune), reps=reps)
-        tuned = c.lookup_tuned(N, K, B, input=IN_FP32, output=OUT_FP32) if tune else None
+        tuned = (c.lookup_tuned(N, K, B, input=IN_FP32, output=OUT_FP32, compute=mode)
+                 if tune else None)
         # the FP8 path on the same FP32 input (per-channel scale), for comparison
         c.herk(A, C, N, K, B, input=IN_FP32, compute=COMPUTE_FP8, output=OUT_FP32, tune=tune)
         fp8_ms = _timed(torch, lambda: c.herk(A, C, N, K, B, input=IN_FP32, compute=COMPUTE_FP8,

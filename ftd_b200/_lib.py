@@ -101,6 +101,8 @@ PROTOTYPES = {
                        ctypes.POINTER(_i), ctypes.POINTER(_f)]),
     "ftdx_lookup_tuned": (_i, [_vp, _i, _i, _i, _i, _i, ctypes.POINTER(_i), ctypes.POINTER(_i),
                                ctypes.POINTER(_f)]),
+    "ftdx_lookup_tuned_compute": (_i, [_vp, _i, _i, _i, _i, _i, _i, ctypes.POINTER(_i),
+                                       ctypes.POINTER(_i), ctypes.POINTER(_f)]),
     "ftdx_set_graph_mode": (_i, [_vp, _i]),
     "ftdx_graph_count": (_i, [_vp]),
     "ftdx_set_strategy": (_i, [_vp, _i, _i]),

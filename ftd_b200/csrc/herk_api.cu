@@ -627,8 +627,16 @@ ftdx_status ftdx_tune(ftdx_handle h, const void* A, void* C, int N, int K, int b
 
 ftdx_status ftdx_lookup_tuned(ftdx_handle h, int N, int K, int batch, ftdx_input input,
                               ftdx_output output, int* store_mode, int* grid, float* ms) {
+  return ftdx_lookup_tuned_compute(h, N, K, batch, input, FTDX_COMPUTE_FP8, output, store_mode,
+                                   grid, ms);
+}
+
+ftdx_status ftdx_lookup_tuned_compute(ftdx_handle h, int N, int K, int batch, ftdx_input input,
+                                      ftdx_compute compute, ftdx_output output, int* store_mode,
+                                      int* grid, float* ms) {
   if (!h) return FTDX_ERR_INVALID_ARG;
-  const HerkCall c{nullptr, nullptr, N, K, batch, input, output, 1.f, 0.f};
+  HerkCall c{nullptr, nullptr, N, K, batch, input, output, 1.f, 0.f};
+  c.compute = compute;
   auto it = h->tuned.find(tune_key(h, c));
   if (it == h->tuned.end()) return fail(h, FTDX_ERR_CACHE, "no tuned entry for this shape");
   if (store_mode) *store_mode = it->second.st.store_mode;

@@ -226,11 +226,12 @@ class Correlator:
         return {"store_mode": sm.value, "grid": g.value, "ms": ms.value}
 
     def lookup_tuned(self, N: int, K: int, batch: int, input: int = IN_INT4,
-                     output: int = OUT_FP32):
-        """The cached strategy for a shape, or None."""
+                     output: int = OUT_FP32, compute: int = COMPUTE_FP8):
+        """The cached strategy for a shape and compute mode, or None."""
         sm, g, ms = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_float(0)
-        st = self._L.ftdx_lookup_tuned(self._h, N, K, batch, input, output, ctypes.byref(sm),
-                                       ctypes.byref(g), ctypes.byref(ms))
+        st = self._L.ftdx_lookup_tuned_compute(self._h, N, K, batch, input, compute, output,
+                                               ctypes.byref(sm), ctypes.byref(g),
+                                               ctypes.byref(ms))
         if st != _lib.FTDX_OK:
             return None
         return {"store_mode": sm.value, "grid": g.value, "ms": ms.value}

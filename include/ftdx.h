@@ -319,9 +319,16 @@ FTDX_API ftdx_status ftdx_tune(ftdx_handle h, const void* A, void* C, int N, int
                                ftdx_input input, ftdx_output output, void* stream,
                                int* store_mode, int* grid, float* ms);
 
-/* Query the tuned strategy of a shape (FTDX_ERR_CACHE when there is none). */
+/* Query the tuned strategy of a shape (FTDX_ERR_CACHE when there is none),
+ * for calls with FP8 compute. */
 FTDX_API ftdx_status ftdx_lookup_tuned(ftdx_handle h, int N, int K, int batch, ftdx_input input,
                                        ftdx_output output, int* store_mode, int* grid, float* ms);
+/* The same for calls with the given compute mode (the tuner keeps separate
+ * entries per compute mode, e.g. FP8 and NVFP4 on the same FP32 input). */
+FTDX_API ftdx_status ftdx_lookup_tuned_compute(ftdx_handle h, int N, int K, int batch,
+                                               ftdx_input input, ftdx_compute compute,
+                                               ftdx_output output, int* store_mode, int* grid,
+                                               float* ms);
 
 /* Graph mode: each distinct call (pointers, sizes, precisions, alpha, beta,
  * strategy) is captured once into a CUDA graph and replayed afterwards

@@ -139,3 +139,23 @@ def test_capture_without_workspace_fails_cleanly():
             with torch.cuda.graph(g, stream=s):
                 c.herk(d, C, N, K, B, input=IN_INT4, output=OUT_FP32, tune=False, stream=s)
         assert "CAPACITY" in str(ei.value)
+
+
+def test_tuned_entries_kept_per_compute_mode():
+    # FP32 input tuned under NVFP4 leaves an NVFP4 entry only; the FP8 lookup
+    # of the same shape stays empty until an FP8 call tunes it
+    from ftd_b200._lib import COMPUTE_FP4, COMPUTE_FP8, IN_FP32
+    N, K, B = 256, 256, 2
+    rng = np.random.default_rng(60)
+    A = torch.from_numpy(rng.standard_normal((B, N, K, 2)).astype(np.float32)).to(DEV)
+    C = torch.empty(B, tri_size(N), 2, device=DEV)
+    with Correlator() as c:
+        c.herk(A, C, N, K, B, input=IN_FP32, compute=COMPUTE_FP4, output=OUT_FP32, tune=True)
+        fp4 = c.lookup_tuned(N, K, B, input=IN_FP32, output=OUT_FP32, compute=COMPUTE_FP4)
+        assert fp4 is not None and fp4["ms"] > 0
+        assert c.lookup_tuned(N, K, B, input=IN_FP32, output=OUT_FP32,
+                              compute=COMPUTE_FP8) is None
+        c.herk(A, C, N, K, B, input=IN_FP32, compute=COMPUTE_FP8, output=OUT_FP32, tune=True)
+        assert c.lookup_tuned(N, K, B, input=IN_FP32, output=OUT_FP32,
+                              compute=COMPUTE_FP8) is not None
+        assert c.device_status() == 0
