@@ -92,7 +92,7 @@ struct ftdx_context {
   // FP8 operand workspace (grown on demand, or pre-sized by ftdx_init_herk)
   uint8_t* z = nullptr;
   size_t z_cap = 0;
-  // per-channel scales of float inputs: qscale[batch], out_scale[batch], amax[batch]
+  // float inputs: promotion arrival words [32 x batch], amax[batch], qscale[batch], out_scale[batch]
   uint8_t* aux = nullptr;
   size_t aux_cap = 0;
   uint32_t* d_status = nullptr;

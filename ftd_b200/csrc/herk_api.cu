@@ -180,7 +180,7 @@ ftdx_status prepare(ftdx_handle h, const HerkCall& c, cudaStream_t s, const Plan
       fused ? FTDX_OK : ensure_workspace(h, size_t((pair ? 3 : 2) * rows * zpitch), s);
   if (st != FTDX_OK) return st;
   if (c.input == FTDX_IN_FP32) {
-    st = ensure_aux(h, size_t(12) * size_t(c.batch) + 256, s);
+    st = ensure_aux(h, size_t(140) * size_t(c.batch) + 256, s);
     if (st != FTDX_OK) return st;
   }
   if (splits > 1) {
@@ -205,9 +205,11 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
   const int64_t rows = int64_t(c.N) * c.batch;
   const bool fp6 = ((strat.store_mode & kStoreFp6) || c.compute == FTDX_COMPUTE_FP6) && fp6_ok(c);
   const bool s8 = !fp6 && pair && (strat.store_mode & kStoreS8) && fp6_ok(c);
-  float* qscale = reinterpret_cast<float*>(h->aux);
+  // float inputs: arrival words (32 per channel), amax, qscale, out_scale
+  uint32_t* arrive = reinterpret_cast<uint32_t*>(h->aux);
+  uint32_t* amax = arrive + int64_t(c.batch) * 32;
+  float* qscale = reinterpret_cast<float*>(amax + c.batch);
   float* out_scale = qscale + c.batch;
-  uint32_t* amax = reinterpret_cast<uint32_t*>(out_scale + c.batch);
   cudaError_t e = cudaSuccess;
   if (!fused) {
     ScopedTimer tm(h, s, 1);
@@ -236,12 +238,14 @@ ftdx_status launch_all(ftdx_handle h, const HerkCall& c, const Strategy& strat, 
           : s8 ? launch_qc_to_planes_s8(qc, h->z, rows, c.K, int(Kp), s, pair)
                : launch_qc_to_planes(qc, h->z, rows, c.K, int(Kp), s, pair);
     } else {
-      if (c.input == FTDX_IN_FP16)
+      if (c.input == FTDX_IN_FP16) {
         e = launch_fp16_to_planes(c.A, h->z, rows, c.K, int(Kp), s);
-      else
+        if (e == cudaSuccess && pair) e = launch_negate_plane(h->z, rows * zpitch, h->sm_count, s);
+      } else {
         e = launch_float_to_planes(c.A, h->z, rows, c.K, int(Kp), int(zpitch), c.N, c.batch,
-                                   is_split(c) ? 1 : 0, qscale, out_scale, amax, h->sm_count, s);
-      if (e == cudaSuccess && pair) e = launch_negate_plane(h->z, rows * zpitch, h->sm_count, s);
+                                   is_split(c) ? 1 : 0, pair ? 1 : 0, qscale, out_scale, amax,
+                                   arrive, h->d_status, h->sm_count, s);
+      }
     }
   }
   if (e != cudaSuccess) return cuda_fail(h, e, "operand promotion launch");

@@ -253,10 +253,14 @@ cudaError_t launch_nvfp4(const void* A, int64_t rows, int K, int n, int batch, u
                          const TileDesc* tiles, const ChanDesc* chans, int num_tiles, void* C,
                          float alpha, float beta, uint32_t* status, int sm_count, void* encode_fn,
                          cudaStream_t s, int split = 0, int pair = 0, int phases = 3);
-// Float complex [rows][K] -> scaled E4M3 planes of pitch zpitch (precision.cu).
+// Float complex [rows][K] -> scaled E4M3 planes of pitch zpitch (precision.cu);
+// neg: also plane 2 (-Re).  arrive: 32 words per channel, 128-byte aligned,
+// directly followed by amax_bits[batch] (the one-pass cooperative kernel
+// needs that placement; any other takes the three-kernel path).
 cudaError_t launch_float_to_planes(const void* a, uint8_t* z, int64_t rows, int K, int Kp,
-                                   int zpitch, int n, int batch, int split, float* qscale,
-                                   float* out_scale, uint32_t* amax_bits, int sm_count,
+                                   int zpitch, int n, int batch, int split, int neg,
+                                   float* qscale, float* out_scale, uint32_t* amax_bits,
+                                   uint32_t* arrive, uint32_t* status, int sm_count,
                                    cudaStream_t s);
 
 }  // namespace ftdx

@@ -344,6 +344,39 @@ def test_fp8_float_modes_match_restated_quantiser(store_mode):
         assert err <= tol
 
 
+@pytest.mark.parametrize("store_mode", [0, 2])
+def test_fp8_float_channel_scales_graph_replay(store_mode):
+    # nine channels whose amplitudes span 1e-3 .. 1e3 (one of them all zero),
+    # an odd K (8-byte loads, a ragged last unit) and a row count that splits
+    # unevenly over the promotion's blocks: every channel against the restated
+    # quantiser at 1e-6 of its own largest element, and graph capture plus
+    # two replays give the direct call's bits
+    B, N, K = 9, 130, 203
+    rng = np.random.default_rng(414)
+    v = (rng.standard_normal((B, N, K)) + 1j * rng.standard_normal((B, N, K))).astype(np.complex64)
+    v *= (10.0 ** np.linspace(-3, 3, B)).astype(np.float32)[:, None, None]
+    v[4] = 0
+    A = torch.from_numpy(np.ascontiguousarray(v).view(np.float32).reshape(B, N, K, 2)).to(DEV)
+    ref = oracle.herk_fp8_scaled(v, False)
+    outs = []
+    with Correlator() as c:
+        c.set_strategy(store_mode, 0)
+        for graph in (False, True, True):
+            c.set_graph_mode(graph)
+            C = torch.full((B, tri_size(N), 2), float("nan"), device=DEV)
+            c.herk(A, C, N, K, B, input=IN_FP32, compute=COMPUTE_FP8, output=OUT_FP32, tune=False)
+            torch.cuda.synchronize()
+            outs.append(C.cpu().numpy())
+        assert c.graph_count() >= 1
+        assert c.device_status() == 0
+    got = outs[0].astype(np.float64)
+    for b in range(B):
+        scale = max(np.abs(ref[b]).max(), 1e-30)
+        assert np.abs(got[b] - ref[b]).max() <= 1e-6 * scale, b
+    assert not np.any(outs[0][4])
+    assert np.array_equal(outs[1], outs[0]) and np.array_equal(outs[2], outs[0])
+
+
 def test_nvfp4_rfi_at_independent_times_and_handle_reuse():
     # bursts at each input's own random times (the union of flagged samples is
     # ~10x the shared-time case: F ~ 120 of K = 1024, still one lo stage), a
