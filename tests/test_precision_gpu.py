@@ -377,6 +377,21 @@ def test_fp8_float_channel_scales_graph_replay(store_mode):
     assert np.array_equal(outs[1], outs[0]) and np.array_equal(outs[2], outs[0])
 
 
+@pytest.mark.parametrize("B,N,K,store_mode", [(1, 64, 128, 0), (40, 16, 64, 2), (3, 129, 1024, 0)])
+def test_fp8_float_promotion_step_edges(B, N, K, store_mode):
+    # one channel (one amax step, one quantisation step), forty small
+    # channels (forty waits between blocks; the CTA pair's -Re plane), and
+    # rows that split unevenly over the promotion's blocks: the restated
+    # quantiser at 1e-6 of each channel's largest element
+    rng = np.random.default_rng(415 + B)
+    v = (rng.standard_normal((B, N, K)) + 1j * rng.standard_normal((B, N, K))).astype(np.complex64)
+    v *= rng.uniform(0.01, 100.0, size=(B, 1, 1)).astype(np.float32)
+    got = run_float(v, COMPUTE_FP8, store_mode).astype(np.float64)
+    ref = oracle.herk_fp8_scaled(v, False)
+    for b in range(B):
+        assert np.abs(got[b] - ref[b]).max() <= 1e-6 * np.abs(ref[b]).max(), b
+
+
 def test_nvfp4_rfi_at_independent_times_and_handle_reuse():
     # bursts at each input's own random times (the union of flagged samples is
     # ~10x the shared-time case: F ~ 120 of K = 1024, still one lo stage), a
