@@ -234,19 +234,9 @@ __device__ __forceinline__ float wait_channel_scale(int cq, float* __restrict__ 
                                                     float* __restrict__ out_scale,
                                                     uint32_t* amax_bits, uint32_t* arrive_word,
                                                     uint32_t* status, bool& aborted) {
-  if (!aborted) {
-    const uint64_t t_start = dev::globaltimer_ns();
-    for (uint32_t it = 0;; ++it) {
-      uint32_t v;
-      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(arrive_word) : "memory");
-      if (v >= gridDim.x) break;
-      if ((it & 15u) == 15u && dev::globaltimer_ns() - t_start > FTDX_WAIT_NS) {
-        atomicOr(status, dev::kStatusTimeoutOther);
-        aborted = true;
-        break;
-      }
-      __nanosleep(64);
-    }
+  if (!aborted && !dev::flag_wait_limit(arrive_word, gridDim.x, FTDX_WAIT_NS)) {
+    atomicOr(status, dev::kStatusTimeoutOther);
+    aborted = true;
   }
   uint32_t mb;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(mb) : "l"(amax_bits + cq) : "memory");

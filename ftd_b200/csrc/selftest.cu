@@ -1,12 +1,16 @@
 // selftest.cu -- exercises the failure path of the kernels' bounded waits
 // without faulting anything (ftdx_wait_selftest): one CTA waits, with a short
-// limit, on an mbarrier that nothing arrives on, gives up, records the
-// timeout in the handle's status word and returns.  The context stays usable.
+// limit, on an mbarrier that nothing arrives on, then on a global flag that
+// nothing sets (the wait between the blocks of the cooperative FP8
+// promotion); when both give up it records the timeout in the handle's
+// status word and returns.  The context stays usable.
 #include "context.h"
 #include "sm100.cuh"
 
 namespace ftdx {
 namespace {
+
+__device__ uint32_t g_never_set = 0;  // no code writes it
 
 __global__ void wait_selftest_kernel(uint32_t* status, uint64_t limit_ns) {
   __shared__ __align__(8) uint64_t bar;
@@ -19,8 +23,9 @@ __global__ void wait_selftest_kernel(uint32_t* status, uint64_t limit_ns) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile int* ab = &abort_flag;
-    if (!dev::mbar_wait_limit(dev::smem_u32(&bar), 0, ab, limit_ns))
-      atomicOr(status, dev::kStatusTimeoutOther);
+    const bool bar_done = dev::mbar_wait_limit(dev::smem_u32(&bar), 0, ab, limit_ns);
+    const bool flag_done = dev::flag_wait_limit(&g_never_set, 1u, limit_ns);
+    if (!bar_done && !flag_done) atomicOr(status, dev::kStatusTimeoutOther);
   }
 }
 

@@ -87,6 +87,21 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
   return mbar_wait_limit(bar, parity, abort_flag, FTDX_WAIT_NS);
 }
 
+// Bounded wait until the global word reaches `target` (acquire loads, polled
+// with a short sleep): the blocks of a cooperative launch waiting on one
+// another.  Returns false after limit_ns nanoseconds.
+__device__ __forceinline__ bool flag_wait_limit(const uint32_t* word, uint32_t target,
+                                                uint64_t limit_ns) {
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t it = 0;; ++it) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(word) : "memory");
+    if (v >= target) return true;
+    if ((it & 15u) == 15u && globaltimer_ns() - t0 > limit_ns) return false;
+    __nanosleep(64);
+  }
+}
+
 // ---------------------------------------------------------------- TMA
 __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* m) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(m)) : "memory");

@@ -233,10 +233,12 @@ FTDX_API ftdx_status ftdx_image_beams(ftdx_handle h, const ftdx_imaging_config* 
                                       void* stream);
 
 /* Failure-path self-test of the bounded device waits (no counterpart in the
- * reference): one kernel waits, for timeout_ms (1..2000), on an mbarrier that
- * nothing arrives on, gives up and records the timeout in the status word;
- * ftdx_device_status then returns FTDX_ERR_TIMEOUT and the handle stays
- * usable.  Nothing traps or faults. */
+ * reference): one kernel waits, for timeout_ms (1..2000) each, on an mbarrier
+ * that nothing arrives on and on a global flag that nothing sets (the waits
+ * inside the correlators and between the blocks of the FP8 promotion), gives
+ * up on both and records the timeout in the status word; ftdx_device_status
+ * then returns FTDX_ERR_TIMEOUT and the handle stays usable.  Nothing traps
+ * or faults. */
 FTDX_API ftdx_status ftdx_wait_selftest(ftdx_handle h, int timeout_ms, void* stream);
 
 /* The XEngine's correlation (ggp::XEngine::compute, lib/xengine.cpp:108-178:

@@ -1,6 +1,7 @@
-"""Failure detection on the GPU without faulting it: a bounded device wait
-is made to run out (an mbarrier nothing arrives on), the timeout shows up in
-the status word, and the same handle then correlates bit-exactly."""
+"""Failure detection on the GPU without faulting it: bounded device waits
+are made to run out (an mbarrier nothing arrives on, then a global flag
+nothing sets), the timeout shows up in the status word, and the same handle
+then correlates bit-exactly."""
 import time
 
 import numpy as np
@@ -24,7 +25,7 @@ def test_bounded_wait_times_out_and_handle_recovers():
         bits = c.device_status()
         dt = time.perf_counter() - t0
         assert bits != 0                 # the timeout bit
-        assert 0.09 < dt < 5.0           # it waited about the limit, then gave up
+        assert 0.19 < dt < 5.0           # it waited about the limit twice, then gave up
         assert c.device_status() == 0    # reading clears it
         # the handle and the context are still good
         N, K, B = 200, 96, 2
