@@ -158,7 +158,10 @@ __global__ void __launch_bounds__(256) quantize_kernel(const float2* __restrict_
 }
 
 // L2 policy that makes lines the first to be evicted (for data read for
-// the last time).
+// the last time).  The loads that use it allocate in L1 at evict-first
+// priority: a thread's four 16-byte loads of a unit fall into sectors that
+// neighbouring lanes share, and the second load of each sector then hits L1
+// (85.1 against 87.7 us at 8 channels with no L1 allocation).
 __device__ __forceinline__ uint64_t l2_evict_first_policy() {
   uint64_t pol;
   asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
@@ -166,7 +169,7 @@ __device__ __forceinline__ uint64_t l2_evict_first_policy() {
 }
 __device__ __forceinline__ float4 ldg_last_use(const float4* p, uint64_t pol) {
   float4 v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+  asm volatile("ld.global.nc.L1::evict_first.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
                : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
                : "l"(p), "l"(pol));
   return v;
