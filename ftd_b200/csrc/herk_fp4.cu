@@ -102,14 +102,19 @@ __device__ __forceinline__ float nvfp4_codes_err(const float (&x)[16], float inv
                                                  uint32_t (&w)[2]) {
   w[0] = w[1] = 0u;
   float err = 0.f;
+  const float2 inv2 = make_float2(inv, inv), gb2 = make_float2(gb, gb);
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
-    const uint32_t byte = fp4x2(__fmul_rn(x[2 * q], inv), __fmul_rn(x[2 * q + 1], inv));
+    // packed FP32 pairs: each component rounds as its scalar operation
+    const float2 xq = make_float2(x[2 * q], x[2 * q + 1]);
+    const float2 s = __fmul2_rn(xq, inv2);
+    const uint32_t byte = fp4x2(s.x, s.y);
     w[q >> 2] |= byte << (8 * (q & 3));
     const float2 h = fp4x2_value(byte);
-    const float d0 = __fmaf_rn(-h.x, gb, x[2 * q]), d1 = __fmaf_rn(-h.y, gb, x[2 * q + 1]);
-    err = __fadd_rn(err, __fmul_rn(d0, d0));
-    err = __fadd_rn(err, __fmul_rn(d1, d1));
+    const float2 d = __ffma2_rn(make_float2(-h.x, -h.y), gb2, xq);
+    const float2 dd = __fmul2_rn(d, d);
+    err = __fadd_rn(err, dd.x);
+    err = __fadd_rn(err, dd.y);
   }
   return err;
 }
@@ -180,8 +185,10 @@ __device__ __forceinline__ void nvfp4_block(const float (&x)[16], float g, int64
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const float2 h = fp4x2_value((xw[q >> 2] >> (8 * (q & 3))) & 0xFFu);
-      res[2 * q] = __fmaf_rn(-h.x, gb, x[2 * q]);
-      res[2 * q + 1] = __fmaf_rn(-h.y, gb, x[2 * q + 1]);
+      const float2 r2 = __ffma2_rn(make_float2(-h.x, -h.y), make_float2(gb, gb),
+                                   make_float2(x[2 * q], x[2 * q + 1]));
+      res[2 * q] = r2.x;
+      res[2 * q + 1] = r2.y;
     }
     uint32_t xl[2], yl[2];
     float gb2 = 0.f;
