@@ -395,6 +395,26 @@ def test_fp8_float_promotion_step_edges(B, N, K, store_mode):
         assert np.abs(got[b] - ref[b]).max() <= tol * np.abs(ref[b]).max(), b
 
 
+@pytest.mark.parametrize("store_mode", [0, 2])
+def test_fp8_float_fp16_output_is_rounded_fp32_output(store_mode):
+    # FP32 voltages, per-channel-scaled FP8, FP16 packed output: the epilogue
+    # rounds the same scaled FP32 sums to half (nearest even), so the FP16
+    # triangles equal the FP32 ones rounded by torch, bit for bit
+    from ftd_b200._lib import OUT_FP16
+    B, N, K = 3, 200, 256
+    rng = np.random.default_rng(416)
+    v = (rng.standard_normal((B, N, K)) + 1j * rng.standard_normal((B, N, K))).astype(np.complex64)
+    A = torch.from_numpy(np.ascontiguousarray(v).view(np.float32).reshape(B, N, K, 2)).to(DEV)
+    C32 = torch.full((B, tri_size(N), 2), float("nan"), device=DEV)
+    C16 = torch.full((B, tri_size(N), 2), float("nan"), dtype=torch.float16, device=DEV)
+    with Correlator() as c:
+        c.set_strategy(store_mode, 0)
+        c.herk(A, C32, N, K, B, input=IN_FP32, compute=COMPUTE_FP8, output=OUT_FP32, tune=False)
+        c.herk(A, C16, N, K, B, input=IN_FP32, compute=COMPUTE_FP8, output=OUT_FP16, tune=False)
+        assert c.device_status() == 0
+    assert torch.equal(C16, C32.half())
+
+
 def test_nvfp4_rfi_at_independent_times_and_handle_reuse():
     # bursts at each input's own random times (the union of flagged samples is
     # ~10x the shared-time case: F ~ 120 of K = 1024, still one lo stage), a
