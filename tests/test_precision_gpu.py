@@ -415,6 +415,27 @@ def test_fp8_float_fp16_output_is_rounded_fp32_output(store_mode):
     assert torch.equal(C16, C32.half())
 
 
+@pytest.mark.parametrize("store_mode", [0, 2])
+def test_fp8_float_alpha_beta(store_mode):
+    # C = alpha * (per-channel-scaled FP8 product) + beta * C_old, with the
+    # diagonal's Im of the product zero before beta (the reference's store
+    # rule); FP32 accumulation and scaling: 1e-6 of the largest element
+    B, N, K = 2, 160, 256
+    rng = np.random.default_rng(417)
+    v = (rng.standard_normal((B, N, K)) + 1j * rng.standard_normal((B, N, K))).astype(np.complex64)
+    A = torch.from_numpy(np.ascontiguousarray(v).view(np.float32).reshape(B, N, K, 2)).to(DEV)
+    old = torch.randn(B, tri_size(N), 2, device=DEV)
+    C = old.clone()
+    with Correlator() as c:
+        c.set_strategy(store_mode, 0)
+        c.herk(A, C, N, K, B, input=IN_FP32, compute=COMPUTE_FP8, output=OUT_FP32, alpha=0.5,
+               beta=-2.0, tune=False)
+        assert c.device_status() == 0
+    ref = 0.5 * oracle.herk_fp8_scaled(v, False) - 2.0 * old.double().cpu().numpy()
+    got = C.double().cpu().numpy()
+    assert np.abs(got - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
 def test_nvfp4_rfi_at_independent_times_and_handle_reuse():
     # bursts at each input's own random times (the union of flagged samples is
     # ~10x the shared-time case: F ~ 120 of K = 1024, still one lo stage), a
