@@ -157,29 +157,53 @@ __device__ __forceinline__ uint32_t nvfp4_quant16(const float (&x)[16], float g,
   return best;
 }
 
-// One 16-value block b of input row r (channel c, input w): the hi codes and,
-// when `lo`, the residual r = fma(-code, g b, x) quantised again with its own
-// block scale (same g).  Each operand row holds the hi half (pitch bytes) then
-// the lo half; the lo k-steps of the scales follow the hi ones.  Scales go to
-// sfa (x rows, one per input) and sfb (x and y rows, two per input).
-__device__ __forceinline__ void nvfp4_block(const float (&x)[16], float g, int64_t r, int c, int w,
-                                            int b, uint8_t* __restrict__ z,
-                                            uint8_t* __restrict__ sfa, uint8_t* __restrict__ sfb,
-                                            int pitch, const SfGeom& sg, bool lo) {
-  const int rpitch = 2 * pitch;
-  const int ksh = pitch / 32;  // k-steps per half
-  uint32_t xw[2], yw[2];
-  float gb = 0.f;
-  const uint32_t bc = nvfp4_quant16(x, g, xw, yw, gb);
-  *reinterpret_cast<uint2*>(z + (2 * r) * rpitch + 8 * b) = make_uint2(xw[0], xw[1]);
-  *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + 8 * b) = make_uint2(yw[0], yw[1]);
+// Where one input row's quantiser output goes: its x and y operand rows
+// (hi half of pitch bytes, lo half after it) and its three scale bytes of
+// k-step 0, block 0 (sf_atom_byte: the x row in sfa, the x and y rows in
+// sfb); k-step ks, block blk is at + ks * 512 + blk in sfa and at
+// + ks * sbk + blk in sfb, the lo k-steps ksh after the hi ones.
+struct Fp4RowOut {
+  uint8_t* zx;
+  uint8_t* zy;
+  uint8_t* sa;
+  uint8_t* sbx;
+  uint8_t* sby;
+  int sbk;    // sfb bytes per k-step: nsub atoms of 512
+  int ksh;    // k-steps per half
+  int pitch;  // bytes per half of an operand row
+};
+__device__ __forceinline__ Fp4RowOut fp4_row_out(int64_t r, int c, int w, uint8_t* z,
+                                                 uint8_t* sfa, uint8_t* sfb, int pitch,
+                                                 const SfGeom& sg) {
+  Fp4RowOut o;
+  o.zx = z + (2 * r) * int64_t(2 * pitch);
+  o.zy = o.zx + 2 * pitch;
   const int64_t ga = int64_t(c) * sg.gA + (w >> 7);
   const int64_t gbk = int64_t(c) * sg.gB + (2 * w) / sg.gbrows;
   const int ob = (2 * w) % sg.gbrows;  // x row in the group; y row next (gbrows is even)
+  o.sa = sfa + sf_atom_byte(ga, sg.nks, 1, 0, w & 127, 0);
+  o.sbx = sfb + sf_atom_byte(gbk, sg.nks, sg.nsub, 0, ob, 0);
+  o.sby = sfb + sf_atom_byte(gbk, sg.nks, sg.nsub, 0, ob + 1, 0);
+  o.sbk = sg.nsub * 512;
+  o.ksh = pitch / 32;
+  o.pitch = pitch;
+  return o;
+}
+
+// One 16-value block b of an input row: the hi codes and, when `lo`, the
+// residual r = fma(-code, g b, x) quantised again with its own block scale
+// (same g), written where `o` says.
+__device__ __forceinline__ void nvfp4_block(const float (&x)[16], float g, int b,
+                                            const Fp4RowOut& o, bool lo) {
+  uint32_t xw[2], yw[2];
+  float gb = 0.f;
+  const uint32_t bc = nvfp4_quant16(x, g, xw, yw, gb);
+  *reinterpret_cast<uint2*>(o.zx + 8 * b) = make_uint2(xw[0], xw[1]);
+  *reinterpret_cast<uint2*>(o.zy + 8 * b) = make_uint2(yw[0], yw[1]);
   const int ks = b >> 2, blk = b & 3;
-  sfa[sf_atom_byte(ga, sg.nks, 1, ks, w & 127, blk)] = uint8_t(bc);
-  sfb[sf_atom_byte(gbk, sg.nks, sg.nsub, ks, ob, blk)] = uint8_t(bc);
-  sfb[sf_atom_byte(gbk, sg.nks, sg.nsub, ks, ob + 1, blk)] = uint8_t(bc);
+  o.sa[ks * 512 + blk] = uint8_t(bc);
+  o.sbx[ks * o.sbk + blk] = uint8_t(bc);
+  o.sby[ks * o.sbk + blk] = uint8_t(bc);
   if (lo) {  // the residual fma(-code, g b, x) quantised with its own block scale
     float res[16];
 #pragma unroll
@@ -193,11 +217,12 @@ __device__ __forceinline__ void nvfp4_block(const float (&x)[16], float g, int64
     uint32_t xl[2], yl[2];
     float gb2 = 0.f;
     const uint32_t bc2 = nvfp4_quant16(res, g, xl, yl, gb2);
-    *reinterpret_cast<uint2*>(z + (2 * r) * rpitch + pitch + 8 * b) = make_uint2(xl[0], xl[1]);
-    *reinterpret_cast<uint2*>(z + (2 * r + 1) * rpitch + pitch + 8 * b) = make_uint2(yl[0], yl[1]);
-    sfa[sf_atom_byte(ga, sg.nks, 1, ksh + ks, w & 127, blk)] = uint8_t(bc2);
-    sfb[sf_atom_byte(gbk, sg.nks, sg.nsub, ksh + ks, ob, blk)] = uint8_t(bc2);
-    sfb[sf_atom_byte(gbk, sg.nks, sg.nsub, ksh + ks, ob + 1, blk)] = uint8_t(bc2);
+    *reinterpret_cast<uint2*>(o.zx + o.pitch + 8 * b) = make_uint2(xl[0], xl[1]);
+    *reinterpret_cast<uint2*>(o.zy + o.pitch + 8 * b) = make_uint2(yl[0], yl[1]);
+    const int kl = o.ksh + ks;
+    o.sa[kl * 512 + blk] = uint8_t(bc2);
+    o.sbx[kl * o.sbk + blk] = uint8_t(bc2);
+    o.sby[kl * o.sbk + blk] = uint8_t(bc2);
   }
 }
 
@@ -359,6 +384,7 @@ __global__ void __launch_bounds__(256, 4) nvfp4_quant_kernel(
     const bool permuted = __ldg(nflag + c) > 0;
     const int lo_from = (kp / 128 - chans[c].pad) * 16;  // first block with a residual
     const int32_t* sc = src + int64_t(c) * kp;
+    const Fp4RowOut o = fp4_row_out(r, c, w, z, sfa, sfb, pitch, sg);
     for (int b = lane; b < blocks_per_row; b += 32) {
       const int t0 = 8 * b;
       float x[16];
@@ -377,7 +403,7 @@ __global__ void __launch_bounds__(256, 4) nvfp4_quant_kernel(
           x[2 * q] = v.x, x[2 * q + 1] = v.y;
         }
       }
-      nvfp4_block(x, g, r, c, w, b, z, sfa, sfb, pitch, sg, b >= lo_from);
+      nvfp4_block(x, g, b, o, b >= lo_from);
     }
   }
 }
